@@ -1,0 +1,163 @@
+"""Pins the oracle (CPU restatement) before it is trusted as the checker:
+
+1. the compiled upstream sources, driven like LoadInitParam::run, reproduce
+   the upstream golden smoke frames (test/functional/true_data/*/4.dat.gz,
+   kept as tests/golden/smoke_frame4.npz);
+2. the restatement, fed the upstream-initialised particles, reproduces the
+   same golden frames;
+3. the restatement is bit-identical to the compiled upstream step on seeded
+   inputs (Boris, Vay, the default adaptive build, absorbing layer, bunch).
+"""
+import numpy as np
+import pytest
+
+from helpers import (GOLDEN, GRIDS, SMOKE, golden_match, oracle_from_workload,
+                     recover_weights, ref_from_workload, seed_fields)
+from oracle import refsim
+from oracle.oracle import OracleSim, random_reverse
+from pdp3_b200 import workloads as W
+
+needs_ref = pytest.mark.skipif(not refsim.available("boris"),
+                               reason="oracle/_ref not built (needs the upstream sources)")
+
+FIELDS = ["E_r", "E_phi", "E_z", "H_r", "H_phi", "H_z", "J_r", "J_phi", "J_z"]
+
+
+def _smoke_ref():
+    ref = refsim.RefSim(SMOKE["r_size"], SMOKE["z_size"], SMOKE["n_grid_r"], SMOKE["n_grid_z"],
+                        SMOKE["dt"], end_time=SMOKE["end_time"], pusher="adaptive")
+    for name, c, m, n, nl, nrt, t in SMOKE["species"]:
+        ref.add_species_upstream_init(name, c, m, n, nl, nrt, t)
+    b = SMOKE["beam"]
+    ref.set_beam(b["charge_e"], b["mass_me"], b["number_macro"], b["bunch_length"],
+                 b["radius"], b["density"], b["velocity"], b["number_bunches"],
+                 b["bunches_distance"])
+    return ref
+
+
+def _run_to_frame(sim, frame_idx, schedule=5):
+    """Steps until the dump test (int)(t/dt) % schedule == 0 fires for the
+    frame_idx-th time (src/loadInitParam.cpp:329); returns the step count."""
+    frame, steps = 0, 0
+    while True:
+        sched = sim.step()
+        steps += 1
+        if sched % schedule == 0:
+            if frame == frame_idx:
+                return steps
+            frame += 1
+
+
+@needs_ref
+def test_reference_build_reproduces_golden_smoke():
+    g = np.load(GOLDEN)
+    ref = _smoke_ref()
+    assert _run_to_frame(ref, 4) == 21
+    for comp in FIELDS:
+        r0, z0, r1, z1 = g[comp + "__box"]
+        ok = golden_match(ref.field(comp)[r0:r1, z0:z1], g[comp])
+        assert ok.all(), (comp, int((~ok).sum()))
+    # The golden rho_beam frame equals one charge weighting of the bunch (the
+    # grid the step leaves in rho_bunch); the current upstream dump code adds
+    # a second weighting (src/loadInitParam.cpp:361-366), which the upstream
+    # test's atol=1 does not detect at these magnitudes (~1e-4).
+    r0, z0, r1, z1 = g["rho_beam__box"]
+    ok = golden_match(ref.field("rho_bunch")[r0:r1, z0:z1], g["rho_beam"])
+    assert ok.all()
+    assert (g["rho_beam"] != 0).sum() > 100
+
+
+@needs_ref
+def test_oracle_reproduces_golden_smoke():
+    g = np.load(GOLDEN)
+    ref = refsim.RefSim(SMOKE["r_size"], SMOKE["z_size"], SMOKE["n_grid_r"], SMOKE["n_grid_z"],
+                        SMOKE["dt"], end_time=SMOKE["end_time"], pusher="boris")
+    orc = OracleSim(SMOKE["r_size"], SMOKE["z_size"], SMOKE["n_grid_r"], SMOKE["n_grid_z"],
+                    SMOKE["dt"], pusher="boris")
+    for idx, (name, c, m, n, nl, nrt, t) in enumerate(SMOKE["species"]):
+        ref.add_species_upstream_init(name, c, m, n, nl, nrt, t)
+        s = ref.species(idx)
+        w = recover_weights(s["q"], s["m"], c * 1.6e-19, m * 9.1e-31)
+        assert not np.isnan(w).any()
+        orc.add_species(c, m, s["r"], s["z"], s["vr"], s["vphi"], s["vz"], w)
+    b = SMOKE["beam"]
+    orc.add_bunch(b["charge_e"], b["mass_me"], b["number_macro"],
+                  b["bunch_length"] / b["velocity"], b["radius"], b["density"], b["velocity"],
+                  0, b["bunches_distance"] / b["velocity"])
+    assert _run_to_frame(orc, 4) == 21
+    for comp in FIELDS:
+        r0, z0, r1, z1 = g[comp + "__box"]
+        ok = golden_match(orc.field(comp)[r0:r1, z0:z1], g[comp])
+        assert ok.all(), (comp, int((~ok).sum()))
+    r0, z0, r1, z1 = g["rho_beam__box"]
+    ok = golden_match(orc.charge_density(mask=1 << 2)[r0:r1, z0:z1], g["rho_beam"])
+    assert ok.all()
+
+
+def _bitwise(ref, orc, n_species):
+    for c in GRIDS:
+        a, b = ref.field(c), orc.field(c)
+        assert np.array_equal(a, b), (c, int((a != b).sum()))
+    for i in range(n_species):
+        sr, so = ref.species(i), orc.species(i)
+        for k in ("r", "z", "vr", "vphi", "vz", "alive"):
+            assert np.array_equal(sr[k], so[k]), (i, k, int((sr[k] != so[k]).sum()))
+
+
+@needs_ref
+@pytest.mark.parametrize("pusher,refpusher", [("boris", "boris"), ("vay", "vay"),
+                                              ("boris", "adaptive")])
+def test_oracle_bitwise_equals_reference_small(pusher, refpusher):
+    wl = W.small_config(beam=True, steps=12)
+    ref = ref_from_workload(wl, pusher=refpusher)
+    orc = oracle_from_workload(wl, pusher=pusher)
+    seed_fields([ref, orc], (wl.n_grid_r, wl.n_grid_z))
+    for _ in range(12):
+        assert ref.step() == orc.step()
+    _bitwise(ref, orc, ref.n_species())
+    assert orc.species(2)["alive"].sum() > 0
+
+
+@needs_ref
+def test_oracle_bitwise_equals_reference_thermal_64x256():
+    wl = W.thermal_config(steps=3)
+    ref = ref_from_workload(wl)
+    orc = oracle_from_workload(wl)
+    seed_fields([ref, orc], (wl.n_grid_r, wl.n_grid_z))
+    for _ in range(3):
+        ref.step()
+        orc.step()
+    _bitwise(ref, orc, 2)
+
+
+def test_oracle_absorbing_layer_profile():
+    """set_pml with 10-cell layers gives floor(n*l) = 10 cells and a
+    quadratic ramp from sigma_1 to sigma_2 (src/geometry.cpp:56-107)."""
+    wl = W.thermal_config(steps=1)
+    orc = OracleSim(wl.r_size, wl.z_size, wl.n_grid_r, wl.n_grid_z, wl.dt, pml=wl.pml)
+    sig = orc.field("sigma")
+    mid = wl.n_grid_r // 2
+    assert sig[mid, 0] == pytest.approx(7e-2)
+    assert sig[mid, wl.n_grid_z // 2] == 0.0
+    assert (sig[mid, :10] > 0).all() and sig[mid, 10] == 0.0
+    assert sig[mid, -1] > 0
+
+
+def test_random_reverse_sequence():
+    # van der Corput digit reversal (src/math/rand.cpp:40-53)
+    assert random_reverse(0, 9) == 0.0
+    assert random_reverse(1, 2) == 0.5
+    assert random_reverse(3, 2) == 0.75
+    assert random_reverse(5, 11) == pytest.approx(5 / 11)
+    assert random_reverse(12, 11) == pytest.approx(1 / 11 + 1 / 121)
+
+
+def test_oracle_neutral_start_and_determinism():
+    wl = W.small_config(steps=5)
+    a, b = oracle_from_workload(wl), oracle_from_workload(wl)
+    assert np.abs(a.charge_density()).max() < 1e-12 * np.abs(a.charge_density(mask=1)).max()
+    a.run(5)
+    b.run(5)
+    for c in GRIDS:
+        assert np.array_equal(a.field(c), b.field(c))
+    assert a.errors == 0
