@@ -1,0 +1,418 @@
+"""Benchmark of the PDP3 per-timestep PIC loop on B200.
+
+    python bench.py [--gpus N] [--steps K] [--warmup W] [--impl ours|reference]
+                    [--precision fp64|fp32] [--workload wake|thermal]
+
+Workload (default): the beam-plasma wake case, 256 x 2048 cells over
+r in [0, 0.1] m, z in [0, 0.8] m, electrons and protons at 64 macroparticles
+per cell and 1e17 m^-3 (67,108,864 plasma particles), 1 eV electrons, a
+gamma = 5 electron bunch (r 5 mm, length 2 cm, 5e16 m^-3, 64 macroparticles
+per bunch cell) injected at z = 0, 10-cell absorbing layer, Courant 0.5,
+relativistic Boris.  Seeded synthetic inputs (no dataset is involved).
+
+A "step" is one full pass of the loop body: bunch injection, H update, J
+clear, push + deposition of every species, E update.  value is
+particle-steps/s (alive macroparticles x steps / s) over all ranks, with the
+state resident in HBM.  Multi-GPU runs are independent replicas (the path
+does not shard: no collective in the data path).  Particle arrays (~3 GB)
+are far larger than L2, so no L2 flush is needed between steps.
+
+--impl reference times the upstream OpenMP CPU step (oracle/_ref, the
+unmodified upstream sources) on a bounded sample of the same workload.
+"""
+import argparse
+import json
+import math
+import os
+import statistics
+import subprocess
+import sys
+import threading
+import time
+
+import numpy as np
+
+ROOT = os.path.dirname(os.path.abspath(__file__))
+if ROOT not in sys.path:
+    sys.path.insert(0, ROOT)
+
+METRIC = "particle-steps/s & cell-updates/s: FP32 vs FP64 GPU form at fixed Gauss error"
+UNIT = "particle-steps/s"
+BYTES_PER_PARTICLE = {"fp64": 88, "fp32": 52}
+PEAKS_FALLBACK = {"hbm_gbs": 6650.0}
+
+
+def load_peaks():
+    try:
+        with open(os.path.join(ROOT, "MEASURED_PEAKS.json")) as f:
+            return json.load(f), "measured"
+    except Exception:
+        return dict(PEAKS_FALLBACK), "fallback"
+
+
+class ClockSampler:
+    """nvidia-smi sampling of SM clocks and throttle reasons during the timed region."""
+
+    QUERY = ("index,clocks.sm,clocks.max.sm,power.draw,clocks_event_reasons.active,"
+             "clocks_event_reasons.hw_slowdown,clocks_event_reasons.hw_thermal_slowdown,"
+             "clocks_event_reasons.sw_thermal_slowdown,clocks_event_reasons.sw_power_cap")
+
+    def __init__(self, index):
+        self.index = index
+        self.proc = None
+        self.lines = []
+
+    def start(self):
+        try:
+            self.proc = subprocess.Popen(
+                ["nvidia-smi", "-i", str(self.index), "--query-gpu=" + self.QUERY,
+                 "--format=csv,noheader,nounits", "-lms", "100"],
+                stdout=subprocess.PIPE, stderr=subprocess.DEVNULL, text=True)
+            self.thread = threading.Thread(target=self._read, daemon=True)
+            self.thread.start()
+        except Exception:
+            self.proc = None
+
+    def _read(self):
+        for line in self.proc.stdout:
+            self.lines.append(line.strip())
+
+    def stop(self):
+        if self.proc is None:
+            return {"sm_mhz": None, "sm_max_mhz": None, "reasons": ["nvidia-smi unavailable"]}
+        time.sleep(0.25)
+        self.proc.terminate()
+        try:
+            self.proc.wait(timeout=5)
+        except Exception:
+            self.proc.kill()
+        sm, smax, reasons = [], None, set()
+        names = ["hw_slowdown", "hw_thermal_slowdown", "sw_thermal_slowdown", "sw_power_cap"]
+        for ln in self.lines:
+            parts = [p.strip() for p in ln.split(",")]
+            if len(parts) < 9:
+                continue
+            try:
+                sm.append(float(parts[1]))
+                smax = float(parts[2])
+            except ValueError:
+                continue
+            for nm, v in zip(names, parts[5:9]):
+                if v.lower() == "active":
+                    reasons.add(nm)
+        return {"sm_mhz": statistics.median(sm) if sm else None, "sm_max_mhz": smax,
+                "reasons": sorted(reasons), "samples": len(sm)}
+
+
+def make_workload(name, seed, ppc=None):
+    from pdp3_b200 import workloads as W
+    if name == "wake":
+        return W.wake_config(seed=seed, steps=1000, ppc=ppc or 64)
+    if name == "thermal":
+        return W.thermal_config(seed=seed, steps=200, ppc=ppc or 32)
+    raise ValueError(name)
+
+
+def species_bytes(sim, wl, precision):
+    """Algorithmic bytes of one pass of the particle phase."""
+    b = BYTES_PER_PARTICLE[precision]
+    total = 0
+    for s in wl.species:
+        total += s.n * b
+    if wl.beam is not None:
+        n_b = wl.beam.number_macro * wl.beam.number_bunches
+        total += n_b * 1  # alive flags read for every bunch slot
+    return total
+
+
+def alive_count(sim, wl):
+    n = sum(s.n for s in wl.species)
+    for sid in range(len(wl.species), len(wl.species) +
+                     (wl.beam.number_bunches if wl.beam is not None else 0)):
+        n += int(sim.species(sid)["alive"].sum())
+    return n
+
+
+# ------------------------------------------------------------ CPU reference
+
+
+def cpu_sample_run(wl, steps, warmup, fraction, threads):
+    """Times the upstream CPU step (oracle/_ref) or, if it is not built, the
+    oracle restatement, on the workload's grid with `fraction` of its plasma
+    particles (a seeded subset) and the full bunch.  Returns (rate, kind,
+    cores, sample text)."""
+    from oracle import refsim
+    rng = np.random.default_rng(12345)
+    sub = []
+    for s in wl.species:
+        k = max(1, int(s.n * fraction))
+        idx = np.sort(rng.choice(s.n, size=k, replace=False))
+        sub.append((s, idx))
+    if refsim.available(wl.pusher if wl.pusher != "boris_classic" else "boris"):
+        kind = "reference"
+        sim = refsim.RefSim(wl.r_size, wl.z_size, wl.n_grid_r, wl.n_grid_z, wl.dt, end_time=1.0,
+                            pml=wl.pml, pusher=wl.pusher)
+        sim.L.ref_set_threads(threads)
+        for s, idx in sub:
+            sim.add_species(s.name, s.charge_e, s.mass_me, s.r[idx], s.z[idx], s.vr[idx],
+                            s.vphi[idx], s.vz[idx], s.w[idx])
+        if wl.beam is not None:
+            b = wl.beam
+            sim.set_beam(b.charge_e, b.mass_me, b.number_macro, b.bunch_length, b.radius,
+                         b.density, b.velocity, b.number_bunches, b.bunches_distance)
+        if warmup:
+            sim.run(warmup)
+        secs = sim.run(steps)
+        n_alive = sum(len(idx) for _, idx in sub)
+        if wl.beam is not None:
+            for sid in range(len(sub), sim.n_species()):
+                n_alive += int(sim.species(sid)["alive"].sum())
+    else:
+        kind = "port"
+        from oracle.oracle import OracleSim
+        os.environ["OMP_NUM_THREADS"] = str(threads)
+        sim = OracleSim(wl.r_size, wl.z_size, wl.n_grid_r, wl.n_grid_z, wl.dt, pml=wl.pml,
+                        pusher=wl.pusher)
+        for s, idx in sub:
+            sim.add_species(s.charge_e, s.mass_me, s.r[idx], s.z[idx], s.vr[idx], s.vphi[idx],
+                            s.vz[idx], s.w[idx])
+        if wl.beam is not None:
+            b = wl.beam
+            sim.add_bunch(b.charge_e, b.mass_me, b.number_macro, b.bunch_length / b.velocity,
+                          b.radius, b.density, b.velocity, 0, b.bunches_distance / b.velocity)
+        sim.run(warmup)
+        t0 = time.perf_counter()
+        sim.run(steps)
+        secs = time.perf_counter() - t0
+        n_alive = sum(len(idx) for _, idx in sub)
+    rate = n_alive * steps / secs
+    sample = ("%s grid (%dx%d nodes), %.4g of the plasma particles (%d) + bunch, %d steps "
+              "after %d warm-up, %d OpenMP threads" % (wl.name, wl.n_grid_r, wl.n_grid_z,
+                                                       fraction, sum(len(i) for _, i in sub),
+                                                       steps, warmup, threads))
+    return rate, kind, threads, sample, secs
+
+
+def run_reference(args, rank, world):
+    if rank != 0:
+        return 0
+    wl = make_workload(args.workload, 1002, args.ppc)
+    threads = os.cpu_count() or 1
+    fraction = args.cpu_fraction
+    steps = max(1, args.steps)
+    rate, kind, cores, sample, secs = cpu_sample_run(wl, steps, args.warmup, fraction, threads)
+    line = {
+        "metric": METRIC, "value": rate, "unit": UNIT, "impl": "reference", "n_gpus": 0,
+        "steps": steps, "warmup": args.warmup, "ms_per_step": 1000.0 * secs / steps,
+        "higher_is_better": True, "scaling": "weak", "vs_baseline": None, "dtype": "f64",
+        "data": "synthetic (seeded)",
+        "config": {"workload": wl.name, "n_grid_r": wl.n_grid_r, "n_grid_z": wl.n_grid_z,
+                   "particles": wl.n_particles, "pusher": wl.pusher, "sample": sample},
+        "cpu_baseline": {"value": rate, "unit": UNIT, "cores": cores, "kind": kind,
+                         "sample": sample},
+        "e2e": {"value": rate, "unit": UNIT, "h2d_bytes_per_step": 0, "d2h_bytes_per_step": 0},
+    }
+    print(json.dumps(line), flush=True)
+    return 0
+
+
+# ------------------------------------------------------------ GPU run
+
+
+def main():
+    ap = argparse.ArgumentParser()
+    ap.add_argument("--gpus", type=int, default=1)
+    ap.add_argument("--steps", type=int, default=20)
+    ap.add_argument("--warmup", type=int, default=3)
+    ap.add_argument("--impl", default="ours", choices=["ours", "reference"])
+    ap.add_argument("--precision", default="fp64", choices=["fp64", "fp32"])
+    ap.add_argument("--workload", default="wake", choices=["wake", "thermal"])
+    ap.add_argument("--ppc", type=int, default=None,
+                    help="macroparticles per cell (profiling runs on a smaller case)")
+    ap.add_argument("--e2e-steps", type=int, default=3)
+    ap.add_argument("--cpu-fraction", type=float, default=1.0 / 32)
+    ap.add_argument("--cpu-steps", type=int, default=3)
+    ap.add_argument("--no-cpu-baseline", action="store_true")
+    args = ap.parse_args()
+
+    world = int(os.environ.get("WORLD_SIZE", "1"))
+    rank = int(os.environ.get("RANK", "0"))
+    local_rank = int(os.environ.get("LOCAL_RANK", "0"))
+
+    if args.impl == "reference":
+        return run_reference(args, rank, world)
+
+    import torch
+    dist = None
+    if world > 1:
+        import datetime
+        import torch.distributed as dist
+        torch.cuda.set_device(local_rank)
+        dist.init_process_group("nccl", timeout=datetime.timedelta(seconds=300),
+                                device_id=torch.device("cuda", local_rank))
+    from pdp3_b200 import api
+
+    assert args.warmup >= 3, "at least 3 warm-up steps"
+    wl = make_workload(args.workload, 1002, args.ppc)
+    sim = api.from_workload(wl, precision=args.precision, device=local_rank)
+    stream = torch.cuda.ExternalStream(sim.stream_ptr, device=torch.device("cuda", local_rank))
+
+    sim.step(args.warmup)
+    sim.sync()
+    if dist is not None:
+        dist.barrier()
+    torch.cuda.synchronize()
+    alive0 = alive_count(sim, wl)
+    sim.reset_timing()
+    sim.set_timing(True)
+    clocks = ClockSampler(local_rank)
+    clocks.start()
+    time.sleep(0.3)
+    ev0 = torch.cuda.Event(enable_timing=True)
+    ev1 = torch.cuda.Event(enable_timing=True)
+    ev0.record(stream)
+    sim.step(args.steps)
+    ev1.record(stream)
+    sim.sync()
+    torch.cuda.synchronize()
+    clk = clocks.stop()
+    ms = ev0.elapsed_time(ev1)
+    tm = sim.timing()
+    sim.set_timing(False)
+    alive1 = alive_count(sim, wl)
+    particle_steps = 0.5 * (alive0 + alive1) * args.steps
+
+    if dist is not None:
+        t = torch.tensor([ms, particle_steps], dtype=torch.float64, device="cuda")
+        mx = t.clone()
+        dist.all_reduce(mx, op=dist.ReduceOp.MAX)
+        dist.all_reduce(t, op=dist.ReduceOp.SUM)
+        ms_max = float(mx[0])
+        total_ps = float(t[1])
+    else:
+        ms_max = ms
+        total_ps = particle_steps
+    value = total_ps / (ms_max / 1000.0)
+
+    # roofline of the dominant kernel (the fused push + deposition)
+    peaks, peak_src = load_peaks()
+    bytes_particle_phase = species_bytes(sim, wl, args.precision)
+    ms_part = tm["ms_particles"] / max(tm["steps"], 1)
+    achieved = bytes_particle_phase / (ms_part / 1000.0) / 1e9
+    n_nodes = wl.n_grid_r * wl.n_grid_z
+    ms_fields = tm["ms_fields"] / max(tm["steps"], 1)
+
+    # end to end through the public API from pinned host buffers: every step
+    # uploads the particle state, steps, and reads the state and E_z back.
+    e2e = None
+    if args.e2e_steps > 0:
+        e2e = run_e2e(sim, wl, torch, stream, args.e2e_steps)
+
+    cpu = None
+    if rank == 0 and world == 1 and not args.no_cpu_baseline:
+        try:
+            rate, kind, cores, sample, _ = cpu_sample_run(
+                wl, args.cpu_steps, 1, args.cpu_fraction, os.cpu_count() or 1)
+            cpu = {"value": rate, "unit": UNIT, "cores": cores, "kind": kind, "sample": sample}
+        except Exception as exc:  # reported, not fatal
+            cpu = {"value": None, "unit": UNIT, "cores": None, "kind": None,
+                   "sample": "failed: %s" % exc}
+
+    traffic = load_traffic(args.workload, args.precision, bytes_particle_phase)
+    if rank == 0:
+        line = {
+            "metric": METRIC, "value": value, "unit": UNIT, "n_gpus": world,
+            "steps": args.steps, "warmup": args.warmup, "ms_per_step": ms_max / args.steps,
+            "higher_is_better": True, "scaling": "weak", "vs_baseline": None,
+            "dtype": "f64" if args.precision == "fp64" else "f32+f64acc",
+            "data": "synthetic (seeded)",
+            "config": {"workload": wl.name, "n_grid_r": wl.n_grid_r, "n_grid_z": wl.n_grid_z,
+                       "particles": wl.n_particles, "pusher": wl.pusher,
+                       "precision": args.precision, "parallelism": "replicas x%d" % world,
+                       "l2": "inputs larger than L2 (particle state %.2f GB)"
+                             % (bytes_particle_phase / 1e9)},
+            "cell_updates_per_s": n_nodes / (ms_fields / 1000.0) if ms_fields > 0 else None,
+            "cell_updates_per_s_step": n_nodes * args.steps * world / (ms_max / 1000.0),
+            "kernel_ms": {"particles": ms_part, "fields": ms_fields,
+                          "other": tm["ms_other"] / max(tm["steps"], 1)},
+            "roofline": {"bound": "hbm", "achieved": achieved, "peak": peaks.get("hbm_gbs"),
+                         "unit": "GB/s", "frac": achieved / peaks.get("hbm_gbs"),
+                         "traffic": traffic, "kernel": "push_deposit (all species)",
+                         "peak_source": peak_src,
+                         "algorithmic_bytes_per_launch": bytes_particle_phase},
+            "e2e": e2e,
+            "cpu_baseline": cpu,
+            "gpu_launches": tm["launches"],
+            "clocks": clk,
+        }
+        print(json.dumps(line), flush=True)
+    sim.close()
+    if dist is not None:
+        dist.barrier()
+        dist.destroy_process_group()
+    return 0
+
+
+def load_traffic(workload, precision, algorithmic):
+    """DRAM traffic per launch of the particle phase from a committed ncu
+    summary (profiles/*.json), or None when none exists."""
+    path = os.path.join(ROOT, "profiles", "traffic_%s_%s.json" % (workload, precision))
+    try:
+        with open(path) as f:
+            return json.load(f)["bytes_per_launch"]
+    except Exception:
+        return None
+
+
+def run_e2e(sim, wl, torch, stream, steps):
+    """Same metric through the public C-ABI with host buffers: each step
+    copies every species' state host->device from pinned memory, runs one
+    step and copies the state and the E_z grid back."""
+    n_sp = len(wl.species) + (wl.beam.number_bunches if wl.beam is not None else 0)
+    bufs = []
+    for sid in range(n_sp):
+        n = sim.species_size(sid)
+        arrs = {k: torch.empty(n, dtype=torch.float64, pin_memory=True).numpy()
+                for k in ("r", "z", "vr", "vphi", "vz")}
+        alive = torch.empty(n, dtype=torch.uint8, pin_memory=True).numpy()
+        st = sim.species(sid)
+        for k in arrs:
+            arrs[k][:] = st[k]
+        alive[:] = st["alive"]
+        bufs.append((sid, arrs, alive, st["w"]))
+    ez = torch.empty(wl.n_grid_r * wl.n_grid_z, dtype=torch.float64, pin_memory=True).numpy()
+    import ctypes
+    from pdp3_b200.api import _U8
+    h2d = d2h = 0
+    for sid, arrs, alive, _ in bufs:
+        h2d += sum(a.nbytes for a in arrs.values()) + (alive.nbytes if sid >= len(wl.species)
+                                                       else 0)
+    d2h = h2d + ez.nbytes
+    sim.sync()
+    torch.cuda.synchronize()
+    t0 = time.perf_counter()
+    alive_total = 0
+    for _ in range(steps):
+        for sid, arrs, alive, _w in bufs:
+            sim.set_species(sid, r=arrs["r"], z=arrs["z"], vr=arrs["vr"], vphi=arrs["vphi"],
+                            vz=arrs["vz"], alive=alive if sid >= len(wl.species) else None)
+        sim.step(1)
+        for sid, arrs, alive, _w in bufs:
+            P = ctypes.POINTER(ctypes.c_double)
+            st = sim.L.pdp3g_get_species(
+                sim.h, sid, *[arrs[k].ctypes.data_as(P) for k in ("r", "z", "vr", "vphi", "vz")],
+                None, alive.ctypes.data_as(_U8))
+            sim._check(st, "get_species")
+        sim._check(sim.L.pdp3g_get_field(sim.h, 2, ez.ctypes.data_as(
+            ctypes.POINTER(ctypes.c_double))), "get_field")
+        alive_total += sum(len(a["r"]) if sid < len(wl.species) else int(al.sum())
+                           for sid, a, al, _ in bufs)
+    secs = time.perf_counter() - t0
+    return {"value": alive_total / secs, "unit": UNIT, "h2d_bytes_per_step": h2d,
+            "d2h_bytes_per_step": d2h, "steps": steps,
+            "note": "per step: full particle state H2D from pinned memory, one step, "
+                    "state + E_z D2H, through the C ABI"}
+
+
+if __name__ == "__main__":
+    sys.exit(main())

@@ -1,0 +1,175 @@
+/*
+ * pdp3g: B200 (sm_100a) implementation of the PDP3 per-timestep
+ * particle-in-cell loop, behind a plain C ABI.
+ *
+ * The upstream code has no plugin or FFI layer; its seam is a set of C++
+ * classes driven by LoadInitParam::run (src/loadInitParam.cpp:471-587).
+ * Each entry point below names the upstream interface it stands in for.
+ * The library owns all device memory; host pointers are borrowed for the
+ * duration of a call.  Calls on one context are not thread-safe; separate
+ * contexts may be used from separate threads.  No entry point calls exit():
+ * every failure is a status code (upstream: exit(1) / exit(78) / abort()).
+ *
+ * Units are SI with the upstream constants (include/constant.h:10-27).
+ * Grids are [n_grid_r][n_grid_z] row-major doubles (upstream: double** rows,
+ * src/field.cpp:10-25).  Particles are given as structure-of-arrays.
+ */
+#ifndef PDP3G_H
+#define PDP3G_H
+
+#include <stdint.h>
+
+#ifdef __cplusplus
+extern "C" {
+#endif
+
+typedef enum {
+  PDP3G_OK = 0,
+  PDP3G_INVALID_ARG = 1,
+  PDP3G_CUDA_ERROR = 2,
+  PDP3G_NAN_DETECTED = 3,   /* upstream: exit(1), src/particles.cpp:1046-1053 */
+  PDP3G_V_GE_C = 4,         /* upstream: exit(1), src/lib.cpp:54-59 */
+  PDP3G_OUT_OF_GRID = 5,    /* a particle reached a cell outside the grid */
+  PDP3G_TIMEOUT = 6,
+  PDP3G_NOT_SUPPORTED = 7,
+  PDP3G_NO_MEMORY = 8
+} pdp3g_status;
+
+typedef enum {
+  PDP3G_PUSHER_BORIS = 0,         /* relativistic Boris (PUSHER_BORIS_RELATIVISTIC; also
+                                     what the default adaptive build computes at -O2) */
+  PDP3G_PUSHER_VAY = 1,           /* PUSHER_VAY, src/particles.cpp:1152-1254 */
+  PDP3G_PUSHER_BORIS_CLASSIC = 2  /* PUSHER_BORIS_CLASSIC */
+} pdp3g_pusher;
+
+typedef enum {
+  PDP3G_FP64 = 0,       /* plain form: FP64 throughout, upstream operation order */
+  PDP3G_FP32_CELL = 1   /* int cell + FP32 offset/momentum, FP64 grid accumulation */
+} pdp3g_precision;
+
+/* grid components (upstream public members, include/eField.h, hField.h, current.h) */
+typedef enum {
+  PDP3G_E_R = 0, PDP3G_E_PHI, PDP3G_E_Z,
+  PDP3G_H_R, PDP3G_H_PHI, PDP3G_H_Z,
+  PDP3G_H_R_HALF, PDP3G_H_PHI_HALF, PDP3G_H_Z_HALF,
+  PDP3G_J_R, PDP3G_J_PHI, PDP3G_J_Z,
+  PDP3G_SIGMA,
+  PDP3G_NCOMP
+} pdp3g_comp;
+
+typedef struct {
+  /* Geometry(r_size, z_size, n_grid_r, n_grid_z), src/geometry.cpp:8-31 */
+  double r_size, z_size;
+  int32_t n_grid_r, n_grid_z;
+  /* Time(current_time, ..., delta_t), src/pdp3Time.cpp:11-18 */
+  double dt, current_time;
+  /* Geometry::set_pml(l1, l2, l3, sigma1, sigma2), src/geometry.cpp:56-107;
+     applied only when one of l1..l3 is non-zero (src/parameters.cpp:244-245) */
+  double pml_l1, pml_l2, pml_l3, pml_sigma1, pml_sigma2;
+  int32_t pusher;       /* pdp3g_pusher */
+  int32_t precision;    /* pdp3g_precision */
+  int32_t device;       /* CUDA device ordinal */
+  int32_t sort_interval;/* particles re-sorted by cell every N steps (0: never) */
+} pdp3g_config;
+
+/* FP64 reductions over the current state (no upstream counterpart; the
+   upstream code prints no energy or residual diagnostics). */
+typedef struct {
+  double field_energy;      /* 1/2 sum (eps0 E^2 + mu0 H^2) dV over node volumes */
+  double kinetic_energy;    /* sum m_i c^2 (gamma_i - 1) over alive particles */
+  double gauss_residual;    /* ||eps0 div E - (rho - rho_0)||_2, interior, sigma == 0 */
+  double gauss_norm;        /* ||rho - rho_0||_2 over the same nodes */
+  double charge_total;      /* sum rho dV */
+  int64_t alive;            /* alive macroparticles */
+} pdp3g_diag;
+
+typedef struct {
+  double ms_step_total;     /* device time of all launches, summed */
+  double ms_particles;      /* push + deposition kernels */
+  double ms_fields;         /* Yee H and E kernels */
+  double ms_sort;           /* counting sort */
+  double ms_other;          /* injection, clears */
+  int64_t launches;         /* kernels launched since the last reset */
+  int64_t particle_launches;
+  int64_t steps;
+  int64_t particle_steps;   /* alive macroparticles pushed, summed over steps */
+} pdp3g_timing;
+
+typedef struct pdp3g_ctx pdp3g_ctx;
+
+/* Geometry + Time + EField/HField/Current construction and
+   LoadInitParam::init_fields (src/loadInitParam.cpp:250-260): all grids 0. */
+pdp3g_status pdp3g_create(const pdp3g_config *cfg, pdp3g_ctx **out);
+void pdp3g_destroy(pdp3g_ctx *ctx);
+
+/* Particles(name, charge_e, mass_me, n, geom) with its public pos/vel arrays
+   filled (include/particles.h:34-100): charge_array = charge_e*e*w,
+   mass_array = mass_me*m_e*w (src/particles.cpp:328-329).  alive may be NULL
+   (all alive).  *id receives the species index (ParticlesList order). */
+pdp3g_status pdp3g_add_species(pdp3g_ctx *ctx, double charge_e, double mass_me, int64_t n,
+                               const double *r, const double *z, const double *vr,
+                               const double *vphi, const double *vz, const double *w,
+                               const uint8_t *alive, int32_t *id);
+
+/* Bunch(name, charge, mass, n, geom, duration, radius, density, velocity,
+   bunch_number, hole_duration), src/bunch.cpp:6-80 (TESTMODE radial
+   sequence), injected progressively by Bunch::bunch_inject
+   (src/bunch.cpp:87-124) at the start of each step. */
+pdp3g_status pdp3g_add_bunch(pdp3g_ctx *ctx, double charge_e, double mass_me, int64_t n,
+                             double duration, double radius, double density, double velocity,
+                             int32_t bunch_number, double hole_duration, int32_t *id);
+
+/* nsteps passes of the LoadInitParam::run loop body (src/loadInitParam.cpp:
+   481-527, 586): bunch injection, HField::calc_field, Current::reset_j,
+   ParticlesList::step_v + full_current_distribution, EField::calc_field,
+   t += dt.  Asynchronous on the context's stream. */
+pdp3g_status pdp3g_step(pdp3g_ctx *ctx, int32_t nsteps);
+
+/* Waits for the stream and reports device-side error flags. */
+pdp3g_status pdp3g_sync(pdp3g_ctx *ctx);
+
+/* EField/HField public arrays and Current::get_j_* (src/current.cpp:88-102):
+   copies one component into host memory [n_grid_r*n_grid_z]. */
+pdp3g_status pdp3g_get_field(pdp3g_ctx *ctx, int32_t comp, double *host_out);
+pdp3g_status pdp3g_set_field(pdp3g_ctx *ctx, int32_t comp, const double *host_in);
+
+/* Particles public state (pos[i][0], pos[i][2], vel[i][0..2], is_alive);
+   any pointer may be NULL. */
+pdp3g_status pdp3g_get_species(pdp3g_ctx *ctx, int32_t id, double *r, double *z, double *vr,
+                               double *vphi, double *vz, double *w, uint8_t *alive);
+pdp3g_status pdp3g_set_species(pdp3g_ctx *ctx, int32_t id, const double *r, const double *z,
+                               const double *vr, const double *vphi, const double *vz,
+                               const uint8_t *alive);
+int64_t pdp3g_species_size(pdp3g_ctx *ctx, int32_t id);
+
+/* ParticlesList::charge_weighting / Particles::charge_weighting
+   (src/particlesList.cpp:14-18, src/particles.cpp:101-226) of the species in
+   species_mask (bit s = species s) into a fresh grid, copied to host. */
+pdp3g_status pdp3g_charge_density(pdp3g_ctx *ctx, uint32_t species_mask, double *host_out);
+
+/* Records rho_0 for the Gauss residual (call after adding species). */
+pdp3g_status pdp3g_mark_initial_charge(pdp3g_ctx *ctx);
+pdp3g_status pdp3g_diagnostics(pdp3g_ctx *ctx, pdp3g_diag *out);
+
+/* Per-kernel device timing with CUDA events on the context's stream. */
+pdp3g_status pdp3g_set_timing(pdp3g_ctx *ctx, int32_t enabled);
+pdp3g_status pdp3g_get_timing(pdp3g_ctx *ctx, pdp3g_timing *out);
+pdp3g_status pdp3g_reset_timing(pdp3g_ctx *ctx);
+
+/* The CUDA stream (cudaStream_t) every launch of this context goes to, so a
+   caller can order its own work or CUDA events against the step. */
+void *pdp3g_stream(pdp3g_ctx *ctx);
+
+/* Time::current_time */
+double pdp3g_current_time(pdp3g_ctx *ctx);
+/* device memory held by the context, bytes */
+int64_t pdp3g_device_bytes(pdp3g_ctx *ctx);
+const char *pdp3g_status_string(pdp3g_status st);
+const char *pdp3g_last_error(pdp3g_ctx *ctx);
+/* 1 when a CUDA device is usable from this process */
+int32_t pdp3g_device_available(void);
+
+#ifdef __cplusplus
+}
+#endif
+#endif

@@ -1,0 +1,260 @@
+"""ctypes binding of libpdp3g.so (the C ABI declared in include/pdp3g.h).
+
+This module never falls back to a CPU path: if the CUDA library is missing
+or no device is usable, constructing a Simulation raises.
+"""
+import ctypes
+import os
+
+import numpy as np
+
+HERE = os.path.dirname(os.path.abspath(__file__))
+LIB_PATH = os.path.join(HERE, "libpdp3g.so")
+
+E_R, E_PHI, E_Z, H_R, H_PHI, H_Z, H_R_HALF, H_PHI_HALF, H_Z_HALF, J_R, J_PHI, J_Z, SIGMA = \
+    range(13)
+COMP = {"E_r": E_R, "E_phi": E_PHI, "E_z": E_Z, "H_r": H_R, "H_phi": H_PHI, "H_z": H_Z,
+        "H_r_half": H_R_HALF, "H_phi_half": H_PHI_HALF, "H_z_half": H_Z_HALF,
+        "J_r": J_R, "J_phi": J_PHI, "J_z": J_Z, "sigma": SIGMA}
+PUSHERS = {"boris": 0, "vay": 1, "boris_classic": 2}
+PRECISIONS = {"fp64": 0, "fp32": 1}
+STATUS = {0: "ok", 1: "invalid argument", 2: "CUDA error", 3: "NaN position",
+          4: "velocity >= c", 5: "particle outside the grid", 6: "timeout",
+          7: "not supported", 8: "out of device memory"}
+
+
+class Pdp3gError(RuntimeError):
+    def __init__(self, status, msg):
+        super().__init__("pdp3g status %d (%s): %s" % (status, STATUS.get(status, "?"), msg))
+        self.status = status
+
+
+class Config(ctypes.Structure):
+    _fields_ = [("r_size", ctypes.c_double), ("z_size", ctypes.c_double),
+                ("n_grid_r", ctypes.c_int32), ("n_grid_z", ctypes.c_int32),
+                ("dt", ctypes.c_double), ("current_time", ctypes.c_double),
+                ("pml_l1", ctypes.c_double), ("pml_l2", ctypes.c_double),
+                ("pml_l3", ctypes.c_double), ("pml_sigma1", ctypes.c_double),
+                ("pml_sigma2", ctypes.c_double),
+                ("pusher", ctypes.c_int32), ("precision", ctypes.c_int32),
+                ("device", ctypes.c_int32), ("sort_interval", ctypes.c_int32)]
+
+
+class Diag(ctypes.Structure):
+    _fields_ = [("field_energy", ctypes.c_double), ("kinetic_energy", ctypes.c_double),
+                ("gauss_residual", ctypes.c_double), ("gauss_norm", ctypes.c_double),
+                ("charge_total", ctypes.c_double), ("alive", ctypes.c_int64)]
+
+
+class Timing(ctypes.Structure):
+    _fields_ = [("ms_step_total", ctypes.c_double), ("ms_particles", ctypes.c_double),
+                ("ms_fields", ctypes.c_double), ("ms_sort", ctypes.c_double),
+                ("ms_other", ctypes.c_double), ("launches", ctypes.c_int64),
+                ("particle_launches", ctypes.c_int64), ("steps", ctypes.c_int64),
+                ("particle_steps", ctypes.c_int64)]
+
+
+_D = ctypes.POINTER(ctypes.c_double)
+_U8 = ctypes.POINTER(ctypes.c_uint8)
+_VP = ctypes.c_void_p
+_I32 = ctypes.c_int32
+_lib = None
+
+EXPORTS = [
+    ("pdp3g_create", _I32, [ctypes.POINTER(Config), ctypes.POINTER(_VP)]),
+    ("pdp3g_destroy", None, [_VP]),
+    ("pdp3g_add_species", _I32, [_VP, ctypes.c_double, ctypes.c_double, ctypes.c_int64] +
+     [_D] * 6 + [_U8, ctypes.POINTER(_I32)]),
+    ("pdp3g_add_bunch", _I32, [_VP, ctypes.c_double, ctypes.c_double, ctypes.c_int64,
+                               ctypes.c_double, ctypes.c_double, ctypes.c_double,
+                               ctypes.c_double, _I32, ctypes.c_double, ctypes.POINTER(_I32)]),
+    ("pdp3g_step", _I32, [_VP, _I32]),
+    ("pdp3g_sync", _I32, [_VP]),
+    ("pdp3g_get_field", _I32, [_VP, _I32, _D]),
+    ("pdp3g_set_field", _I32, [_VP, _I32, _D]),
+    ("pdp3g_get_species", _I32, [_VP, _I32] + [_D] * 6 + [_U8]),
+    ("pdp3g_set_species", _I32, [_VP, _I32] + [_D] * 5 + [_U8]),
+    ("pdp3g_species_size", ctypes.c_int64, [_VP, _I32]),
+    ("pdp3g_charge_density", _I32, [_VP, ctypes.c_uint32, _D]),
+    ("pdp3g_mark_initial_charge", _I32, [_VP]),
+    ("pdp3g_diagnostics", _I32, [_VP, ctypes.POINTER(Diag)]),
+    ("pdp3g_set_timing", _I32, [_VP, _I32]),
+    ("pdp3g_get_timing", _I32, [_VP, ctypes.POINTER(Timing)]),
+    ("pdp3g_reset_timing", _I32, [_VP]),
+    ("pdp3g_current_time", ctypes.c_double, [_VP]),
+    ("pdp3g_stream", _VP, [_VP]),
+    ("pdp3g_device_bytes", ctypes.c_int64, [_VP]),
+    ("pdp3g_status_string", ctypes.c_char_p, [_I32]),
+    ("pdp3g_last_error", ctypes.c_char_p, [_VP]),
+    ("pdp3g_device_available", _I32, []),
+]
+
+
+def load(path=LIB_PATH):
+    """Loads the CUDA library; raises if it has not been built."""
+    global _lib
+    if _lib is not None:
+        return _lib
+    if not os.path.exists(path):
+        raise FileNotFoundError("%s is missing: build it with `python -m pdp3_b200.build` "
+                                "(there is no CPU fallback)" % path)
+    L = ctypes.CDLL(path)
+    for name, res, args in EXPORTS:
+        fn = getattr(L, name)
+        fn.restype = res
+        fn.argtypes = args
+    _lib = L
+    return L
+
+
+def _p(a):
+    return a.ctypes.data_as(_D)
+
+
+def _f64(a):
+    return np.ascontiguousarray(a, dtype=np.float64)
+
+
+class Simulation:
+    """One device-resident PDP3 simulation (grids + species) on a CUDA device."""
+
+    def __init__(self, r_size, z_size, n_grid_r, n_grid_z, dt, current_time=0.0, pml=None,
+                 pusher="boris", precision="fp64", device=0, sort_interval=0):
+        self.L = load()
+        if not self.L.pdp3g_device_available():
+            raise RuntimeError("no CUDA device available to pdp3g")
+        pml = [0.0] * 5 if pml is None else list(pml)
+        cfg = Config(r_size, z_size, n_grid_r, n_grid_z, dt, current_time, pml[0], pml[1],
+                     pml[2], pml[3], pml[4], PUSHERS[pusher], PRECISIONS[precision], device,
+                     sort_interval)
+        h = _VP()
+        st = self.L.pdp3g_create(ctypes.byref(cfg), ctypes.byref(h))
+        if st != 0:
+            raise Pdp3gError(st, "pdp3g_create")
+        self.h = h
+        self.nr, self.nz = n_grid_r, n_grid_z
+
+    def _check(self, st, what):
+        if st != 0:
+            msg = self.L.pdp3g_last_error(self.h)
+            raise Pdp3gError(st, "%s: %s" % (what, msg.decode() if msg else ""))
+
+    def add_species(self, charge_e, mass_me, r, z, vr, vphi, vz, w, alive=None):
+        arrs = [_f64(a) for a in (r, z, vr, vphi, vz, w)]
+        al = None if alive is None else np.ascontiguousarray(alive, dtype=np.uint8)
+        sid = _I32()
+        self._check(self.L.pdp3g_add_species(self.h, charge_e, mass_me, len(arrs[0]),
+                                             *[_p(a) for a in arrs],
+                                             al.ctypes.data_as(_U8) if al is not None else None,
+                                             ctypes.byref(sid)), "add_species")
+        return sid.value
+
+    def add_bunch(self, charge_e, mass_me, n, duration, radius, density, velocity,
+                  bunch_number=0, hole_duration=0.0):
+        sid = _I32()
+        self._check(self.L.pdp3g_add_bunch(self.h, charge_e, mass_me, int(n), duration, radius,
+                                           density, velocity, int(bunch_number), hole_duration,
+                                           ctypes.byref(sid)), "add_bunch")
+        return sid.value
+
+    def step(self, n=1):
+        self._check(self.L.pdp3g_step(self.h, int(n)), "step")
+
+    def sync(self):
+        self._check(self.L.pdp3g_sync(self.h), "sync")
+
+    def status(self):
+        """Status of pdp3g_sync without raising."""
+        return self.L.pdp3g_sync(self.h)
+
+    def field(self, name):
+        out = np.empty(self.nr * self.nz)
+        self._check(self.L.pdp3g_get_field(self.h, COMP[name], _p(out)), "get_field")
+        return out.reshape(self.nr, self.nz)
+
+    def set_field(self, name, arr):
+        a = _f64(arr).reshape(-1)
+        assert a.size == self.nr * self.nz
+        self._check(self.L.pdp3g_set_field(self.h, COMP[name], _p(a)), "set_field")
+
+    def species_size(self, sid):
+        return int(self.L.pdp3g_species_size(self.h, sid))
+
+    def species(self, sid):
+        n = self.species_size(sid)
+        out = {k: np.empty(n) for k in ("r", "z", "vr", "vphi", "vz", "w")}
+        alive = np.empty(n, dtype=np.uint8)
+        self._check(self.L.pdp3g_get_species(self.h, sid, *[_p(out[k]) for k in
+                                                            ("r", "z", "vr", "vphi", "vz", "w")],
+                                             alive.ctypes.data_as(_U8)), "get_species")
+        out["alive"] = alive
+        return out
+
+    def set_species(self, sid, r=None, z=None, vr=None, vphi=None, vz=None, alive=None):
+        keep = [None if a is None else _f64(a) for a in (r, z, vr, vphi, vz)]
+        al = None if alive is None else np.ascontiguousarray(alive, dtype=np.uint8)
+        self._check(self.L.pdp3g_set_species(
+            self.h, sid, *[(_p(a) if a is not None else None) for a in keep],
+            al.ctypes.data_as(_U8) if al is not None else None), "set_species")
+
+    def charge_density(self, mask=0xFFFFFFFF):
+        out = np.empty(self.nr * self.nz)
+        self._check(self.L.pdp3g_charge_density(self.h, mask, _p(out)), "charge_density")
+        return out.reshape(self.nr, self.nz)
+
+    def mark_initial_charge(self):
+        self._check(self.L.pdp3g_mark_initial_charge(self.h), "mark_initial_charge")
+
+    def diagnostics(self):
+        d = Diag()
+        self._check(self.L.pdp3g_diagnostics(self.h, ctypes.byref(d)), "diagnostics")
+        return {f: getattr(d, f) for f, _ in Diag._fields_}
+
+    def set_timing(self, on=True):
+        self._check(self.L.pdp3g_set_timing(self.h, 1 if on else 0), "set_timing")
+
+    def reset_timing(self):
+        self._check(self.L.pdp3g_reset_timing(self.h), "reset_timing")
+
+    def timing(self):
+        t = Timing()
+        self._check(self.L.pdp3g_get_timing(self.h, ctypes.byref(t)), "get_timing")
+        return {f: getattr(t, f) for f, _ in Timing._fields_}
+
+    @property
+    def time(self):
+        return self.L.pdp3g_current_time(self.h)
+
+    @property
+    def stream_ptr(self):
+        return int(self.L.pdp3g_stream(self.h) or 0)
+
+    @property
+    def device_bytes(self):
+        return int(self.L.pdp3g_device_bytes(self.h))
+
+    def close(self):
+        if getattr(self, "h", None):
+            self.L.pdp3g_destroy(self.h)
+            self.h = None
+
+    def __del__(self):
+        try:
+            self.close()
+        except Exception:
+            pass
+
+
+def from_workload(wl, precision="fp64", device=0, pusher=None, sort_interval=0):
+    """Builds a Simulation holding a pdp3_b200.workloads.Workload."""
+    sim = Simulation(wl.r_size, wl.z_size, wl.n_grid_r, wl.n_grid_z, wl.dt, pml=wl.pml,
+                     pusher=pusher or wl.pusher, precision=precision, device=device,
+                     sort_interval=sort_interval)
+    for s in wl.species:
+        sim.add_species(s.charge_e, s.mass_me, s.r, s.z, s.vr, s.vphi, s.vz, s.w)
+    if wl.beam is not None:
+        b = wl.beam
+        for nb in range(b.number_bunches):
+            sim.add_bunch(b.charge_e, b.mass_me, b.number_macro, b.bunch_length / b.velocity,
+                          b.radius, b.density, b.velocity, nb, b.bunches_distance / b.velocity)
+    return sim

@@ -1,0 +1,69 @@
+"""Builds pdp3_b200/libpdp3g.so with nvcc for sm_100a (in-tree, no JIT cache).
+
+Translation units of the FP64 plain form are compiled with --fmad=false so
+that their arithmetic matches the CPU step's operation by operation; the
+FP32 cell-local form keeps fused multiply-add.
+
+    python -m pdp3_b200.build [--force]
+"""
+import os
+import shutil
+import subprocess
+import sys
+
+HERE = os.path.dirname(os.path.abspath(__file__))
+CSRC = os.path.join(HERE, "csrc")
+BUILD = os.path.join(HERE, "_build")
+LIB = os.path.join(HERE, "libpdp3g.so")
+ROOT = os.path.dirname(HERE)
+
+ARCH = ["-gencode", "arch=compute_100a,code=sm_100a"]
+COMMON = ["-O3", "-lineinfo", "-std=c++17", "-Xcompiler", "-fPIC", "--expt-relaxed-constexpr",
+          "-I" + os.path.join(ROOT, "include"), "-I" + CSRC]
+# translation unit -> extra flags
+UNITS = {
+    "capi.cu": [],
+    "fields.cu": ["--fmad=false"],
+    "particles_f64.cu": ["--fmad=false"],
+}
+HEADERS = ["pdp3g_internal.cuh"]
+
+
+def nvcc():
+    for cand in (os.environ.get("NVCC"), "/usr/local/cuda/bin/nvcc", shutil.which("nvcc")):
+        if cand and os.path.exists(cand):
+            return cand
+    raise RuntimeError("nvcc not found")
+
+
+def _newer(src_list, dst):
+    if not os.path.exists(dst):
+        return True
+    t = os.path.getmtime(dst)
+    return any(os.path.getmtime(s) > t for s in src_list)
+
+
+def build(force=False, verbose=False):
+    os.makedirs(BUILD, exist_ok=True)
+    nv = nvcc()
+    hdrs = [os.path.join(CSRC, h) for h in HEADERS] + [os.path.join(ROOT, "include", "pdp3g.h")]
+    objs = []
+    for unit, extra in UNITS.items():
+        src = os.path.join(CSRC, unit)
+        obj = os.path.join(BUILD, unit.replace(".cu", ".o"))
+        objs.append(obj)
+        if force or _newer([src] + hdrs, obj):
+            cmd = [nv] + ARCH + COMMON + extra + ["-c", src, "-o", obj]
+            if verbose:
+                print(" ".join(cmd))
+            subprocess.run(cmd, check=True)
+    if force or _newer(objs, LIB):
+        cmd = [nv] + ARCH + ["-shared", "--cudart", "static", "-o", LIB] + objs
+        if verbose:
+            print(" ".join(cmd))
+        subprocess.run(cmd, check=True)
+    return LIB
+
+
+if __name__ == "__main__":
+    build(force="--force" in sys.argv, verbose=True)

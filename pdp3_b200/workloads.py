@@ -128,6 +128,14 @@ def thermal_plasma(rng, r_size, z_size, n_grid_r, n_grid_z, ppc, density_fn, t_e
     return [el, ion]
 
 
+def absorbing_layer(n_grid_r, n_grid_z, cells, sigma1=1e-5, sigma2=7e-2):
+    """set_pml arguments for a `cells`-cell layer at r_max and both z ends
+    (the upstream code takes floor(n_grid * comparative_l) cells,
+    src/geometry.cpp:60-66; the +0.5 keeps floor() off the integer edge)."""
+    return [(cells + 0.5) / n_grid_z, (cells + 0.5) / n_grid_z, (cells + 0.5) / n_grid_r,
+            sigma1, sigma2]
+
+
 def gamma_velocity(gamma):
     return LIGHT_SPEED * math.sqrt(1.0 - 1.0 / (gamma * gamma))
 
@@ -141,7 +149,7 @@ def thermal_config(seed=1001, n_grid_r=65, n_grid_z=257, r_size=0.05, z_size=0.2
     dz = z_size / (n_grid_z - 1)
     sp = thermal_plasma(rng, r_size, z_size, n_grid_r, n_grid_z, ppc,
                         lambda zc: np.full_like(zc, density), 1.0)
-    pml = [10.0 / n_grid_z, 10.0 / n_grid_z, 10.0 / n_grid_r, 1e-5, 7e-2]
+    pml = absorbing_layer(n_grid_r, n_grid_z, 10)
     return Workload("thermal_%dx%d_ppc%d" % (n_grid_r - 1, n_grid_z - 1, ppc), r_size, z_size,
                     n_grid_r, n_grid_z, courant_dt(dr, dz), steps, pml, "boris", sp)
 
@@ -157,10 +165,10 @@ def wake_config(seed=1002, n_grid_r=257, n_grid_z=2049, r_size=0.1, z_size=0.8, 
     dz = z_size / (n_grid_z - 1)
     sp = thermal_plasma(rng, r_size, z_size, n_grid_r, n_grid_z, ppc,
                         lambda zc: np.full_like(zc, density), 1.0)
-    pml = [10.0 / n_grid_z, 10.0 / n_grid_z, 10.0 / n_grid_r, 1e-5, 7e-2]
+    pml = absorbing_layer(n_grid_r, n_grid_z, 10)
     bunch_cells = (beam_radius / dr) * (beam_length / dz)
     beam = BeamInit(-1.0, 1.0, int(round(64 * bunch_cells)), beam_length, beam_radius,
-                    beam_density, gamma_velocity(beam_gamma), 1, 0.0, "hash", seed)
+                    beam_density, gamma_velocity(beam_gamma), 1, 0.0, "reverse", seed)
     return Workload("wake_%dx%d_ppc%d" % (n_grid_r - 1, n_grid_z - 1, ppc), r_size, z_size,
                     n_grid_r, n_grid_z, courant_dt(dr, dz), steps, pml, pusher, sp, beam)
 

@@ -1,0 +1,157 @@
+"""GPU parity of the FP64 plain form against the oracle (CPU restatement of
+the upstream step), through the C ABI.
+
+Tolerances (FP64, stated per check):
+  * Yee updates alone: bit-identical (same operations, no reduction);
+  * one full step: every grid within 1e-12 of the oracle's max|x| per array
+    (J is summed with atomics, so its summation order differs), every
+    particle array within 1e-12 relative (CUDA log/pow differ from glibc by
+    an ulp or two), alive flags identical;
+  * N steps: grids within 1e-9 of max|x| (rounding differences grow through
+    the coupled field/particle update), and field energy within 1e-10.
+"""
+import numpy as np
+import pytest
+
+from helpers import GRIDS, oracle_from_workload, rel_inf, seed_fields
+from pdp3_b200 import api
+from pdp3_b200 import workloads as W
+
+pytestmark = pytest.mark.gpu
+
+
+def gpu_from_workload(wl, pusher=None):
+    return api.from_workload(wl, pusher=pusher)
+
+
+def compare_particles(gpu, orc, sid, tol):
+    a, b = gpu.species(sid), orc.species(sid)
+    assert np.array_equal(a["alive"], b["alive"])
+    m = b["alive"].astype(bool)
+    for k in ("r", "z", "vr", "vphi", "vz"):
+        scale = max(float(np.abs(b[k][m]).max()) if m.any() else 0.0, 1e-300)
+        err = float(np.abs(a[k][m] - b[k][m]).max()) / scale if m.any() else 0.0
+        assert err <= tol, (sid, k, err)
+
+
+def field_energy(sim, nr, nz, dr, dz):
+    """1/2 sum(eps0 E^2 + mu0 H^2) over node ring volumes (numpy check)."""
+    i = np.arange(nr, dtype=np.float64)
+    vol = np.where(i == 0, np.pi * dz * dr * dr / 4.0, 2.0 * np.pi * dz * dr * dr * i)[:, None]
+    e2 = sum(sim.field(c) ** 2 for c in ("E_r", "E_phi", "E_z"))
+    h2 = sum(sim.field(c) ** 2 for c in ("H_r", "H_phi", "H_z"))
+    return 0.5 * float(((8.85e-12 * e2 + 1.26e-6 * h2) * vol).sum())
+
+
+def test_yee_only_step_is_bit_identical():
+    wl = W.small_config(n_grid_r=33, n_grid_z=65, r_size=0.02, z_size=0.08, ppc=1)
+    wl.species = []
+    orc = oracle_from_workload(wl)
+    gpu = gpu_from_workload(wl)
+    seed_fields([orc, gpu], (wl.n_grid_r, wl.n_grid_z), seed=11)
+    for _ in range(3):
+        orc.step()
+        gpu.step()
+    gpu.sync()
+    for c in GRIDS + ["sigma"]:
+        assert np.array_equal(gpu.field(c), orc.field(c)), c
+
+
+@pytest.mark.parametrize("pusher", ["boris", "vay", "boris_classic"])
+def test_one_step_parity_small_with_bunch(pusher):
+    wl = W.small_config(beam=True, pusher=pusher)
+    orc = oracle_from_workload(wl)
+    gpu = gpu_from_workload(wl)
+    seed_fields([orc, gpu], (wl.n_grid_r, wl.n_grid_z), seed=3)
+    orc.step()
+    gpu.step()
+    gpu.sync()
+    for c in GRIDS:
+        assert rel_inf(gpu.field(c), orc.field(c)) <= 1e-12, c
+    for sid in range(3):
+        compare_particles(gpu, orc, sid, 1e-12)
+
+
+def test_one_step_parity_thermal_64x256():
+    """The 64x256-cell, 32 ppc thermal plasma (1,048,576 particles) with the
+    10-cell absorbing layer: one step from seeded fields."""
+    wl = W.thermal_config(steps=1)
+    orc = oracle_from_workload(wl)
+    gpu = gpu_from_workload(wl)
+    seed_fields([orc, gpu], (wl.n_grid_r, wl.n_grid_z), seed=4)
+    orc.step()
+    gpu.step()
+    gpu.sync()
+    for c in GRIDS:
+        assert rel_inf(gpu.field(c), orc.field(c)) <= 1e-12, c
+    for sid in range(2):
+        compare_particles(gpu, orc, sid, 1e-12)
+
+
+def test_multi_step_parity_small_bunch_injection_and_loss():
+    wl = W.small_config(beam=True, steps=40)
+    orc = oracle_from_workload(wl)
+    gpu = gpu_from_workload(wl)
+    for _ in range(40):
+        orc.step()
+    gpu.step(40)
+    gpu.sync()
+    assert gpu.time == orc.time
+    for c in GRIDS:
+        assert rel_inf(gpu.field(c), orc.field(c)) <= 1e-9, c
+    alive_g = gpu.species(2)["alive"]
+    alive_o = orc.species(2)["alive"]
+    assert alive_g.sum() > 0
+    assert np.array_equal(alive_g, alive_o)
+    fe_o = field_energy(orc, wl.n_grid_r, wl.n_grid_z, wl.dr, wl.dz)
+    fe_g = field_energy(gpu, wl.n_grid_r, wl.n_grid_z, wl.dr, wl.dz)
+    assert fe_o > 0 and abs(fe_g - fe_o) <= 1e-10 * fe_o
+
+
+def test_charge_density_matches_oracle():
+    wl = W.small_config(beam=True)
+    orc = oracle_from_workload(wl)
+    gpu = gpu_from_workload(wl)
+    for _ in range(5):
+        orc.step()
+    gpu.step(5)
+    gpu.sync()
+    for mask in (1, 2, 4, 7):
+        a, b = gpu.charge_density(mask), orc.charge_density(mask)
+        assert rel_inf(a, b) <= 1e-12, mask
+
+
+def test_nan_particle_reports_status_without_fault():
+    wl = W.small_config()
+    gpu = gpu_from_workload(wl)
+    s = gpu.species(0)
+    r = s["r"].copy()
+    r[5] = np.nan
+    gpu.set_species(0, r=r)
+    gpu.step()
+    assert gpu.status() == 3  # PDP3G_NAN_DETECTED
+    gpu.close()
+
+
+def test_particle_outside_grid_reports_status_without_fault():
+    wl = W.small_config()
+    gpu = gpu_from_workload(wl)
+    s = gpu.species(0)
+    z = s["z"].copy()
+    z[7] = 50.0 * wl.z_size
+    gpu.set_species(0, z=z)
+    gpu.step()
+    assert gpu.status() == 5  # PDP3G_OUT_OF_GRID
+    gpu.close()
+
+
+def test_superluminal_velocity_reports_status():
+    wl = W.small_config()
+    gpu = gpu_from_workload(wl)
+    s = gpu.species(0)
+    vz = s["vz"].copy()
+    vz[3] = 4.0e8
+    gpu.set_species(0, vz=vz)
+    gpu.step()
+    assert gpu.status() == 4  # PDP3G_V_GE_C
+    gpu.close()
