@@ -318,7 +318,7 @@ def main():
             cpu = {"value": None, "unit": UNIT, "cores": None, "kind": None,
                    "sample": "failed: %s" % exc}
 
-    traffic = load_traffic(args.workload, args.precision, bytes_particle_phase)
+    traffic = load_traffic(args.workload, args.precision, wl)
     if rank == 0:
         line = {
             "metric": METRIC, "value": value, "unit": UNIT, "n_gpus": world,
@@ -353,15 +353,21 @@ def main():
     return 0
 
 
-def load_traffic(workload, precision, algorithmic):
-    """DRAM traffic per launch of the particle phase from a committed ncu
-    summary (profiles/*.json), or None when none exists."""
-    path = os.path.join(ROOT, "profiles", "traffic_%s_%s.json" % (workload, precision))
+def load_traffic(workload, precision, wl):
+    """DRAM bytes (read + write) of one pass of the particle phase, from the
+    committed ncu summary of the same kernel on the 8-ppc case of this
+    workload, scaled by particle count (the traffic is per particle: the
+    kernel streams each particle once).  None when no summary exists."""
+    path = os.path.join(ROOT, "profiles", "push_deposit_%s_%s_ppc8.md" % (precision, workload))
     try:
         with open(path) as f:
-            return json.load(f)["bytes_per_launch"]
-    except Exception:
-        return None
+            for line in f:
+                if line.startswith("dram_bytes_per_particle:"):
+                    per = float(line.split(":")[1])
+                    return per * sum(s.n for s in wl.species)
+    except OSError:
+        pass
+    return None
 
 
 def run_e2e(sim, wl, torch, stream, steps):

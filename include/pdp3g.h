@@ -77,8 +77,10 @@ typedef struct {
 typedef struct {
   double field_energy;      /* 1/2 sum (eps0 E^2 + mu0 H^2) dV over node volumes */
   double kinetic_energy;    /* sum m_i c^2 (gamma_i - 1) over alive particles */
-  double gauss_residual;    /* ||eps0 div E - (rho - rho_0)||_2, interior, sigma == 0 */
-  double gauss_norm;        /* ||rho - rho_0||_2 over the same nodes */
+  double gauss_residual;    /* ||eps0 div E - (rho - rho_0)||_2 over the nodes
+                               2 <= i <= nr-3, 2 <= k <= nz-3 with sigma == 0 */
+  double gauss_norm;        /* sqrt(sum over species ||rho_s||_2^2), same nodes:
+                               the charge-density scale the residual is relative to */
   double charge_total;      /* sum rho dV */
   int64_t alive;            /* alive macroparticles */
 } pdp3g_diag;

@@ -25,6 +25,7 @@ UNITS = {
     "capi.cu": [],
     "fields.cu": ["--fmad=false"],
     "particles_f64.cu": ["--fmad=false"],
+    "diag.cu": [],
 }
 HEADERS = ["pdp3g_internal.cuh"]
 

@@ -41,7 +41,10 @@ struct pdp3g_ctx {
   unsigned *d_err = nullptr;
   double *d_inv_pow11 = nullptr;
   double *d_rho0 = nullptr;
-  double *d_scratch = nullptr;
+  double *d_scratch = nullptr;   // one grid (charge density)
+  double *d_scratch2 = nullptr;  // one grid (per-species charge density)
+  double *d_partials = nullptr;  // per-block reduction partials
+  double *d_red = nullptr;       // reduction results
   size_t scratch_bytes = 0;
   bool has_rho0 = false;
   std::vector<Species> species;
@@ -281,6 +284,9 @@ void pdp3g_destroy(pdp3g_ctx *ctx) {
   cudaFree(ctx->d_inv_pow11);
   cudaFree(ctx->d_rho0);
   cudaFree(ctx->d_scratch);
+  cudaFree(ctx->d_scratch2);
+  cudaFree(ctx->d_partials);
+  cudaFree(ctx->d_red);
   if (ctx->stream) cudaStreamDestroy(ctx->stream);
   delete ctx;
 }
@@ -521,22 +527,36 @@ pdp3g_status pdp3g_set_species(pdp3g_ctx *ctx, int32_t id, const double *r, cons
   return PDP3G_OK;
 }
 
+static pdp3g_status ensure_scratch(pdp3g_ctx *ctx) {
+  size_t ng = (size_t)ctx->cfg.n_grid_r * ctx->cfg.n_grid_z;
+  if (ctx->d_scratch) return PDP3G_OK;
+  CK(dalloc(ctx, &ctx->d_scratch, ng));
+  CK(dalloc(ctx, &ctx->d_scratch2, ng));
+  CK(dalloc(ctx, &ctx->d_partials, (size_t)diag_blocks() * 4));
+  CK(dalloc(ctx, &ctx->d_red, 16));
+  ctx->scratch_bytes = ng * sizeof(double);
+  return PDP3G_OK;
+}
+
+// charge weighting of the species in mask into dst (device grid)
+static pdp3g_status rho_into(pdp3g_ctx *ctx, uint32_t mask, double *dst) {
+  size_t ng = (size_t)ctx->cfg.n_grid_r * ctx->cfg.n_grid_z;
+  CK(cudaMemsetAsync(dst, 0, ng * sizeof(double), ctx->stream));
+  for (size_t s = 0; s < ctx->species.size() && s < 32; s++)
+    if (mask & (1u << s)) {
+      launch_charge_density_f64(ctx->g, ctx->species[s].dev, dst, ctx->stream);
+      ctx->launches++;
+    }
+  return PDP3G_OK;
+}
+
 pdp3g_status pdp3g_charge_density(pdp3g_ctx *ctx, uint32_t mask, double *host_out) {
   if (!ctx || !host_out) return PDP3G_INVALID_ARG;
   CK(cudaSetDevice(ctx->device));
+  pdp3g_status st = ensure_scratch(ctx);
+  if (st != PDP3G_OK) return st;
   size_t ng = (size_t)ctx->cfg.n_grid_r * ctx->cfg.n_grid_z;
-  if (!ctx->d_scratch || ctx->scratch_bytes < ng * sizeof(double)) {
-    cudaFree(ctx->d_scratch);
-    ctx->d_scratch = nullptr;
-    CK(dalloc(ctx, &ctx->d_scratch, ng));
-    ctx->scratch_bytes = ng * sizeof(double);
-  }
-  CK(cudaMemsetAsync(ctx->d_scratch, 0, ng * sizeof(double), ctx->stream));
-  for (size_t s = 0; s < ctx->species.size() && s < 32; s++)
-    if (mask & (1u << s)) {
-      launch_charge_density_f64(ctx->g, ctx->species[s].dev, ctx->d_scratch, ctx->stream);
-      ctx->launches++;
-    }
+  if ((st = rho_into(ctx, mask, ctx->d_scratch)) != PDP3G_OK) return st;
   CK(cudaMemcpyAsync(host_out, ctx->d_scratch, ng * sizeof(double), cudaMemcpyDeviceToHost,
                      ctx->stream));
   CK(cudaStreamSynchronize(ctx->stream));
@@ -544,12 +564,52 @@ pdp3g_status pdp3g_charge_density(pdp3g_ctx *ctx, uint32_t mask, double *host_ou
 }
 
 pdp3g_status pdp3g_mark_initial_charge(pdp3g_ctx *ctx) {
-  return fail(ctx, PDP3G_NOT_SUPPORTED, "diagnostics not built yet");
+  if (!ctx) return PDP3G_INVALID_ARG;
+  CK(cudaSetDevice(ctx->device));
+  size_t ng = (size_t)ctx->cfg.n_grid_r * ctx->cfg.n_grid_z;
+  if (!ctx->d_rho0) CK(dalloc(ctx, &ctx->d_rho0, ng));
+  pdp3g_status st = rho_into(ctx, 0xFFFFFFFFu, ctx->d_rho0);
+  if (st != PDP3G_OK) return st;
+  CK(cudaStreamSynchronize(ctx->stream));
+  ctx->has_rho0 = true;
+  return PDP3G_OK;
 }
 
 pdp3g_status pdp3g_diagnostics(pdp3g_ctx *ctx, pdp3g_diag *out) {
-  (void)out;
-  return fail(ctx, PDP3G_NOT_SUPPORTED, "diagnostics not built yet");
+  if (!ctx || !out) return PDP3G_INVALID_ARG;
+  CK(cudaSetDevice(ctx->device));
+  pdp3g_status st = ensure_scratch(ctx);
+  if (st != PDP3G_OK) return st;
+  cudaStream_t s = ctx->stream;
+  double *red = ctx->d_red;
+  // red[0..2]: field energy, sum res^2, sum rho dV; red[3]: sum over species of |rho_s|^2;
+  // red[4..5]: kinetic energy, alive (accumulated below on the host)
+  if ((st = rho_into(ctx, 0xFFFFFFFFu, ctx->d_scratch)) != PDP3G_OK) return st;
+  launch_grid_diag(ctx->g, ctx->d_scratch, ctx->has_rho0 ? ctx->d_rho0 : nullptr,
+                   ctx->d_partials, red, s);
+  double host[16] = {0};
+  CK(cudaMemcpyAsync(host, red, 3 * sizeof(double), cudaMemcpyDeviceToHost, s));
+  CK(cudaStreamSynchronize(s));
+  double rho_sq = 0, kin = 0, alive = 0;
+  for (size_t sp = 0; sp < ctx->species.size() && sp < 32; sp++) {
+    if ((st = rho_into(ctx, 1u << sp, ctx->d_scratch2)) != PDP3G_OK) return st;
+    launch_rho_norm(ctx->g, ctx->d_scratch2, ctx->d_partials, red + 8, s);
+    launch_kinetic_f64(ctx->species[sp].dev, ctx->d_partials, red + 9, s);
+    double h3[3];
+    CK(cudaMemcpyAsync(h3, red + 8, 3 * sizeof(double), cudaMemcpyDeviceToHost, s));
+    CK(cudaStreamSynchronize(s));
+    rho_sq += h3[0];
+    kin += h3[1];
+    alive += h3[2];
+  }
+  CK(cudaGetLastError());
+  out->field_energy = host[0];
+  out->gauss_residual = std::sqrt(host[1]);
+  out->charge_total = host[2];
+  out->gauss_norm = std::sqrt(rho_sq);
+  out->kinetic_energy = kin;
+  out->alive = (int64_t)alive;
+  return PDP3G_OK;
 }
 
 pdp3g_status pdp3g_set_timing(pdp3g_ctx *ctx, int32_t enabled) {

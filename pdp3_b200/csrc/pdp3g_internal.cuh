@@ -51,6 +51,12 @@ void launch_push_deposit_f64(const GridDev &g, const SpeciesDev &s, int pusher, 
                              cudaStream_t st);
 void launch_charge_density_f64(const GridDev &g, const SpeciesDev &s, double *rho,
                                cudaStream_t st);
+int diag_blocks();
+void launch_grid_diag(const GridDev &g, const double *rho, const double *rho0, double *partials,
+                      double *out, cudaStream_t st);
+void launch_rho_norm(const GridDev &g, const double *rho, double *partials, double *out,
+                     cudaStream_t st);
+void launch_kinetic_f64(const SpeciesDev &s, double *partials, double *out, cudaStream_t st);
 void launch_bunch_inject(const SpeciesDev &s, long long start, long long count, double dl,
                          double half_dz, double velocity, const double *inv_pow11,
                          cudaStream_t st);

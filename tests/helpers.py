@@ -47,11 +47,14 @@ def golden_match(values, golden):
 def oracle_from_workload(wl, pusher=None):
     o = OracleSim(wl.r_size, wl.z_size, wl.n_grid_r, wl.n_grid_z, wl.dt, pml=wl.pml,
                   pusher=pusher or wl.pusher)
+    o._dr, o._dz = wl.dr, wl.dz
+    o._species_mass = [s.mass_me * 9.1e-31 for s in wl.species]
     for s in wl.species:
         o.add_species(s.charge_e, s.mass_me, s.r, s.z, s.vr, s.vphi, s.vz, s.w)
     if wl.beam is not None:
         b = wl.beam
         assert b.inject_rng == "reverse", "the oracle injects with the upstream TESTMODE sequence"
+        o._species_mass += [b.mass_me * 9.1e-31] * b.number_bunches
         for nb in range(b.number_bunches):
             o.add_bunch(b.charge_e, b.mass_me, b.number_macro, b.bunch_length / b.velocity,
                         b.radius, b.density, b.velocity, nb, b.bunches_distance / b.velocity)
@@ -87,3 +90,42 @@ def rel_inf(a, b):
     if scale == 0.0:
         return float(np.abs(a).max())
     return float(np.abs(a - b).max()) / scale
+
+
+EPS0, MU0, C2 = 8.85e-12, 1.26e-6, 9.0e16
+
+
+def diagnostics_np(sim, n_species, rho0=None):
+    """The pdp3g_diagnostics quantities computed with numpy from an oracle
+    simulation built by oracle_from_workload (grids and particles)."""
+    nr, nz = sim.nr, sim.nz
+    sig = sim.field("sigma")
+    er, ez = sim.field("E_r"), sim.field("E_z")
+    dr, dz = sim._dr, sim._dz
+    i = np.arange(nr, dtype=np.float64)[:, None]
+    vol = np.where(i == 0, np.pi * dz * dr * dr / 4.0, 2.0 * np.pi * dz * dr * dr * i)
+    e2 = sum(sim.field(c) ** 2 for c in ("E_r", "E_phi", "E_z"))
+    h2 = sum(sim.field(c) ** 2 for c in ("H_r", "H_phi", "H_z"))
+    fe = float((0.5 * (EPS0 * e2 + MU0 * h2) * vol).sum())
+    rho = sim.charge_density()
+    mask = np.zeros((nr, nz), dtype=bool)
+    mask[2:nr - 2, 2:nz - 2] = True
+    mask &= sig == 0.0
+    div = np.zeros((nr, nz))
+    div[1:, 1:] = (er[1:, 1:] * (i[1:] + 0.5) - er[:-1, 1:] * (i[1:] - 0.5)) / (i[1:] * dr) + \
+        (ez[1:, 1:] - ez[1:, :-1]) / dz
+    r0 = 0.0 if rho0 is None else rho0
+    res = EPS0 * div - (rho - r0)
+    rho_sq = sum(float((sim.charge_density(1 << s)[mask] ** 2).sum()) for s in range(n_species))
+    kin, alive = 0.0, 0
+    for s in range(n_species):
+        p = sim.species(s)
+        m = p["alive"].astype(bool)
+        mass = sim._species_mass[s] * p["w"][m]
+        b2 = (p["vr"][m] ** 2 + p["vphi"][m] ** 2 + p["vz"][m] ** 2) / C2
+        sq = np.sqrt(1.0 - b2)
+        kin += float((mass * C2 * b2 / (sq * (1.0 + sq))).sum())
+        alive += int(m.sum())
+    return {"field_energy": fe, "gauss_residual": float(np.sqrt((res[mask] ** 2).sum())),
+            "gauss_norm": float(np.sqrt(rho_sq)), "charge_total": float((rho * vol).sum()),
+            "kinetic_energy": kin, "alive": alive}

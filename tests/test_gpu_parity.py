@@ -155,3 +155,25 @@ def test_superluminal_velocity_reports_status():
     gpu.step()
     assert gpu.status() == 4  # PDP3G_V_GE_C
     gpu.close()
+
+
+def test_diagnostics_match_oracle_and_gauss_law_holds():
+    """FP64 diagnostics on the device agree with the same quantities computed
+    from the oracle's state; the Gauss residual stays at rounding level
+    relative to the charge-density scale (no absorbing layer: it damps E)."""
+    from helpers import diagnostics_np
+    wl = W.thermal_config(steps=10, ppc=4)
+    wl.pml = None
+    orc = oracle_from_workload(wl)
+    gpu = gpu_from_workload(wl)
+    gpu.mark_initial_charge()
+    orc.run(10)
+    gpu.step(10)
+    gpu.sync()
+    dg = gpu.diagnostics()
+    do = diagnostics_np(orc, 2)
+    for k in ("field_energy", "kinetic_energy", "gauss_norm"):
+        assert abs(dg[k] - do[k]) <= 1e-9 * abs(do[k]), (k, dg[k], do[k])
+    assert dg["alive"] == do["alive"]
+    assert dg["gauss_residual"] <= 1e-10 * dg["gauss_norm"]
+    assert do["gauss_residual"] <= 1e-10 * do["gauss_norm"]

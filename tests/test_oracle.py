@@ -161,3 +161,18 @@ def test_oracle_neutral_start_and_determinism():
     for c in GRIDS:
         assert np.array_equal(a.field(c), b.field(c))
     assert a.errors == 0
+
+
+def test_upstream_deposition_conserves_charge():
+    """The upstream r-z and azimuthal deposition is charge-conserving for the
+    upstream charge weighting and the Yee divergence: starting neutral, the
+    Gauss residual stays at FP64 rounding level (no absorbing layer)."""
+    from helpers import diagnostics_np
+    wl = W.thermal_config(steps=10, ppc=4)
+    wl.pml = None
+    o = oracle_from_workload(wl)
+    o.run(10)
+    d = diagnostics_np(o, 2)
+    assert d["gauss_norm"] > 0
+    assert d["gauss_residual"] <= 1e-11 * d["gauss_norm"]
+    assert d["kinetic_energy"] > 0 and d["alive"] == sum(s.n for s in wl.species)
