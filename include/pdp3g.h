@@ -127,6 +127,13 @@ pdp3g_status pdp3g_add_bunch(pdp3g_ctx *ctx, double charge_e, double mass_me, in
    t += dt.  Asynchronous on the context's stream. */
 pdp3g_status pdp3g_step(pdp3g_ctx *ctx, int32_t nsteps);
 
+/* Stable sort of every plasma species by cell index (an integer LSD radix
+   sort of (cell, index) pairs; the permutation equals a stable sort of the
+   cell keys).  No upstream counterpart: upstream particles stay in creation
+   order.  Bunch species keep their slot order.  pdp3g_step also sorts every
+   cfg.sort_interval steps. */
+pdp3g_status pdp3g_sort(pdp3g_ctx *ctx);
+
 /* Waits for the stream and reports device-side error flags. */
 pdp3g_status pdp3g_sync(pdp3g_ctx *ctx);
 

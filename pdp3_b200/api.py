@@ -70,6 +70,7 @@ EXPORTS = [
                                ctypes.c_double, _I32, ctypes.c_double, ctypes.POINTER(_I32)]),
     ("pdp3g_step", _I32, [_VP, _I32]),
     ("pdp3g_sync", _I32, [_VP]),
+    ("pdp3g_sort", _I32, [_VP]),
     ("pdp3g_get_field", _I32, [_VP, _I32, _D]),
     ("pdp3g_set_field", _I32, [_VP, _I32, _D]),
     ("pdp3g_get_species", _I32, [_VP, _I32] + [_D] * 6 + [_U8]),
@@ -159,6 +160,9 @@ class Simulation:
 
     def step(self, n=1):
         self._check(self.L.pdp3g_step(self.h, int(n)), "step")
+
+    def sort(self):
+        self._check(self.L.pdp3g_sort(self.h), "sort")
 
     def sync(self):
         self._check(self.L.pdp3g_sync(self.h), "sync")

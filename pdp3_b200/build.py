@@ -25,6 +25,8 @@ UNITS = {
     "capi.cu": [],
     "fields.cu": ["--fmad=false"],
     "particles_f64.cu": ["--fmad=false"],
+    "particles_f32.cu": [],
+    "sort.cu": [],
     "diag.cu": [],
 }
 HEADERS = ["pdp3g_internal.cuh"]

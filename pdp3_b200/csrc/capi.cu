@@ -3,6 +3,7 @@
 // host <-> device copies for the upstream-style public state.
 #include <cuda_runtime.h>
 
+#include <algorithm>
 #include <cmath>
 #include <cstdio>
 #include <cstring>
@@ -17,8 +18,11 @@ using namespace pdp3g;
 namespace {
 
 struct Species {
-  SpeciesDev dev{};
+  SpeciesDev dev{};      // FP64 plain form
+  SpeciesF32 f32{};      // FP32 cell-local form
+  bool fp32 = false;
   bool is_bunch = false;
+  double charge_si = 0, mass_si = 0;  // per unit weight
   // Bunch parameters (src/bunch.cpp:17-26)
   double duration = 0, radius = 0, density = 0, velocity = 0, hole_duration = 0;
   double bunch_number = 0;
@@ -45,6 +49,9 @@ struct pdp3g_ctx {
   double *d_scratch2 = nullptr;  // one grid (per-species charge density)
   double *d_partials = nullptr;  // per-block reduction partials
   double *d_red = nullptr;       // reduction results
+  char *d_sort = nullptr;        // radix-sort scratch
+  size_t sort_bytes = 0;
+  int64_t sorts = 0;
   size_t scratch_bytes = 0;
   bool has_rho0 = false;
   std::vector<Species> species;
@@ -56,6 +63,7 @@ struct pdp3g_ctx {
   int64_t launches = 0, particle_launches = 0, steps = 0;
   std::string last_error;
   int64_t bytes = 0;
+  int f32_blocks_per_sm = 4;  // CTAs per SM for the FP32 particle kernel
 };
 
 namespace {
@@ -197,7 +205,8 @@ pdp3g_status pdp3g_create(const pdp3g_config *cfg, pdp3g_ctx **out) {
   if (!cfg || !out) return PDP3G_INVALID_ARG;
   *out = nullptr;
   if (cfg->n_grid_r < 3 || cfg->n_grid_z < 3 || !(cfg->r_size > 0) || !(cfg->z_size > 0) ||
-      !(cfg->dt > 0) || cfg->pusher < 0 || cfg->pusher > 2 || cfg->precision != PDP3G_FP64)
+      !(cfg->dt > 0) || cfg->pusher < 0 || cfg->pusher > 2 ||
+      (cfg->precision != PDP3G_FP64 && cfg->precision != PDP3G_FP32_CELL))
     return PDP3G_INVALID_ARG;
   pdp3g_ctx *ctx = new pdp3g_ctx();
   ctx->cfg = *cfg;
@@ -276,6 +285,14 @@ void pdp3g_destroy(pdp3g_ctx *ctx) {
     cudaFree(sp.dev.vz);
     cudaFree((void *)sp.dev.w);
     cudaFree(sp.dev.alive);
+    cudaFree(sp.f32.cell);
+    cudaFree(sp.f32.fr);
+    cudaFree(sp.f32.fz);
+    cudaFree(sp.f32.ur);
+    cudaFree(sp.f32.uphi);
+    cudaFree(sp.f32.uz);
+    cudaFree((void *)sp.f32.w);
+    if (sp.f32.alive != sp.dev.alive) cudaFree(sp.f32.alive);
   }
   for (auto &se : ctx->step_events)
     for (auto &e : se.ev) cudaEventDestroy(e);
@@ -287,6 +304,7 @@ void pdp3g_destroy(pdp3g_ctx *ctx) {
   cudaFree(ctx->d_scratch2);
   cudaFree(ctx->d_partials);
   cudaFree(ctx->d_red);
+  cudaFree(ctx->d_sort);
   if (ctx->stream) cudaStreamDestroy(ctx->stream);
   delete ctx;
 }
@@ -305,6 +323,70 @@ static pdp3g_status alloc_species(pdp3g_ctx *ctx, Species &sp, int64_t n, bool w
   return PDP3G_OK;
 }
 
+// FP64 (r, z, v) -> cell-local FP32 (cell, offsets, u = gamma v / c)
+static pdp3g_status to_cell_local(pdp3g_ctx *ctx, int64_t n, const double *r, const double *z,
+                                  const double *vr, const double *vphi, const double *vz,
+                                  std::vector<int> &cell, std::vector<float> &fr,
+                                  std::vector<float> &fz, std::vector<float> &ur,
+                                  std::vector<float> &uphi, std::vector<float> &uz) {
+  const int nr = ctx->cfg.n_grid_r, nz = ctx->cfg.n_grid_z, ncz = nz - 1;
+  const double dr = ctx->dr, dz = ctx->dz;
+  cell.resize(n); fr.resize(n); fz.resize(n); ur.resize(n); uphi.resize(n); uz.resize(n);
+  for (int64_t p = 0; p < n; p++) {
+    if (!std::isfinite(r[p]) || !std::isfinite(z[p]))
+      return fail(ctx, PDP3G_NAN_DETECTED, "particle position is NaN or Inf");
+    int i = (int)std::ceil(r[p] / dr) - 1, k = (int)std::ceil(z[p] / dz) - 1;
+    if (i < 0) i = 0;
+    if (k < 0) k = 0;
+    if (i > nr - 2 || k > nz - 2) return fail(ctx, PDP3G_OUT_OF_GRID, "particle outside the grid");
+    cell[p] = i * ncz + k;
+    fr[p] = (float)(r[p] / dr - i);
+    fz[p] = (float)(z[p] / dz - k);
+    const double v2 = vr[p] * vr[p] + vphi[p] * vphi[p] + vz[p] * vz[p];
+    if (!(v2 < LIGHT_SPEED_POW_2)) return fail(ctx, PDP3G_V_GE_C, "velocity >= c");
+    const double gc = 1.0 / (LIGHT_SPEED * std::sqrt(1.0 - v2 / LIGHT_SPEED_POW_2));
+    ur[p] = (float)(vr[p] * gc);
+    uphi[p] = (float)(vphi[p] * gc);
+    uz[p] = (float)(vz[p] * gc);
+  }
+  return PDP3G_OK;
+}
+
+static void f32_constants(pdp3g_ctx *ctx, Species &sp) {
+  const double dt = ctx->cfg.dt, dr = ctx->dr, dz = ctx->dz;
+  const double q = sp.charge_si, m = sp.mass_si, c = LIGHT_SPEED;
+  const double const1 = q * dt / (2 * m);
+  SpeciesF32 &f = sp.f32;
+  f.ke = (float)(const1 / c);
+  f.kb = (float)(MAGN_CONST * const1);
+  f.cr = (float)(c * dt / (2 * dr));
+  f.cz = (float)(c * dt / (2 * dz));
+  f.kphi = (float)(q * c / (2 * PI * dz * dr * dr));
+  f.kz = (float)(q / (4 * PI * dr * dr * dt));
+  f.kr = (float)(q / (2 * PI * dr * dz * dt));
+  f.vay_e = (float)(2 * const1);
+  f.vay_b = (float)(MAGN_CONST * const1 * 2 * const1 * const1);
+  f.inv_c2 = (float)(1.0 / LIGHT_SPEED_POW_2);
+}
+
+static pdp3g_status upload_f32(pdp3g_ctx *ctx, Species &sp, int64_t n, const double *r,
+                               const double *z, const double *vr, const double *vphi,
+                               const double *vz) {
+  std::vector<int> cell;
+  std::vector<float> fr, fz, ur, uphi, uz;
+  pdp3g_status st = to_cell_local(ctx, n, r, z, vr, vphi, vz, cell, fr, fz, ur, uphi, uz);
+  if (st != PDP3G_OK) return st;
+  SpeciesF32 &f = sp.f32;
+  size_t b = sizeof(float) * (size_t)n;
+  CK(cudaMemcpy(f.cell, cell.data(), sizeof(int) * (size_t)n, cudaMemcpyHostToDevice));
+  CK(cudaMemcpy(f.fr, fr.data(), b, cudaMemcpyHostToDevice));
+  CK(cudaMemcpy(f.fz, fz.data(), b, cudaMemcpyHostToDevice));
+  CK(cudaMemcpy(f.ur, ur.data(), b, cudaMemcpyHostToDevice));
+  CK(cudaMemcpy(f.uphi, uphi.data(), b, cudaMemcpyHostToDevice));
+  CK(cudaMemcpy(f.uz, uz.data(), b, cudaMemcpyHostToDevice));
+  return PDP3G_OK;
+}
+
 pdp3g_status pdp3g_add_species(pdp3g_ctx *ctx, double charge_e, double mass_me, int64_t n,
                                const double *r, const double *z, const double *vr,
                                const double *vphi, const double *vz, const double *w,
@@ -314,8 +396,37 @@ pdp3g_status pdp3g_add_species(pdp3g_ctx *ctx, double charge_e, double mass_me, 
   if (n > (int64_t)1 << 40) return fail(ctx, PDP3G_INVALID_ARG, "add_species: n too large");
   CK(cudaSetDevice(ctx->device));
   Species sp;
-  sp.dev.charge = charge_e * EL_CHARGE;  // src/particles.cpp:30-32
-  sp.dev.mass = mass_me * EL_MASS;
+  sp.charge_si = charge_e * EL_CHARGE;  // src/particles.cpp:30-32
+  sp.mass_si = mass_me * EL_MASS;
+  if (ctx->cfg.precision == PDP3G_FP32_CELL) {
+    sp.fp32 = true;
+    SpeciesF32 &f = sp.f32;
+    f.n = n;
+    f.kind = KIND_PLASMA;
+    f32_constants(ctx, sp);
+    CK(dalloc(ctx, &f.cell, (size_t)n));
+    CK(dalloc(ctx, &f.fr, (size_t)n));
+    CK(dalloc(ctx, &f.fz, (size_t)n));
+    CK(dalloc(ctx, &f.ur, (size_t)n));
+    CK(dalloc(ctx, &f.uphi, (size_t)n));
+    CK(dalloc(ctx, &f.uz, (size_t)n));
+    float *wf = nullptr;
+    CK(dalloc(ctx, &wf, (size_t)n));
+    f.w = wf;
+    pdp3g_status st = upload_f32(ctx, sp, n, r, z, vr, vphi, vz);
+    if (st != PDP3G_OK) return st;
+    std::vector<float> wv(w, w + n);
+    CK(cudaMemcpy(wf, wv.data(), sizeof(float) * (size_t)n, cudaMemcpyHostToDevice));
+    if (alive) {
+      CK(dalloc(ctx, &f.alive, (size_t)n));
+      CK(cudaMemcpy(f.alive, alive, (size_t)n, cudaMemcpyHostToDevice));
+    }
+    ctx->species.push_back(sp);
+    if (id) *id = (int32_t)ctx->species.size() - 1;
+    return PDP3G_OK;
+  }
+  sp.dev.charge = sp.charge_si;
+  sp.dev.mass = sp.mass_si;
   sp.dev.kind = KIND_PLASMA;
   pdp3g_status st = alloc_species(ctx, sp, n, alive != nullptr);
   if (st != PDP3G_OK) return st;
@@ -372,6 +483,7 @@ pdp3g_status pdp3g_add_bunch(pdp3g_ctx *ctx, double charge_e, double mass_me, in
   Species &sp = ctx->species[sid];
   sp.is_bunch = true;
   sp.dev.kind = KIND_BUNCH;
+  sp.f32.kind = KIND_BUNCH;
   sp.duration = duration;
   sp.radius = radius;
   sp.density = density;
@@ -384,7 +496,40 @@ pdp3g_status pdp3g_add_bunch(pdp3g_ctx *ctx, double charge_e, double mass_me, in
 
 int64_t pdp3g_species_size(pdp3g_ctx *ctx, int32_t id) {
   if (!ctx || id < 0 || id >= (int32_t)ctx->species.size()) return -1;
-  return ctx->species[id].dev.n;
+  const Species &sp = ctx->species[id];
+  return sp.fp32 ? sp.f32.n : sp.dev.n;
+}
+
+// stable sort of every plasma species by cell (bunch species keep their
+// slot order, which the injection schedule indexes)
+static pdp3g_status sort_all(pdp3g_ctx *ctx) {
+  long long nmax = 0;
+  for (auto &sp : ctx->species)
+    if (!sp.is_bunch) nmax = std::max<long long>(nmax, sp.fp32 ? sp.f32.n : sp.dev.n);
+  if (nmax <= 1) return PDP3G_OK;
+  const size_t need = sort_layout(nmax).total;
+  if (ctx->sort_bytes < need) {
+    cudaFree(ctx->d_sort);
+    ctx->d_sort = nullptr;
+    ctx->sort_bytes = 0;
+    CK(dalloc(ctx, &ctx->d_sort, need));
+    ctx->sort_bytes = need;
+  }
+  for (auto &sp : ctx->species) {
+    if (sp.is_bunch) continue;
+    int nl = sp.fp32 ? sort_species_f32(ctx->g, sp.f32, ctx->d_sort, ctx->stream)
+                     : sort_species_f64(ctx->g, sp.dev, ctx->d_sort, ctx->stream);
+    ctx->launches += nl;
+  }
+  ctx->sorts++;
+  CK(cudaGetLastError());
+  return PDP3G_OK;
+}
+
+pdp3g_status pdp3g_sort(pdp3g_ctx *ctx) {
+  if (!ctx) return PDP3G_INVALID_ARG;
+  CK(cudaSetDevice(ctx->device));
+  return sort_all(ctx);
 }
 
 pdp3g_status pdp3g_step(pdp3g_ctx *ctx, int32_t nsteps) {
@@ -403,7 +548,7 @@ pdp3g_status pdp3g_step(pdp3g_ctx *ctx, int32_t nsteps) {
       double end = begin + sp.duration;
       double dl = sp.velocity * dt;
       int steps_amount = (int)std::ceil(sp.duration / dt);
-      unsigned int number = (unsigned int)sp.dev.n;
+      unsigned int number = (unsigned int)(sp.fp32 ? sp.f32.n : sp.dev.n);
       unsigned int particles_in_step = number / steps_amount;
       int start_number = (ctx->t - begin) / dt * particles_in_step;
       if (ctx->t >= begin && ctx->t < end && particles_in_step > 0) {
@@ -413,8 +558,16 @@ pdp3g_status pdp3g_step(pdp3g_ctx *ctx, int32_t nsteps) {
         if (start >= (long long)number) count = 0;
         else if (start + count > (long long)number) count = (long long)number - start;
         if (count > 0) {
-          launch_bunch_inject(sp.dev, start, count, dl, ctx->dz / 2.0, sp.velocity,
-                              ctx->d_inv_pow11, st);
+          if (sp.fp32) {
+            const double gv = sp.velocity /
+                              (LIGHT_SPEED * std::sqrt(1.0 - sp.velocity * sp.velocity /
+                                                                  LIGHT_SPEED_POW_2));
+            launch_bunch_inject_f32(sp.f32, start, count, dl, ctx->dz / 2.0, ctx->dz,
+                                    ctx->cfg.n_grid_z - 1, (float)gv, ctx->d_inv_pow11, st);
+          } else {
+            launch_bunch_inject(sp.dev, start, count, dl, ctx->dz / 2.0, sp.velocity,
+                                ctx->d_inv_pow11, st);
+          }
           ctx->launches++;
         }
       }
@@ -426,10 +579,18 @@ pdp3g_status pdp3g_step(pdp3g_ctx *ctx, int32_t nsteps) {
     if (ev) cudaEventRecord(ev->ev[2], st);
     // 3. Current::reset_j
     CK(cudaMemsetAsync(ctx->g.jr, 0, sizeof(double) * ng * 3, st));
+    if (ctx->cfg.sort_interval > 0 && ctx->steps % ctx->cfg.sort_interval == 0) {
+      pdp3g_status ss = sort_all(ctx);
+      if (ss != PDP3G_OK) return ss;
+    }
     if (ev) cudaEventRecord(ev->ev[3], st);
     // 4. ParticlesList::step_v + full_current_distribution
     for (auto &sp : ctx->species) {
-      launch_push_deposit_f64(ctx->g, sp.dev, ctx->cfg.pusher, ctx->n_sm, st);
+      if (sp.fp32)
+        launch_push_deposit_f32(ctx->g, sp.f32, ctx->cfg.pusher, ctx->n_sm, ctx->f32_blocks_per_sm,
+                                st);
+      else
+        launch_push_deposit_f64(ctx->g, sp.dev, ctx->cfg.pusher, ctx->n_sm, st);
       ctx->launches++;
       ctx->particle_launches++;
     }
@@ -486,9 +647,43 @@ pdp3g_status pdp3g_get_species(pdp3g_ctx *ctx, int32_t id, double *r, double *z,
                                double *vphi, double *vz, double *w, uint8_t *alive) {
   if (!ctx || id < 0 || id >= (int32_t)ctx->species.size()) return PDP3G_INVALID_ARG;
   CK(cudaSetDevice(ctx->device));
-  const SpeciesDev &d = ctx->species[id].dev;
-  size_t b = sizeof(double) * (size_t)d.n;
   cudaStream_t st = ctx->stream;
+  const Species &sp = ctx->species[id];
+  if (sp.fp32) {
+    const SpeciesF32 &f = sp.f32;
+    const size_t n = (size_t)f.n;
+    std::vector<int> cell(n);
+    std::vector<float> fr(n), fz(n), ur(n), uphi(n), uz(n), wf(n);
+    CK(cudaMemcpyAsync(cell.data(), f.cell, sizeof(int) * n, cudaMemcpyDeviceToHost, st));
+    CK(cudaMemcpyAsync(fr.data(), f.fr, sizeof(float) * n, cudaMemcpyDeviceToHost, st));
+    CK(cudaMemcpyAsync(fz.data(), f.fz, sizeof(float) * n, cudaMemcpyDeviceToHost, st));
+    CK(cudaMemcpyAsync(ur.data(), f.ur, sizeof(float) * n, cudaMemcpyDeviceToHost, st));
+    CK(cudaMemcpyAsync(uphi.data(), f.uphi, sizeof(float) * n, cudaMemcpyDeviceToHost, st));
+    CK(cudaMemcpyAsync(uz.data(), f.uz, sizeof(float) * n, cudaMemcpyDeviceToHost, st));
+    CK(cudaMemcpyAsync(wf.data(), f.w, sizeof(float) * n, cudaMemcpyDeviceToHost, st));
+    if (alive) {
+      if (f.alive)
+        CK(cudaMemcpyAsync(alive, f.alive, n, cudaMemcpyDeviceToHost, st));
+      else
+        memset(alive, 1, n);
+    }
+    CK(cudaStreamSynchronize(st));
+    const int ncz = ctx->cfg.n_grid_z - 1;
+    for (size_t p = 0; p < n; p++) {
+      const int i = cell[p] / ncz, k = cell[p] - (cell[p] / ncz) * ncz;
+      if (r) r[p] = (i + (double)fr[p]) * ctx->dr;
+      if (z) z[p] = (k + (double)fz[p]) * ctx->dz;
+      const double u2 = (double)ur[p] * ur[p] + (double)uphi[p] * uphi[p] + (double)uz[p] * uz[p];
+      const double c_over_g = LIGHT_SPEED / std::sqrt(1.0 + u2);
+      if (vr) vr[p] = ur[p] * c_over_g;
+      if (vphi) vphi[p] = uphi[p] * c_over_g;
+      if (vz) vz[p] = uz[p] * c_over_g;
+      if (w) w[p] = wf[p];
+    }
+    return PDP3G_OK;
+  }
+  const SpeciesDev &d = sp.dev;
+  size_t b = sizeof(double) * (size_t)d.n;
   if (r) CK(cudaMemcpyAsync(r, d.r, b, cudaMemcpyDeviceToHost, st));
   if (z) CK(cudaMemcpyAsync(z, d.z, b, cudaMemcpyDeviceToHost, st));
   if (vr) CK(cudaMemcpyAsync(vr, d.vr, b, cudaMemcpyDeviceToHost, st));
@@ -511,6 +706,27 @@ pdp3g_status pdp3g_set_species(pdp3g_ctx *ctx, int32_t id, const double *r, cons
   if (!ctx || id < 0 || id >= (int32_t)ctx->species.size()) return PDP3G_INVALID_ARG;
   CK(cudaSetDevice(ctx->device));
   Species &sp = ctx->species[id];
+  if (sp.fp32) {
+    // the cell index packs r and z: rebuild the full FP64 state, replace the
+    // given arrays and convert back
+    const size_t n = (size_t)sp.f32.n;
+    std::vector<double> R(n), Z(n), VR(n), VP(n), VZ(n);
+    pdp3g_status gs = pdp3g_get_species(ctx, id, R.data(), Z.data(), VR.data(), VP.data(),
+                                        VZ.data(), nullptr, nullptr);
+    if (gs != PDP3G_OK) return gs;
+    if (r) memcpy(R.data(), r, n * sizeof(double));
+    if (z) memcpy(Z.data(), z, n * sizeof(double));
+    if (vr) memcpy(VR.data(), vr, n * sizeof(double));
+    if (vphi) memcpy(VP.data(), vphi, n * sizeof(double));
+    if (vz) memcpy(VZ.data(), vz, n * sizeof(double));
+    gs = upload_f32(ctx, sp, (int64_t)n, R.data(), Z.data(), VR.data(), VP.data(), VZ.data());
+    if (gs != PDP3G_OK) return gs;
+    if (alive) {
+      if (!sp.f32.alive) CK(dalloc(ctx, &sp.f32.alive, n));
+      CK(cudaMemcpy(sp.f32.alive, alive, n, cudaMemcpyHostToDevice));
+    }
+    return PDP3G_OK;
+  }
   SpeciesDev &d = sp.dev;
   size_t b = sizeof(double) * (size_t)d.n;
   cudaStream_t st = ctx->stream;
@@ -544,7 +760,11 @@ static pdp3g_status rho_into(pdp3g_ctx *ctx, uint32_t mask, double *dst) {
   CK(cudaMemsetAsync(dst, 0, ng * sizeof(double), ctx->stream));
   for (size_t s = 0; s < ctx->species.size() && s < 32; s++)
     if (mask & (1u << s)) {
-      launch_charge_density_f64(ctx->g, ctx->species[s].dev, dst, ctx->stream);
+      const Species &sp = ctx->species[s];
+      if (sp.fp32)
+        launch_charge_density_f32(ctx->g, sp.f32, sp.charge_si, dst, ctx->stream);
+      else
+        launch_charge_density_f64(ctx->g, sp.dev, dst, ctx->stream);
       ctx->launches++;
     }
   return PDP3G_OK;
@@ -594,7 +814,11 @@ pdp3g_status pdp3g_diagnostics(pdp3g_ctx *ctx, pdp3g_diag *out) {
   for (size_t sp = 0; sp < ctx->species.size() && sp < 32; sp++) {
     if ((st = rho_into(ctx, 1u << sp, ctx->d_scratch2)) != PDP3G_OK) return st;
     launch_rho_norm(ctx->g, ctx->d_scratch2, ctx->d_partials, red + 8, s);
-    launch_kinetic_f64(ctx->species[sp].dev, ctx->d_partials, red + 9, s);
+    if (ctx->species[sp].fp32)
+      launch_kinetic_f32(ctx->species[sp].f32, ctx->species[sp].mass_si, ctx->d_partials, red + 9,
+                         s);
+    else
+      launch_kinetic_f64(ctx->species[sp].dev, ctx->d_partials, red + 9, s);
     double h3[3];
     CK(cudaMemcpyAsync(h3, red + 8, 3 * sizeof(double), cudaMemcpyDeviceToHost, s));
     CK(cudaStreamSynchronize(s));

@@ -118,6 +118,10 @@ __global__ void __launch_bounds__(RED_THREADS) k_kinetic_f64(SpeciesDev s, doubl
 
 int diag_blocks() { return 148 * 4; }
 
+void launch_finalize(const double *partials, int nblocks, int nv, double *out, cudaStream_t st) {
+  k_finalize<<<1, RED_THREADS, 0, st>>>(partials, nblocks, nv, out);
+}
+
 void launch_grid_diag(const GridDev &g, const double *rho, const double *rho0, double *partials,
                       double *out, cudaStream_t st) {
   const int nb = diag_blocks();

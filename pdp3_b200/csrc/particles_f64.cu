@@ -239,7 +239,7 @@ __device__ __forceinline__ void deposit_jphi(const GridDev &g, double q, double 
 #define DENS_STRICT(q, r, dr, dz, dt) ((q) / (PI * 4. * (r) * (dz) * (dz) * (dr) * (dt)))
 
 // Particles::simple_current_distribution, src/particles.cpp:333-474
-__device__ __noinline__ void simple_current(const GridDev &g, double q, double radius_new,
+__device__ __forceinline__ void simple_current(const GridDev &g, double q, double radius_new,
                                             double longitude_new, double radius_old,
                                             double longitude_old, int i_n, int k_n) {
   const double dr = g.dr, dz = g.dz, delta_t = g.dt;
@@ -289,7 +289,7 @@ __device__ __noinline__ void simple_current(const GridDev &g, double q, double r
 }
 
 // Particles::strict_motion_weighting, src/particles.cpp:786-988
-__device__ __noinline__ void strict_motion(const GridDev &g, double q, double radius_new,
+__device__ __forceinline__ void strict_motion(const GridDev &g, double q, double radius_new,
                                            double longitude_new, double radius_old,
                                            double longitude_old) {
   const double dr = g.dr, dz = g.dz, delta_t = g.dt;
@@ -524,7 +524,9 @@ __device__ __forceinline__ void deposit_rz(const GridDev &g, double q, double r_
 }
 
 // The fused particle phase for one species.
-__global__ void __launch_bounds__(256) k_push_deposit_f64(GridDev g, SpeciesDev s, int pusher) {
+// 4 CTAs of 256 threads per SM (64 registers): the kernel is latency-bound
+// and gains more from residency than it loses to the few spilled registers.
+__global__ void __launch_bounds__(256, 4) k_push_deposit_f64(GridDev g, SpeciesDev s, int pusher) {
   const double half_dt = g.dt / 2.;
   const double dr = g.dr, dz = g.dz;
   const double radius_wall = g.r_size - dr / 2.;

@@ -3,6 +3,7 @@
 
 #include <cuda_runtime.h>
 #include <stdint.h>
+#include <climits>
 
 namespace pdp3g {
 
@@ -44,7 +45,90 @@ struct SpeciesDev {
   int kind;
 };
 
-// host-side launchers (fields.cu, particles_f64.cu, diag.cu)
+// FP32 cell-local species (particles_f32.cu).
+struct SpeciesF32 {
+  int *cell;           // i * (nz - 1) + k
+  float *fr, *fz;      // in-cell offsets in (0, 1]
+  float *ur, *uphi, *uz;  // gamma v / c
+  const float *w;
+  uint8_t *alive;      // bunch species only
+  long long n;
+  int kind;
+  // species constants (FP32)
+  float ke;     // charge dt / (2 mass c):  du per V/m (Boris)
+  float kb;     // mu0 charge dt / (2 mass): rotation vector per A/m (Boris)
+  float cr, cz; // c dt / (2 dr), c dt / (2 dz): half-step move per unit v/c, in cells
+  float kphi;   // charge c / (2 pi dz dr^2): j_phi per (w u_phi/gamma x weight)
+  float kz;     // charge / (4 pi dr^2 dt)
+  float kr;     // charge / (2 pi dr dz dt)
+  float vay_e;  // charge dt / mass (upstream Vay: e * 2 const1)
+  float vay_b;  // 2 mu0 const1^3 (upstream Vay: b * mu0 const1 * 2 const1 * const1)
+  float inv_c2; // 1 / c^2
+};
+
+// Particles::charge_weighting per particle, src/particles.cpp:101-226
+// (adds q at (r, z) into rho with the upstream volume weights).
+__device__ __forceinline__ void charge_weight_one(const GridDev &g, double *rho, double r,
+                                                  double z, double q) {
+  const double dr = g.dr, dz = g.dz;
+  int r_i = (int)ceil(r / dr) - 1, z_k = (int)ceil(z / dz) - 1;
+  if (r_i < 0) r_i = 0;
+  if (z_k < 0) z_k = 0;
+  double r1, r2, r3, ro_v, v_1, v_2, w[4];
+  const double dz1 = (z_k + 0.5) * dz - (z - 0.5 * dz);
+  const double dz2 = (z + 0.5 * dz) - (z_k + 0.5) * dz;
+  if (r > dr) {
+    r1 = r - 0.5 * dr; r2 = (r_i + 0.5) * dr; r3 = r + 0.5 * dr;
+    ro_v = q / (2. * PI * dz * dr * r);
+    v_1 = PI * dz * dr * dr * 2.0 * (r_i);
+    v_2 = PI * dz * dr * dr * 2.0 * (r_i + 1);
+    w[0] = ro_v * PI * dz1 * (r2 * r2 - r1 * r1) / v_1;
+    w[1] = ro_v * PI * dz1 * (r3 * r3 - r2 * r2) / v_2;
+    w[2] = ro_v * PI * dz2 * (r2 * r2 - r1 * r1) / v_1;
+    w[3] = ro_v * PI * dz2 * (r3 * r3 - r2 * r2) / v_2;
+  } else if (r <= dr / 2.) {
+    r_i = 0;
+    r2 = (r_i + 0.5) * dr; r3 = r + 0.5 * dr;
+    ro_v = q / (PI * dz * (2. * r * r + dr * dr / 2.));
+    v_1 = PI * dz * dr * dr / 4.;
+    v_2 = PI * dz * dr * dr * 2.0 * (r_i + 1);
+    w[0] = ro_v * PI * dz1 * (dr * dr / 2. - r * dr + r * r) / v_1;
+    w[1] = ro_v * PI * dz1 * (r3 * r3 - r2 * r2) / v_2;
+    w[2] = ro_v * PI * dz2 * (dr * dr / 2. - r * dr + r * r) / v_1;
+    w[3] = ro_v * PI * dz2 * (r3 * r3 - r2 * r2) / v_2;
+  } else {
+    r1 = r - 0.5 * dr; r2 = (r_i + 0.5) * dr; r3 = r + 0.5 * dr;
+    ro_v = q / (2. * PI * dz * dr * r);
+    v_1 = PI * dz * dr * dr / 4.;
+    v_2 = PI * dz * dr * dr * 2.0 * (r_i + 1);
+    w[0] = ro_v * PI * dz1 * (r2 * r2 - r1 * r1) / v_1;
+    w[1] = ro_v * PI * dz1 * (r3 * r3 - r2 * r2) / v_2;
+    w[2] = ro_v * PI * dz2 * (r2 * r2 - r1 * r1) / v_1;
+    w[3] = ro_v * PI * dz2 * (r3 * r3 - r2 * r2) / v_2;
+  }
+  const int ii[4] = {r_i, r_i + 1, r_i, r_i + 1}, kk[4] = {z_k, z_k, z_k + 1, z_k + 1};
+#pragma unroll
+  for (int j = 0; j < 4; j++) {
+    if ((unsigned)ii[j] >= (unsigned)g.nr || (unsigned)kk[j] >= (unsigned)g.nz) {
+      atomicOr(g.err, ERR_OUT_OF_GRID);
+      continue;
+    }
+    atomicAdd(rho + (size_t)ii[j] * g.nz + kk[j], w[j]);
+  }
+}
+
+// byte offsets of the radix sort's scratch (sort.cu)
+struct SortLayout {
+  long long nsub, m, nb;
+  size_t keys_a, keys_b, idx_a, idx_b, H, bs, tmp, total;
+};
+SortLayout sort_layout(long long n);
+int sort_species_f64(const GridDev &g, SpeciesDev &s, char *scratch, cudaStream_t st);
+int sort_species_f32(const GridDev &g, SpeciesF32 &s, char *scratch, cudaStream_t st);
+int sort_keys(const unsigned *keys, long long n, int key_bits, char *scratch,
+              unsigned *perm_out, cudaStream_t st);
+
+// host-side launchers (fields.cu, particles_f64.cu, particles_f32.cu, diag.cu)
 void launch_yee_h(const GridDev &g, cudaStream_t st);
 void launch_yee_e(const GridDev &g, cudaStream_t st);
 void launch_push_deposit_f64(const GridDev &g, const SpeciesDev &s, int pusher, int n_sm,
@@ -52,6 +136,16 @@ void launch_push_deposit_f64(const GridDev &g, const SpeciesDev &s, int pusher, 
 void launch_charge_density_f64(const GridDev &g, const SpeciesDev &s, double *rho,
                                cudaStream_t st);
 int diag_blocks();
+void launch_finalize(const double *partials, int nblocks, int nv, double *out, cudaStream_t st);
+void launch_push_deposit_f32(const GridDev &g, const SpeciesF32 &s, int pusher, int n_sm,
+                             int blocks_per_sm, cudaStream_t st);
+void launch_bunch_inject_f32(const SpeciesF32 &s, long long start, long long count, double dl,
+                             double half_dz, double dz, int ncz, float uz,
+                             const double *inv_pow11, cudaStream_t st);
+void launch_charge_density_f32(const GridDev &g, const SpeciesF32 &s, double charge,
+                               double *rho, cudaStream_t st);
+void launch_kinetic_f32(const SpeciesF32 &s, double mass, double *partials, double *out,
+                        cudaStream_t st);
 void launch_grid_diag(const GridDev &g, const double *rho, const double *rho0, double *partials,
                       double *out, cudaStream_t st);
 void launch_rho_norm(const GridDev &g, const double *rho, double *partials, double *out,
