@@ -165,6 +165,28 @@ pdp3g_status pdp3g_set_timing(pdp3g_ctx *ctx, int32_t enabled);
 pdp3g_status pdp3g_get_timing(pdp3g_ctx *ctx, pdp3g_timing *out);
 pdp3g_status pdp3g_reset_timing(pdp3g_ctx *ctx);
 
+/* Allocation-free grid diagnostics, for callers that cannot allocate device
+   memory (code running during CUDA graph capture, hosts whose caching
+   allocator owns all device memory, embedders that forbid cudaMalloc after
+   start-up).  No counterpart in the upstream code.
+   Inputs are device pointers to [n_grid_r][n_grid_z] grids (rho0 may be
+   NULL for a zero initial charge); out is a device pointer to 3 doubles:
+   {field energy, Gauss residual, total charge}, defined as the same fields
+   of pdp3g_diagnostics.  Work goes to `stream` (a cudaStream_t, NULL for the
+   default stream) on the calling thread's current device.
+   Scratch: a static 96 KiB device array (4096 chunks of 4096 nodes) that each
+   GPU loading the library holds until exit; grids above 16,777,216 nodes are
+   rejected with PDP3G_INVALID_ARG.  Every call shares that array and no
+   entry needs clearing (each call overwrites the slots it reads), but calls
+   that overlap on the GPU race on it: serialise them.  The first call on a
+   device looks up the array's device address; make that first call before
+   any stream capture.  Calls no cudaMalloc/cudaFree. */
+pdp3g_status pdp3g_field_diagnostics_noalloc(
+    const double *e_r, const double *e_phi, const double *e_z, const double *h_r,
+    const double *h_phi, const double *h_z, const double *rho, const double *rho0,
+    const double *sigma, int32_t n_grid_r, int32_t n_grid_z, double r_size, double z_size,
+    double *out, void *stream);
+
 /* The CUDA stream (cudaStream_t) every launch of this context goes to, so a
    caller can order its own work or CUDA events against the step. */
 void *pdp3g_stream(pdp3g_ctx *ctx);

@@ -88,6 +88,8 @@ EXPORTS = [
     ("pdp3g_status_string", ctypes.c_char_p, [_I32]),
     ("pdp3g_last_error", ctypes.c_char_p, [_VP]),
     ("pdp3g_device_available", _I32, []),
+    ("pdp3g_field_diagnostics_noalloc", _I32, [_VP] * 9 + [_I32, _I32, ctypes.c_double,
+                                                          ctypes.c_double, _VP, _VP]),
 ]
 
 

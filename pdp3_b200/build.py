@@ -28,6 +28,7 @@ UNITS = {
     "particles_f32.cu": [],
     "sort.cu": [],
     "diag.cu": [],
+    "noalloc.cu": [],
 }
 HEADERS = ["pdp3g_internal.cuh"]
 
