@@ -127,6 +127,26 @@ pdp3g_status pdp3g_add_bunch(pdp3g_ctx *ctx, double charge_e, double mass_me, in
    t += dt.  Asynchronous on the context's stream. */
 pdp3g_status pdp3g_step(pdp3g_ctx *ctx, int32_t nsteps);
 
+/* The phases of pdp3g_step, one per upstream call of the loop body, for
+   hosts that keep the upstream call sequence (asynchronous, context stream):
+     pdp3g_inject        LoadInitParam::init_beam / Bunch::bunch_inject
+                         (src/loadInitParam.cpp:481, src/bunch.cpp:87-124)
+     pdp3g_calc_h        HField::calc_field (src/hField.cpp:93-157)
+     pdp3g_reset_j       Current::reset_j (src/current.cpp:125-135)
+     pdp3g_push_deposit  ParticlesList::step_v + full_current_distribution
+                         (src/particlesList.cpp:20-24, 50-54), fused
+     pdp3g_calc_e        EField::calc_field (src/eField.cpp:85-170)
+     pdp3g_advance_time  t += dt (src/loadInitParam.cpp:586) */
+pdp3g_status pdp3g_inject(pdp3g_ctx *ctx);
+pdp3g_status pdp3g_calc_h(pdp3g_ctx *ctx);
+pdp3g_status pdp3g_reset_j(pdp3g_ctx *ctx);
+pdp3g_status pdp3g_push_deposit(pdp3g_ctx *ctx);
+pdp3g_status pdp3g_calc_e(pdp3g_ctx *ctx);
+pdp3g_status pdp3g_advance_time(pdp3g_ctx *ctx);
+/* Time::current_time assignment (the upstream loop advances it directly,
+   src/loadInitParam.cpp:586); the bunch injection schedule reads it. */
+pdp3g_status pdp3g_set_time(pdp3g_ctx *ctx, double current_time);
+
 /* Stable sort of every plasma species by cell index (an integer LSD radix
    sort of (cell, index) pairs; the permutation equals a stable sort of the
    cell keys).  No upstream counterpart: upstream particles stay in creation

@@ -71,6 +71,13 @@ EXPORTS = [
     ("pdp3g_step", _I32, [_VP, _I32]),
     ("pdp3g_sync", _I32, [_VP]),
     ("pdp3g_sort", _I32, [_VP]),
+    ("pdp3g_inject", _I32, [_VP]),
+    ("pdp3g_calc_h", _I32, [_VP]),
+    ("pdp3g_reset_j", _I32, [_VP]),
+    ("pdp3g_push_deposit", _I32, [_VP]),
+    ("pdp3g_calc_e", _I32, [_VP]),
+    ("pdp3g_advance_time", _I32, [_VP]),
+    ("pdp3g_set_time", _I32, [_VP, ctypes.c_double]),
     ("pdp3g_get_field", _I32, [_VP, _I32, _D]),
     ("pdp3g_set_field", _I32, [_VP, _I32, _D]),
     ("pdp3g_get_species", _I32, [_VP, _I32] + [_D] * 6 + [_U8]),

@@ -532,82 +532,159 @@ pdp3g_status pdp3g_sort(pdp3g_ctx *ctx) {
   return sort_all(ctx);
 }
 
+// ---- the step's phases (LoadInitParam::run, src/loadInitParam.cpp:481-527, 586)
+
+// Bunch::bunch_inject for every bunch (src/bunch.cpp:87-124)
+static void phase_inject(pdp3g_ctx *ctx) {
+  cudaStream_t st = ctx->stream;
+  for (auto &sp : ctx->species) {
+    if (!sp.is_bunch) continue;
+    const double dt = ctx->cfg.dt;
+    double begin = sp.duration * sp.bunch_number + sp.hole_duration * sp.bunch_number;
+    double end = begin + sp.duration;
+    double dl = sp.velocity * dt;
+    int steps_amount = (int)std::ceil(sp.duration / dt);
+    unsigned int number = (unsigned int)(sp.fp32 ? sp.f32.n : sp.dev.n);
+    unsigned int particles_in_step = number / steps_amount;
+    int start_number = (ctx->t - begin) / dt * particles_in_step;
+    if (ctx->t >= begin && ctx->t < end && particles_in_step > 0) {
+      // indices start_number + i for i < particles_in_step, kept below number
+      long long start = (long long)(unsigned int)start_number;
+      long long count = particles_in_step;
+      if (start >= (long long)number) count = 0;
+      else if (start + count > (long long)number) count = (long long)number - start;
+      if (count > 0) {
+        if (sp.fp32) {
+          const double gv = sp.velocity / (LIGHT_SPEED * std::sqrt(1.0 - sp.velocity * sp.velocity /
+                                                                              LIGHT_SPEED_POW_2));
+          launch_bunch_inject_f32(sp.f32, start, count, dl, ctx->dz / 2.0, ctx->dz,
+                                  ctx->cfg.n_grid_z - 1, (float)gv, ctx->d_inv_pow11, st);
+        } else {
+          launch_bunch_inject(sp.dev, start, count, dl, ctx->dz / 2.0, sp.velocity,
+                              ctx->d_inv_pow11, st);
+        }
+        ctx->launches++;
+      }
+    }
+  }
+}
+
+// HField::calc_field (src/hField.cpp:93-157)
+static void phase_calc_h(pdp3g_ctx *ctx) {
+  launch_yee_h(ctx->g, ctx->stream);
+  ctx->launches++;
+}
+
+// Current::reset_j (src/current.cpp:125-135)
+static cudaError_t phase_reset_j(pdp3g_ctx *ctx) {
+  const size_t ng = (size_t)ctx->cfg.n_grid_r * ctx->cfg.n_grid_z;
+  return cudaMemsetAsync(ctx->g.jr, 0, sizeof(double) * ng * 3, ctx->stream);
+}
+
+// ParticlesList::step_v + full_current_distribution (src/particlesList.cpp:20-54)
+static void phase_particles(pdp3g_ctx *ctx) {
+  for (auto &sp : ctx->species) {
+    if (sp.fp32)
+      launch_push_deposit_f32(ctx->g, sp.f32, ctx->cfg.pusher, ctx->n_sm, ctx->f32_blocks_per_sm,
+                              ctx->stream);
+    else
+      launch_push_deposit_f64(ctx->g, sp.dev, ctx->cfg.pusher, ctx->n_sm, ctx->stream);
+    ctx->launches++;
+    ctx->particle_launches++;
+  }
+}
+
+// EField::calc_field (src/eField.cpp:85-170)
+static void phase_calc_e(pdp3g_ctx *ctx) {
+  launch_yee_e(ctx->g, ctx->stream);
+  ctx->launches++;
+}
+
+// t += dt (src/loadInitParam.cpp:586)
+static void phase_advance(pdp3g_ctx *ctx) {
+  ctx->t = ctx->t + ctx->cfg.dt;
+  ctx->steps++;
+}
+
 pdp3g_status pdp3g_step(pdp3g_ctx *ctx, int32_t nsteps) {
   if (!ctx || nsteps < 0) return PDP3G_INVALID_ARG;
   CK(cudaSetDevice(ctx->device));
   cudaStream_t st = ctx->stream;
-  const size_t ng = (size_t)ctx->cfg.n_grid_r * ctx->cfg.n_grid_z;
   for (int s = 0; s < nsteps; s++) {
     StepEvents *ev = ctx->timing ? next_events(ctx) : nullptr;
     if (ev) cudaEventRecord(ev->ev[0], st);
-    // 1. Bunch::bunch_inject for every bunch (src/bunch.cpp:87-124)
-    for (auto &sp : ctx->species) {
-      if (!sp.is_bunch) continue;
-      const double dt = ctx->cfg.dt;
-      double begin = sp.duration * sp.bunch_number + sp.hole_duration * sp.bunch_number;
-      double end = begin + sp.duration;
-      double dl = sp.velocity * dt;
-      int steps_amount = (int)std::ceil(sp.duration / dt);
-      unsigned int number = (unsigned int)(sp.fp32 ? sp.f32.n : sp.dev.n);
-      unsigned int particles_in_step = number / steps_amount;
-      int start_number = (ctx->t - begin) / dt * particles_in_step;
-      if (ctx->t >= begin && ctx->t < end && particles_in_step > 0) {
-        // indices start_number + i for i < particles_in_step, kept below number
-        long long start = (long long)(unsigned int)start_number;
-        long long count = particles_in_step;
-        if (start >= (long long)number) count = 0;
-        else if (start + count > (long long)number) count = (long long)number - start;
-        if (count > 0) {
-          if (sp.fp32) {
-            const double gv = sp.velocity /
-                              (LIGHT_SPEED * std::sqrt(1.0 - sp.velocity * sp.velocity /
-                                                                  LIGHT_SPEED_POW_2));
-            launch_bunch_inject_f32(sp.f32, start, count, dl, ctx->dz / 2.0, ctx->dz,
-                                    ctx->cfg.n_grid_z - 1, (float)gv, ctx->d_inv_pow11, st);
-          } else {
-            launch_bunch_inject(sp.dev, start, count, dl, ctx->dz / 2.0, sp.velocity,
-                                ctx->d_inv_pow11, st);
-          }
-          ctx->launches++;
-        }
-      }
-    }
+    phase_inject(ctx);
     if (ev) cudaEventRecord(ev->ev[1], st);
-    // 2. HField::calc_field
-    launch_yee_h(ctx->g, st);
-    ctx->launches++;
+    phase_calc_h(ctx);
     if (ev) cudaEventRecord(ev->ev[2], st);
-    // 3. Current::reset_j
-    CK(cudaMemsetAsync(ctx->g.jr, 0, sizeof(double) * ng * 3, st));
+    CK(phase_reset_j(ctx));
     if (ctx->cfg.sort_interval > 0 && ctx->steps % ctx->cfg.sort_interval == 0) {
       pdp3g_status ss = sort_all(ctx);
       if (ss != PDP3G_OK) return ss;
     }
     if (ev) cudaEventRecord(ev->ev[3], st);
-    // 4. ParticlesList::step_v + full_current_distribution
-    for (auto &sp : ctx->species) {
-      if (sp.fp32)
-        launch_push_deposit_f32(ctx->g, sp.f32, ctx->cfg.pusher, ctx->n_sm, ctx->f32_blocks_per_sm,
-                                st);
-      else
-        launch_push_deposit_f64(ctx->g, sp.dev, ctx->cfg.pusher, ctx->n_sm, st);
-      ctx->launches++;
-      ctx->particle_launches++;
-    }
+    phase_particles(ctx);
     if (ev) cudaEventRecord(ev->ev[4], st);
-    // 5. EField::calc_field
-    launch_yee_e(ctx->g, st);
-    ctx->launches++;
+    phase_calc_e(ctx);
     if (ev) cudaEventRecord(ev->ev[5], st);
-    // 6. t += dt (src/loadInitParam.cpp:586)
-    ctx->t = ctx->t + ctx->cfg.dt;
-    ctx->steps++;
+    phase_advance(ctx);
     if (ctx->timing && ctx->events_used >= 4096) {
       pdp3g_status hs = harvest_timing(ctx);
       if (hs != PDP3G_OK) return hs;
     }
   }
   CK(cudaGetLastError());
+  return PDP3G_OK;
+}
+
+pdp3g_status pdp3g_inject(pdp3g_ctx *ctx) {
+  if (!ctx) return PDP3G_INVALID_ARG;
+  CK(cudaSetDevice(ctx->device));
+  phase_inject(ctx);
+  CK(cudaGetLastError());
+  return PDP3G_OK;
+}
+
+pdp3g_status pdp3g_calc_h(pdp3g_ctx *ctx) {
+  if (!ctx) return PDP3G_INVALID_ARG;
+  CK(cudaSetDevice(ctx->device));
+  phase_calc_h(ctx);
+  CK(cudaGetLastError());
+  return PDP3G_OK;
+}
+
+pdp3g_status pdp3g_reset_j(pdp3g_ctx *ctx) {
+  if (!ctx) return PDP3G_INVALID_ARG;
+  CK(cudaSetDevice(ctx->device));
+  CK(phase_reset_j(ctx));
+  return PDP3G_OK;
+}
+
+pdp3g_status pdp3g_push_deposit(pdp3g_ctx *ctx) {
+  if (!ctx) return PDP3G_INVALID_ARG;
+  CK(cudaSetDevice(ctx->device));
+  phase_particles(ctx);
+  CK(cudaGetLastError());
+  return PDP3G_OK;
+}
+
+pdp3g_status pdp3g_calc_e(pdp3g_ctx *ctx) {
+  if (!ctx) return PDP3G_INVALID_ARG;
+  CK(cudaSetDevice(ctx->device));
+  phase_calc_e(ctx);
+  CK(cudaGetLastError());
+  return PDP3G_OK;
+}
+
+pdp3g_status pdp3g_set_time(pdp3g_ctx *ctx, double current_time) {
+  if (!ctx || !std::isfinite(current_time)) return PDP3G_INVALID_ARG;
+  ctx->t = current_time;
+  return PDP3G_OK;
+}
+
+pdp3g_status pdp3g_advance_time(pdp3g_ctx *ctx) {
+  if (!ctx) return PDP3G_INVALID_ARG;
+  phase_advance(ctx);
   return PDP3G_OK;
 }
 

@@ -88,59 +88,62 @@ __device__ __forceinline__ float atanh_ratio_m1(float s) {
 
 // One straight piece of the step inside cell (ci, ck), endpoints given as
 // offsets (ao, co) -> (an, cn) relative to that cell (each in [0, 1]).
-__device__ __forceinline__ void deposit_piece(const GridDev &g, const Tile &t, int ci, int ck,
-                                              float ao, float co, float an, float cn, float kz,
-                                              float kr) {
+// out = {j_z(ci, ck), j_z(ci+1, ck), j_r(ci, ck), j_r(ci, ck+1)}.
+__device__ __forceinline__ void piece_values(int ci, float ao, float co, float an, float cn,
+                                             float kz, float kr, float out[4]) {
   const float drho = an - ao, dzeta = cn - co;
   const float fi = (float)ci;
   const float fm = 0.5f * (ao + an);
   const float rho_m = fi + fm;
-  // j_z at (ci, ck) and (ci + 1, ck)
+  const float beta = 1.0f - co;  // ((k+1) dz - z_o)/dz
   if (ci >= 1) {
     const float s = 0.5f * drho / rho_m;
     const float eps = atanh_ratio_m1(s);
     const float ii1 = fi * (fi + 1.0f);
-    const float bz0 = ((1.0f - fm) * (2.0f * fi + fm) + ii1 * eps) / (fi * rho_m);
-    const float bz1 = (fm * (2.0f * fi + 1.0f + fm) - ii1 * eps) / ((fi + 1.0f) * rho_m);
-    dep(g, t, 2, ci, ck, kz * dzeta * bz0);
-    dep(g, t, 2, ci + 1, ck, kz * dzeta * bz1);
+    const float inv_rm = 1.0f / rho_m;
+    out[0] = kz * dzeta * ((1.0f - fm) * (2.0f * fi + fm) + ii1 * eps) * inv_rm / fi;
+    out[1] = kz * dzeta * (fm * (2.0f * fi + 1.0f + fm) - ii1 * eps) * inv_rm / (fi + 1.0f);
     const float rho_o = fi + ao, rho_n = fi + an;
-    const float beta = 1.0f - co;  // ((k+1) dz - z_o)/dz
-    const float inv_on = 1.0f / (rho_o * rho_n);
-    const float q1 = drho * inv_on;
-    const float q2 = dzeta * drho / (2.0f * rho_n * rho_m);
-    const float q3 = dzeta * eps / rho_m;
+    const float q1 = drho / (rho_o * rho_n);
+    const float q2 = dzeta * drho * 0.5f * inv_rm / rho_n;
+    const float q3 = dzeta * eps * inv_rm;
     const float h = 0.5f * ii1;
-    const float tr0 = 0.5f * drho * beta - 0.25f * dzeta * drho + h * (q1 * beta - q2 - q3);
-    const float tr1 = 0.5f * drho * co + 0.25f * dzeta * drho + h * (q1 * co + q2 + q3);
-    const float inv_r0 = 1.0f / (fi + 0.5f);
-    dep(g, t, 0, ci, ck, kr * tr0 * inv_r0);
-    dep(g, t, 0, ci, ck + 1, kr * tr1 * inv_r0);
+    const float inv_r0 = kr / (fi + 0.5f);
+    out[2] = inv_r0 * (0.5f * drho * beta - 0.25f * dzeta * drho + h * (q1 * beta - q2 - q3));
+    out[3] = inv_r0 * (0.5f * drho * co + 0.25f * dzeta * drho + h * (q1 * co + q2 + q3));
   } else {
     // i = 0: src/particles.cpp:415-473 (no log terms; i(i+1) = 0)
-    dep(g, t, 2, 0, ck, 8.0f * kz * dzeta * (1.0f - fm));
-    dep(g, t, 2, 1, ck, kz * dzeta * (1.0f + fm));
-    const float beta = 1.0f - co;
-    const float tr0 = 0.5f * drho * beta - 0.25f * dzeta * drho;
-    const float tr1 = 0.5f * drho * co + 0.25f * dzeta * drho;
-    dep(g, t, 0, 0, ck, 2.0f * kr * tr0);
-    dep(g, t, 0, 0, ck + 1, 2.0f * kr * tr1);
+    out[0] = 8.0f * kz * dzeta * (1.0f - fm);
+    out[1] = kz * dzeta * (1.0f + fm);
+    out[2] = 2.0f * kr * (0.5f * drho * beta - 0.25f * dzeta * drho);
+    out[3] = 2.0f * kr * (0.5f * drho * co + 0.25f * dzeta * drho);
   }
 }
 
+__device__ __forceinline__ void dep_rz(const GridDev &g, const Tile &t, int ci, int ck,
+                                       const float v[4]) {
+  dep(g, t, 2, ci, ck, v[0]);
+  dep(g, t, 2, ci + 1, ck, v[1]);
+  dep(g, t, 0, ci, ck, v[2]);
+  dep(g, t, 0, ci, ck + 1, v[3]);
+}
+
 // The step's straight path from (i, a, k, b) to (in, an, kn, bn) split at the
-// cell faces it crosses (at most one r face and one z face).
-__device__ __forceinline__ void deposit_path(const GridDev &g, const Tile &t, int i, float a,
+// cell faces it crosses (at most one r face and one z face).  The first
+// piece's cell and values are returned (the caller reduces them across the
+// warp); further pieces are deposited directly.  Returns false when the
+// path spans more than one cell in r or z (nothing is deposited, as upstream).
+__device__ __forceinline__ bool deposit_path(const GridDev &g, const Tile &t, int i, float a,
                                              int k, float b, int in, float an, int kn, float bn,
-                                             float kz, float kr) {
+                                             float kz, float kr, int &c0i, int &c0k,
+                                             float first[4]) {
   const int di = in - i, dk = kn - k;
-  if (di < -1 || di > 1 || dk < -1 || dk > 1) return;  // more than one cell: nothing, as upstream
+  if (di < -1 || di > 1 || dk < -1 || dk > 1) return false;
   // end point relative to the start cell
   const float A = (float)di + an, B = (float)dk + bn;
   float tr = 2.0f, tz = 2.0f;
   if (di != 0) tr = ((di > 0 ? 1.0f : 0.0f) - a) / (A - a);
   if (dk != 0) tz = ((dk > 0 ? 1.0f : 0.0f) - b) / (B - b);
-  // pieces in order of t
   float ts[2];
   int kind[2];  // 0: r face, 1: z face
   int np = 0;
@@ -155,6 +158,9 @@ __device__ __forceinline__ void deposit_path(const GridDev &g, const Tile &t, in
   }
   int ci = i, ck = k;
   float pa = a, pb = b;  // current point relative to (i, k)
+  c0i = i;
+  c0k = k;
+#pragma unroll 1
   for (int p = 0; p <= np; p++) {
     float qa, qb;
     if (p < np) {
@@ -172,12 +178,58 @@ __device__ __forceinline__ void deposit_path(const GridDev &g, const Tile &t, in
       qb = B;
     }
     const float oi = (float)(ci - i), ok = (float)(ck - k);
-    deposit_piece(g, t, ci, ck, pa - oi, pb - ok, qa - oi, qb - ok, kz, kr);
+    if (p == 0) {
+      piece_values(ci, pa - oi, pb - ok, qa - oi, qb - ok, kz, kr, first);
+    } else {
+      float v[4];
+      piece_values(ci, pa - oi, pb - ok, qa - oi, qb - ok, kz, kr, v);
+      dep_rz(g, t, ci, ck, v);
+    }
     if (p < np) {
       if (kind[p] == 0) ci += di; else ck += dk;
     }
     pa = qa;
     pb = qb;
+  }
+  return true;
+}
+
+// Warp-level segmented sum of the 4 deposits of each run of consecutive
+// lanes with the same key (particles sorted by cell form long runs); the
+// last lane of a run adds the run's totals.  Lanes with key < 0 hold nothing.
+// node layout: MODE 0 = j_phi at (i,k), (i+1,k), (i,k+1), (i+1,k+1);
+//              MODE 1 = j_z at (i,k), (i+1,k), j_r at (i,k), (i,k+1).
+template <int MODE>
+__device__ __forceinline__ void warp_run_deposit(const GridDev &g, const Tile &t, int key, int i,
+                                                 int k, float v[4]) {
+  const unsigned FULL = 0xffffffffu;
+  const int lane = threadIdx.x & 31;
+  const int prev = __shfl_up_sync(FULL, key, 1);
+  const int next = __shfl_down_sync(FULL, key, 1);
+  const bool head = lane == 0 || prev != key;
+  const bool tail = lane == 31 || next != key;
+  const unsigned heads = __ballot_sync(FULL, head);
+  const unsigned le = lane == 31 ? FULL : ((2u << lane) - 1u);
+  const int seg_start = 31 - __clz(heads & le);
+#pragma unroll
+  for (int j = 0; j < 4; j++) {
+    float x = v[j];
+#pragma unroll
+    for (int off = 1; off < 32; off <<= 1) {
+      const float y = __shfl_up_sync(FULL, x, off);
+      if (lane >= seg_start + off) x += y;
+    }
+    v[j] = x;
+  }
+  if (tail && key >= 0) {
+    if (MODE == 0) {
+      dep(g, t, 1, i, k, v[0]);
+      dep(g, t, 1, i + 1, k, v[1]);
+      dep(g, t, 1, i, k + 1, v[2]);
+      dep(g, t, 1, i + 1, k + 1, v[3]);
+    } else {
+      dep_rz(g, t, i, k, v);
+    }
   }
 }
 
@@ -220,7 +272,7 @@ __device__ __forceinline__ float gather4(const GridDev &g, const double *__restr
   return wz0 * (f00 * wr0 + f10 * wr1) + wz1 * (f01 * wr0 + f11 * wr1);
 }
 
-__global__ void __launch_bounds__(F32_THREADS) k_push_deposit_f32(GridDev g, SpeciesF32 s,
+__global__ void __launch_bounds__(F32_THREADS, 4) k_push_deposit_f32(GridDev g, SpeciesF32 s,
                                                                    int pusher) {
   __shared__ float acc[3 * TILE_CAP];
   __shared__ int red[4][F32_THREADS / 32];
@@ -263,6 +315,9 @@ __global__ void __launch_bounds__(F32_THREADS) k_push_deposit_f32(GridDev g, Spe
     t.nrb = -box[1] - box[0] + 4;
     t.nzb = -box[3] - box[2] + 4;
     t.on = box[0] != INT_MAX && t.nrb * t.nzb <= TILE_CAP;
+    // this lane's j_phi and first r-z piece, reduced across the warp below
+    int key_phi = -1, key_rz = -1, phi_i = 0, phi_k = 0, rz_i = 0, rz_k = 0;
+    float vphi4[4] = {0.f, 0.f, 0.f, 0.f}, vrz4[4] = {0.f, 0.f, 0.f, 0.f};
     if (live) {
       const float a = s.fr[p], b = s.fz[p];
       float u[3] = {s.ur[p], s.uphi[p], s.uz[p]};
@@ -358,10 +413,13 @@ __global__ void __launch_bounds__(F32_THREADS) k_push_deposit_f32(GridDev g, Spe
         const float wa = (1.0f - f1) * (2.0f * fi1 + f1) / (rho1 * v1);
         const float wb = f1 * (2.0f * fi1 + 1.0f + f1) / (rho1 * 2.0f * (fi1 + 1.0f));
         const float pref = s.kphi * w * u[1] * inv_g;
-        dep(g, t, 1, i1, k1, pref * (1.0f - g1) * wa);
-        dep(g, t, 1, i1 + 1, k1, pref * (1.0f - g1) * wb);
-        dep(g, t, 1, i1, k1 + 1, pref * g1 * wa);
-        dep(g, t, 1, i1 + 1, k1 + 1, pref * g1 * wb);
+        vphi4[0] = pref * (1.0f - g1) * wa;
+        vphi4[1] = pref * (1.0f - g1) * wb;
+        vphi4[2] = pref * g1 * wa;
+        vphi4[3] = pref * g1 * wb;
+        phi_i = i1;
+        phi_k = k1;
+        key_phi = i1 * g.nz + k1;
       }
       // ---- second half move, walls, rz rotation (src/particles.cpp:1355-1365)
       float xa2 = a1 + dr_h;
@@ -386,7 +444,8 @@ __global__ void __launch_bounds__(F32_THREADS) k_push_deposit_f32(GridDev g, Spe
       renorm(in, an);
       renorm(kn, bn);
       if (alive_now) {
-        deposit_path(g, t, i, a, k, b, in, an, kn, bn, s.kz * w, s.kr * w);
+        if (deposit_path(g, t, i, a, k, b, in, an, kn, bn, s.kz * w, s.kr * w, rz_i, rz_k, vrz4))
+          key_rz = rz_i * g.nz + rz_k;
         // back_velocity_to_rz (src/particles.cpp:1005-1015): cos = x/r, sin = y/r
         const float inv_r2 = 1.0f / r2;
         const float st = dy * inv_r2, ct = x2 * inv_r2;
@@ -409,6 +468,8 @@ __global__ void __launch_bounds__(F32_THREADS) k_push_deposit_f32(GridDev g, Spe
       s.uphi[p] = u[1];
       s.uz[p] = u[2];
     }
+    warp_run_deposit<0>(g, t, key_phi, phi_i, phi_k, vphi4);
+    warp_run_deposit<1>(g, t, key_rz, rz_i, rz_k, vrz4);
     __syncthreads();
     // ---- flush the tile into the FP64 grid currents
     if (t.on) {
