@@ -13,7 +13,10 @@ relativistic Boris.  Seeded synthetic inputs (no dataset is involved).
 A "step" is one full pass of the loop body: bunch injection, H update, J
 clear, push + deposition of every species, E update.  value is
 particle-steps/s (alive macroparticles x steps / s) over all ranks, with the
-state resident in HBM.  Multi-GPU runs are independent replicas (the path
+state resident in HBM, of the FP32 cell-local form (int cell + FP32 offsets
+and momenta, FP64 grids); the FP64 plain form runs the same workload beside
+it, and both report the Gauss-law residual and energies after the run
+("forms").  Multi-GPU runs are independent replicas (the path
 does not shard: no collective in the data path).  Particle arrays (~3 GB)
 are far larger than L2, so no L2 flush is needed between steps.
 
@@ -121,7 +124,7 @@ def species_bytes(sim, wl, precision):
         total += s.n * b
     if wl.beam is not None:
         n_b = wl.beam.number_macro * wl.beam.number_bunches
-        total += n_b * 1  # alive flags read for every bunch slot
+        total += n_b * 2  # alive flag read (every slot) and written
     return total
 
 
@@ -225,7 +228,8 @@ def main():
     ap.add_argument("--steps", type=int, default=20)
     ap.add_argument("--warmup", type=int, default=3)
     ap.add_argument("--impl", default="ours", choices=["ours", "reference"])
-    ap.add_argument("--precision", default="fp64", choices=["fp64", "fp32"])
+    ap.add_argument("--precision", default="fp32", choices=["fp64", "fp32"],
+                    help="the form reported as value (the other is measured beside it)")
     ap.add_argument("--workload", default="wake", choices=["wake", "thermal"])
     ap.add_argument("--ppc", type=int, default=None,
                     help="macroparticles per cell (profiling runs on a smaller case)")
@@ -254,53 +258,87 @@ def main():
 
     assert args.warmup >= 3, "at least 3 warm-up steps"
     wl = make_workload(args.workload, 1002, args.ppc)
-    sim = api.from_workload(wl, precision=args.precision, device=local_rank)
-    stream = torch.cuda.ExternalStream(sim.stream_ptr, device=torch.device("cuda", local_rank))
-
-    sim.step(args.warmup)
-    sim.sync()
-    if dist is not None:
-        dist.barrier()
-    torch.cuda.synchronize()
-    alive0 = alive_count(sim, wl)
-    sim.reset_timing()
-    sim.set_timing(True)
     clocks = ClockSampler(local_rank)
-    clocks.start()
-    time.sleep(0.3)
-    ev0 = torch.cuda.Event(enable_timing=True)
-    ev1 = torch.cuda.Event(enable_timing=True)
-    ev0.record(stream)
-    sim.step(args.steps)
-    ev1.record(stream)
-    sim.sync()
-    torch.cuda.synchronize()
-    clk = clocks.stop()
-    ms = ev0.elapsed_time(ev1)
-    tm = sim.timing()
-    sim.set_timing(False)
-    alive1 = alive_count(sim, wl)
-    particle_steps = 0.5 * (alive0 + alive1) * args.steps
 
-    if dist is not None:
-        t = torch.tensor([ms, particle_steps], dtype=torch.float64, device="cuda")
-        mx = t.clone()
-        dist.all_reduce(mx, op=dist.ReduceOp.MAX)
-        dist.all_reduce(t, op=dist.ReduceOp.SUM)
-        ms_max = float(mx[0])
-        total_ps = float(t[1])
-    else:
-        ms_max = ms
-        total_ps = particle_steps
-    value = total_ps / (ms_max / 1000.0)
+    def measure(precision, sample_clocks):
+        """W warm-up + K timed steps of one form; timing with CUDA events on
+        the library's stream, max over ranks."""
+        sim = api.from_workload(wl, precision=precision, device=local_rank)
+        sim.mark_initial_charge()
+        stream = torch.cuda.ExternalStream(sim.stream_ptr,
+                                           device=torch.device("cuda", local_rank))
+        sim.step(args.warmup)
+        sim.sync()
+        if dist is not None:
+            dist.barrier()
+        torch.cuda.synchronize()
+        alive0 = alive_count(sim, wl)
+        sim.reset_timing()
+        sim.set_timing(True)
+        if sample_clocks:
+            clocks.start()
+            time.sleep(0.3)
+        ev0 = torch.cuda.Event(enable_timing=True)
+        ev1 = torch.cuda.Event(enable_timing=True)
+        ev0.record(stream)
+        sim.step(args.steps)
+        ev1.record(stream)
+        sim.sync()
+        torch.cuda.synchronize()
+        clk = clocks.stop() if sample_clocks else None
+        ms = ev0.elapsed_time(ev1)
+        tm = sim.timing()
+        sim.set_timing(False)
+        alive1 = alive_count(sim, wl)
+        particle_steps = 0.5 * (alive0 + alive1) * args.steps
+        if dist is not None:
+            t = torch.tensor([ms, particle_steps], dtype=torch.float64, device="cuda")
+            mx = t.clone()
+            dist.all_reduce(mx, op=dist.ReduceOp.MAX)
+            dist.all_reduce(t, op=dist.ReduceOp.SUM)
+            ms_max, total_ps = float(mx[0]), float(t[1])
+        else:
+            ms_max, total_ps = ms, particle_steps
+        diag = sim.diagnostics()
+        return sim, stream, {"ms": ms_max, "value": total_ps / (ms_max / 1000.0), "tm": tm,
+                             "clk": clk, "diag": diag}
+
+    # headline: the FP32 cell-local form; the FP64 plain form beside it
+    head_prec = args.precision
+    other_prec = "fp64" if head_prec == "fp32" else "fp32"
+    sim_o, _, res_o = measure(other_prec, False)
+    sim_o.close()
+    del sim_o
+    sim, stream, res = measure(head_prec, True)
+    value, ms_max, tm, clk = res["value"], res["ms"], res["tm"], res["clk"]
 
     # roofline of the dominant kernel (the fused push + deposition)
     peaks, peak_src = load_peaks()
-    bytes_particle_phase = species_bytes(sim, wl, args.precision)
+    bytes_particle_phase = species_bytes(sim, wl, head_prec)
     ms_part = tm["ms_particles"] / max(tm["steps"], 1)
     achieved = bytes_particle_phase / (ms_part / 1000.0) / 1e9
     n_nodes = wl.n_grid_r * wl.n_grid_z
     ms_fields = tm["ms_fields"] / max(tm["steps"], 1)
+
+    def gauss_rel(d):
+        return d["gauss_residual"] / d["gauss_norm"] if d["gauss_norm"] > 0 else None
+
+    d32 = res["diag"] if head_prec == "fp32" else res_o["diag"]
+    d64 = res_o["diag"] if head_prec == "fp32" else res["diag"]
+    v32 = res["value"] if head_prec == "fp32" else res_o["value"]
+    v64 = res_o["value"] if head_prec == "fp32" else res["value"]
+    forms = {
+        "fp32_cell_local": {"value": v32, "gauss_rel_residual": gauss_rel(d32),
+                            "field_energy_J": d32["field_energy"],
+                            "kinetic_energy_J": d32["kinetic_energy"]},
+        "fp64_plain": {"value": v64, "gauss_rel_residual": gauss_rel(d64),
+                       "field_energy_J": d64["field_energy"],
+                       "kinetic_energy_J": d64["kinetic_energy"]},
+        "fp32_over_fp64": v32 / v64,
+        "field_energy_rel_diff": abs(d32["field_energy"] - d64["field_energy"]) /
+        d64["field_energy"] if d64["field_energy"] > 0 else None,
+        "after_steps": args.warmup + args.steps,
+    }
 
     # end to end through the public API from pinned host buffers: every step
     # uploads the particle state, steps, and reads the state and E_z back.
@@ -318,26 +356,28 @@ def main():
             cpu = {"value": None, "unit": UNIT, "cores": None, "kind": None,
                    "sample": "failed: %s" % exc}
 
-    traffic = load_traffic(args.workload, args.precision, wl)
+    traffic = load_traffic(args.workload, head_prec, wl)
     if rank == 0:
         line = {
             "metric": METRIC, "value": value, "unit": UNIT, "n_gpus": world,
             "steps": args.steps, "warmup": args.warmup, "ms_per_step": ms_max / args.steps,
             "higher_is_better": True, "scaling": "weak", "vs_baseline": None,
-            "dtype": "f64" if args.precision == "fp64" else "f32+f64acc",
+            "dtype": "f64" if head_prec == "fp64" else "f32+f64acc",
             "data": "synthetic (seeded)",
             "config": {"workload": wl.name, "n_grid_r": wl.n_grid_r, "n_grid_z": wl.n_grid_z,
                        "particles": wl.n_particles, "pusher": wl.pusher,
-                       "precision": args.precision, "parallelism": "replicas x%d" % world,
+                       "precision": head_prec, "parallelism": "replicas x%d" % world,
                        "l2": "inputs larger than L2 (particle state %.2f GB)"
                              % (bytes_particle_phase / 1e9)},
+            "forms": forms,
             "cell_updates_per_s": n_nodes / (ms_fields / 1000.0) if ms_fields > 0 else None,
             "cell_updates_per_s_step": n_nodes * args.steps * world / (ms_max / 1000.0),
             "kernel_ms": {"particles": ms_part, "fields": ms_fields,
                           "other": tm["ms_other"] / max(tm["steps"], 1)},
             "roofline": {"bound": "hbm", "achieved": achieved, "peak": peaks.get("hbm_gbs"),
                          "unit": "GB/s", "frac": achieved / peaks.get("hbm_gbs"),
-                         "traffic": traffic, "kernel": "push_deposit (all species)",
+                         "traffic": traffic,
+                         "kernel": "k_push_deposit_%s (all species)" % head_prec[-2:],
                          "peak_source": peak_src,
                          "algorithmic_bytes_per_launch": bytes_particle_phase},
             "e2e": e2e,

@@ -207,6 +207,35 @@ pdp3g_status pdp3g_field_diagnostics_noalloc(
     const double *sigma, int32_t n_grid_r, int32_t n_grid_z, double r_size, double z_size,
     double *out, void *stream);
 
+/* ---- Batched ensemble (no upstream counterpart: the upstream runs one
+   simulation per process).  Independent runs, each a context created with
+   precision PDP3G_FP32_CELL on the same device (different grids, species
+   and bunches allowed), are advanced together by one persistent cooperative
+   kernel per pdp3g_ensemble_run call, replayed from a captured CUDA graph
+   (a direct cooperative launch if the capture is refused).  Each run's
+   state stays in its context (pdp3g_get_field etc. work as usual).  The
+   kernel checks a host-mapped cancel flag and a time budget once per step
+   and returns PDP3G_TIMEOUT when either stops it; the steps done are
+   reported by pdp3g_ensemble_info and added to every run's time. */
+typedef struct pdp3g_ensemble pdp3g_ensemble;
+typedef struct {
+  int32_t runs, blocks_per_sm, blocks, used_graph;
+  double last_ms;            /* device time of the last run call */
+  int64_t last_steps_done;
+  int64_t particles;         /* macroparticle slots over all runs */
+} pdp3g_ensemble_stats;
+pdp3g_status pdp3g_ensemble_create(pdp3g_ctx *const *runs, int32_t n_runs, pdp3g_ensemble **out);
+pdp3g_status pdp3g_ensemble_run(pdp3g_ensemble *e, int32_t nsteps);
+/* tries every feasible CTAs-per-SM count for steps_per_trial steps each (the
+   trial steps advance the runs) and keeps the fastest */
+pdp3g_status pdp3g_ensemble_autotune(pdp3g_ensemble *e, int32_t steps_per_trial,
+                                     int32_t *blocks_per_sm);
+pdp3g_status pdp3g_ensemble_set_budget(pdp3g_ensemble *e, double max_ms);  /* 0: none */
+pdp3g_status pdp3g_ensemble_cancel(pdp3g_ensemble *e, int32_t cancel);     /* any thread */
+pdp3g_status pdp3g_ensemble_info(pdp3g_ensemble *e, pdp3g_ensemble_stats *out);
+const char *pdp3g_ensemble_last_error(pdp3g_ensemble *e);
+void pdp3g_ensemble_destroy(pdp3g_ensemble *e);
+
 /* The CUDA stream (cudaStream_t) every launch of this context goes to, so a
    caller can order its own work or CUDA events against the step. */
 void *pdp3g_stream(pdp3g_ctx *ctx);

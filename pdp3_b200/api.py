@@ -46,6 +46,13 @@ class Diag(ctypes.Structure):
                 ("charge_total", ctypes.c_double), ("alive", ctypes.c_int64)]
 
 
+class EnsembleInfo(ctypes.Structure):
+    _fields_ = [("runs", ctypes.c_int32), ("blocks_per_sm", ctypes.c_int32),
+                ("blocks", ctypes.c_int32), ("used_graph", ctypes.c_int32),
+                ("last_ms", ctypes.c_double), ("last_steps_done", ctypes.c_int64),
+                ("particles", ctypes.c_int64)]
+
+
 class Timing(ctypes.Structure):
     _fields_ = [("ms_step_total", ctypes.c_double), ("ms_particles", ctypes.c_double),
                 ("ms_fields", ctypes.c_double), ("ms_sort", ctypes.c_double),
@@ -95,6 +102,14 @@ EXPORTS = [
     ("pdp3g_status_string", ctypes.c_char_p, [_I32]),
     ("pdp3g_last_error", ctypes.c_char_p, [_VP]),
     ("pdp3g_device_available", _I32, []),
+    ("pdp3g_ensemble_create", _I32, [ctypes.POINTER(_VP), _I32, ctypes.POINTER(_VP)]),
+    ("pdp3g_ensemble_run", _I32, [_VP, _I32]),
+    ("pdp3g_ensemble_autotune", _I32, [_VP, _I32, ctypes.POINTER(_I32)]),
+    ("pdp3g_ensemble_set_budget", _I32, [_VP, ctypes.c_double]),
+    ("pdp3g_ensemble_cancel", _I32, [_VP, _I32]),
+    ("pdp3g_ensemble_info", _I32, [_VP, ctypes.POINTER(EnsembleInfo)]),
+    ("pdp3g_ensemble_last_error", ctypes.c_char_p, [_VP]),
+    ("pdp3g_ensemble_destroy", None, [_VP]),
     ("pdp3g_field_diagnostics_noalloc", _I32, [_VP] * 9 + [_I32, _I32, ctypes.c_double,
                                                           ctypes.c_double, _VP, _VP]),
 ]
@@ -271,3 +286,57 @@ def from_workload(wl, precision="fp64", device=0, pusher=None, sort_interval=0):
             sim.add_bunch(b.charge_e, b.mass_me, b.number_macro, b.bunch_length / b.velocity,
                           b.radius, b.density, b.velocity, nb, b.bunches_distance / b.velocity)
     return sim
+
+
+class Ensemble:
+    """Independent FP32 runs advanced together by one persistent kernel."""
+
+    def __init__(self, sims):
+        self.L = load()
+        self.sims = list(sims)
+        arr = (_VP * len(self.sims))(*[s.h for s in self.sims])
+        h = _VP()
+        st = self.L.pdp3g_ensemble_create(arr, len(self.sims), ctypes.byref(h))
+        if st != 0:
+            msg = self.L.pdp3g_last_error(self.sims[0].h)
+            raise Pdp3gError(st, "ensemble_create: %s" % (msg.decode() if msg else ""))
+        self.h = h
+
+    def _check(self, st, what):
+        if st != 0:
+            msg = self.L.pdp3g_ensemble_last_error(self.h)
+            raise Pdp3gError(st, "%s: %s" % (what, msg.decode() if msg else ""))
+
+    def run(self, nsteps):
+        self._check(self.L.pdp3g_ensemble_run(self.h, int(nsteps)), "ensemble_run")
+
+    def run_status(self, nsteps):
+        return self.L.pdp3g_ensemble_run(self.h, int(nsteps))
+
+    def autotune(self, steps_per_trial=2):
+        b = _I32()
+        self._check(self.L.pdp3g_ensemble_autotune(self.h, int(steps_per_trial), ctypes.byref(b)),
+                    "ensemble_autotune")
+        return b.value
+
+    def set_budget(self, max_ms):
+        self._check(self.L.pdp3g_ensemble_set_budget(self.h, float(max_ms)), "set_budget")
+
+    def cancel(self, on=True):
+        self._check(self.L.pdp3g_ensemble_cancel(self.h, 1 if on else 0), "cancel")
+
+    def info(self):
+        i = EnsembleInfo()
+        self._check(self.L.pdp3g_ensemble_info(self.h, ctypes.byref(i)), "ensemble_info")
+        return {f: getattr(i, f) for f, _ in EnsembleInfo._fields_}
+
+    def close(self):
+        if getattr(self, "h", None):
+            self.L.pdp3g_ensemble_destroy(self.h)
+            self.h = None
+
+    def __del__(self):
+        try:
+            self.close()
+        except Exception:
+            pass

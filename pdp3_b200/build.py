@@ -29,10 +29,11 @@ UNITS = {
     # budget is set by FP32 storage, not by these operations
     "particles_f32.cu": ["--prec-div=false", "--prec-sqrt=false"],
     "sort.cu": [],
+    "ensemble.cu": ["--prec-div=false", "--prec-sqrt=false"],
     "diag.cu": [],
     "noalloc.cu": [],
 }
-HEADERS = ["pdp3g_internal.cuh"]
+HEADERS = ["pdp3g_internal.cuh", "particles_f32.cuh", "fields_body.cuh"]
 
 
 def nvcc():

@@ -50,6 +50,8 @@ struct pdp3g_ctx {
   double *d_partials = nullptr;  // per-block reduction partials
   double *d_red = nullptr;       // reduction results
   char *d_sort = nullptr;        // radix-sort scratch
+  double *d_stage = nullptr;     // FP64 staging for the cell-local layout's conversions
+  size_t stage_n = 0;
   size_t sort_bytes = 0;
   int64_t sorts = 0;
   size_t scratch_bytes = 0;
@@ -305,6 +307,7 @@ void pdp3g_destroy(pdp3g_ctx *ctx) {
   cudaFree(ctx->d_partials);
   cudaFree(ctx->d_red);
   cudaFree(ctx->d_sort);
+  cudaFree(ctx->d_stage);
   if (ctx->stream) cudaStreamDestroy(ctx->stream);
   delete ctx;
 }
@@ -320,35 +323,6 @@ static pdp3g_status alloc_species(pdp3g_ctx *ctx, Species &sp, int64_t n, bool w
   sp.dev.w = w;
   if (with_alive) CK(dalloc(ctx, &sp.dev.alive, n));
   sp.dev.n = n;
-  return PDP3G_OK;
-}
-
-// FP64 (r, z, v) -> cell-local FP32 (cell, offsets, u = gamma v / c)
-static pdp3g_status to_cell_local(pdp3g_ctx *ctx, int64_t n, const double *r, const double *z,
-                                  const double *vr, const double *vphi, const double *vz,
-                                  std::vector<int> &cell, std::vector<float> &fr,
-                                  std::vector<float> &fz, std::vector<float> &ur,
-                                  std::vector<float> &uphi, std::vector<float> &uz) {
-  const int nr = ctx->cfg.n_grid_r, nz = ctx->cfg.n_grid_z, ncz = nz - 1;
-  const double dr = ctx->dr, dz = ctx->dz;
-  cell.resize(n); fr.resize(n); fz.resize(n); ur.resize(n); uphi.resize(n); uz.resize(n);
-  for (int64_t p = 0; p < n; p++) {
-    if (!std::isfinite(r[p]) || !std::isfinite(z[p]))
-      return fail(ctx, PDP3G_NAN_DETECTED, "particle position is NaN or Inf");
-    int i = (int)std::ceil(r[p] / dr) - 1, k = (int)std::ceil(z[p] / dz) - 1;
-    if (i < 0) i = 0;
-    if (k < 0) k = 0;
-    if (i > nr - 2 || k > nz - 2) return fail(ctx, PDP3G_OUT_OF_GRID, "particle outside the grid");
-    cell[p] = i * ncz + k;
-    fr[p] = (float)(r[p] / dr - i);
-    fz[p] = (float)(z[p] / dz - k);
-    const double v2 = vr[p] * vr[p] + vphi[p] * vphi[p] + vz[p] * vz[p];
-    if (!(v2 < LIGHT_SPEED_POW_2)) return fail(ctx, PDP3G_V_GE_C, "velocity >= c");
-    const double gc = 1.0 / (LIGHT_SPEED * std::sqrt(1.0 - v2 / LIGHT_SPEED_POW_2));
-    ur[p] = (float)(vr[p] * gc);
-    uphi[p] = (float)(vphi[p] * gc);
-    uz[p] = (float)(vz[p] * gc);
-  }
   return PDP3G_OK;
 }
 
@@ -369,22 +343,50 @@ static void f32_constants(pdp3g_ctx *ctx, Species &sp) {
   f.inv_c2 = (float)(1.0 / LIGHT_SPEED_POW_2);
 }
 
+static pdp3g_status stage_reserve(pdp3g_ctx *ctx, size_t n) {
+  if (ctx->stage_n >= n) return PDP3G_OK;
+  cudaFree(ctx->d_stage);
+  ctx->d_stage = nullptr;
+  ctx->stage_n = 0;
+  CK(dalloc(ctx, &ctx->d_stage, 6 * n));
+  ctx->stage_n = n;
+  return PDP3G_OK;
+}
+
+// converts the FP64 arrays already in the staging buffer (r, z, vr, vphi, vz
+// and, if with_w, w at slots 0..5) into the species' cell-local arrays
+static pdp3g_status convert_staged_f32(pdp3g_ctx *ctx, Species &sp, bool with_w) {
+  const size_t n = (size_t)sp.f32.n;
+  double *S = ctx->d_stage;
+  CK(cudaMemsetAsync(ctx->d_err + 1, 0, sizeof(unsigned), ctx->stream));
+  launch_f64_to_cell(sp.f32, S, S + n, S + 2 * n, S + 3 * n, S + 4 * n, with_w ? S + 5 * n : nullptr,
+                     ctx->dr, ctx->dz, ctx->cfg.n_grid_r, ctx->cfg.n_grid_z, ctx->d_err + 1,
+                     ctx->stream);
+  ctx->launches++;
+  unsigned err = 0;
+  CK(cudaMemcpyAsync(&err, ctx->d_err + 1, sizeof(unsigned), cudaMemcpyDeviceToHost, ctx->stream));
+  CK(cudaStreamSynchronize(ctx->stream));
+  if (err & ERR_NAN) return fail(ctx, PDP3G_NAN_DETECTED, "particle position is NaN or Inf");
+  if (err & ERR_V_GE_C) return fail(ctx, PDP3G_V_GE_C, "velocity >= c");
+  if (err & ERR_OUT_OF_GRID) return fail(ctx, PDP3G_OUT_OF_GRID, "particle outside the grid");
+  return PDP3G_OK;
+}
+
 static pdp3g_status upload_f32(pdp3g_ctx *ctx, Species &sp, int64_t n, const double *r,
                                const double *z, const double *vr, const double *vphi,
-                               const double *vz) {
-  std::vector<int> cell;
-  std::vector<float> fr, fz, ur, uphi, uz;
-  pdp3g_status st = to_cell_local(ctx, n, r, z, vr, vphi, vz, cell, fr, fz, ur, uphi, uz);
+                               const double *vz, const double *w) {
+  pdp3g_status st = stage_reserve(ctx, (size_t)n);
   if (st != PDP3G_OK) return st;
-  SpeciesF32 &f = sp.f32;
-  size_t b = sizeof(float) * (size_t)n;
-  CK(cudaMemcpy(f.cell, cell.data(), sizeof(int) * (size_t)n, cudaMemcpyHostToDevice));
-  CK(cudaMemcpy(f.fr, fr.data(), b, cudaMemcpyHostToDevice));
-  CK(cudaMemcpy(f.fz, fz.data(), b, cudaMemcpyHostToDevice));
-  CK(cudaMemcpy(f.ur, ur.data(), b, cudaMemcpyHostToDevice));
-  CK(cudaMemcpy(f.uphi, uphi.data(), b, cudaMemcpyHostToDevice));
-  CK(cudaMemcpy(f.uz, uz.data(), b, cudaMemcpyHostToDevice));
-  return PDP3G_OK;
+  double *S = ctx->d_stage;
+  const size_t b = sizeof(double) * (size_t)n;
+  cudaStream_t s = ctx->stream;
+  CK(cudaMemcpyAsync(S, r, b, cudaMemcpyHostToDevice, s));
+  CK(cudaMemcpyAsync(S + n, z, b, cudaMemcpyHostToDevice, s));
+  CK(cudaMemcpyAsync(S + 2 * n, vr, b, cudaMemcpyHostToDevice, s));
+  CK(cudaMemcpyAsync(S + 3 * n, vphi, b, cudaMemcpyHostToDevice, s));
+  CK(cudaMemcpyAsync(S + 4 * n, vz, b, cudaMemcpyHostToDevice, s));
+  if (w) CK(cudaMemcpyAsync(S + 5 * n, w, b, cudaMemcpyHostToDevice, s));
+  return convert_staged_f32(ctx, sp, w != nullptr);
 }
 
 pdp3g_status pdp3g_add_species(pdp3g_ctx *ctx, double charge_e, double mass_me, int64_t n,
@@ -413,10 +415,8 @@ pdp3g_status pdp3g_add_species(pdp3g_ctx *ctx, double charge_e, double mass_me, 
     float *wf = nullptr;
     CK(dalloc(ctx, &wf, (size_t)n));
     f.w = wf;
-    pdp3g_status st = upload_f32(ctx, sp, n, r, z, vr, vphi, vz);
+    pdp3g_status st = upload_f32(ctx, sp, n, r, z, vr, vphi, vz, w);
     if (st != PDP3G_OK) return st;
-    std::vector<float> wv(w, w + n);
-    CK(cudaMemcpy(wf, wv.data(), sizeof(float) * (size_t)n, cudaMemcpyHostToDevice));
     if (alive) {
       CK(dalloc(ctx, &f.alive, (size_t)n));
       CK(cudaMemcpy(f.alive, alive, (size_t)n, cudaMemcpyHostToDevice));
@@ -729,15 +729,16 @@ pdp3g_status pdp3g_get_species(pdp3g_ctx *ctx, int32_t id, double *r, double *z,
   if (sp.fp32) {
     const SpeciesF32 &f = sp.f32;
     const size_t n = (size_t)f.n;
-    std::vector<int> cell(n);
-    std::vector<float> fr(n), fz(n), ur(n), uphi(n), uz(n), wf(n);
-    CK(cudaMemcpyAsync(cell.data(), f.cell, sizeof(int) * n, cudaMemcpyDeviceToHost, st));
-    CK(cudaMemcpyAsync(fr.data(), f.fr, sizeof(float) * n, cudaMemcpyDeviceToHost, st));
-    CK(cudaMemcpyAsync(fz.data(), f.fz, sizeof(float) * n, cudaMemcpyDeviceToHost, st));
-    CK(cudaMemcpyAsync(ur.data(), f.ur, sizeof(float) * n, cudaMemcpyDeviceToHost, st));
-    CK(cudaMemcpyAsync(uphi.data(), f.uphi, sizeof(float) * n, cudaMemcpyDeviceToHost, st));
-    CK(cudaMemcpyAsync(uz.data(), f.uz, sizeof(float) * n, cudaMemcpyDeviceToHost, st));
-    CK(cudaMemcpyAsync(wf.data(), f.w, sizeof(float) * n, cudaMemcpyDeviceToHost, st));
+    pdp3g_status rs = stage_reserve(ctx, n);
+    if (rs != PDP3G_OK) return rs;
+    double *S = ctx->d_stage;
+    launch_cell_to_f64(f, ctx->dr, ctx->dz, ctx->cfg.n_grid_z - 1, S, S + n, S + 2 * n, S + 3 * n,
+                       S + 4 * n, w ? S + 5 * n : nullptr, st);
+    ctx->launches++;
+    const size_t b = sizeof(double) * n;
+    double *outs[6] = {r, z, vr, vphi, vz, w};
+    for (int j = 0; j < 6; j++)
+      if (outs[j]) CK(cudaMemcpyAsync(outs[j], S + j * n, b, cudaMemcpyDeviceToHost, st));
     if (alive) {
       if (f.alive)
         CK(cudaMemcpyAsync(alive, f.alive, n, cudaMemcpyDeviceToHost, st));
@@ -745,18 +746,6 @@ pdp3g_status pdp3g_get_species(pdp3g_ctx *ctx, int32_t id, double *r, double *z,
         memset(alive, 1, n);
     }
     CK(cudaStreamSynchronize(st));
-    const int ncz = ctx->cfg.n_grid_z - 1;
-    for (size_t p = 0; p < n; p++) {
-      const int i = cell[p] / ncz, k = cell[p] - (cell[p] / ncz) * ncz;
-      if (r) r[p] = (i + (double)fr[p]) * ctx->dr;
-      if (z) z[p] = (k + (double)fz[p]) * ctx->dz;
-      const double u2 = (double)ur[p] * ur[p] + (double)uphi[p] * uphi[p] + (double)uz[p] * uz[p];
-      const double c_over_g = LIGHT_SPEED / std::sqrt(1.0 + u2);
-      if (vr) vr[p] = ur[p] * c_over_g;
-      if (vphi) vphi[p] = uphi[p] * c_over_g;
-      if (vz) vz[p] = uz[p] * c_over_g;
-      if (w) w[p] = wf[p];
-    }
     return PDP3G_OK;
   }
   const SpeciesDev &d = sp.dev;
@@ -784,23 +773,29 @@ pdp3g_status pdp3g_set_species(pdp3g_ctx *ctx, int32_t id, const double *r, cons
   CK(cudaSetDevice(ctx->device));
   Species &sp = ctx->species[id];
   if (sp.fp32) {
-    // the cell index packs r and z: rebuild the full FP64 state, replace the
-    // given arrays and convert back
+    // the cell index packs r and z: rebuild the full FP64 state on the
+    // device, replace the given arrays and convert back
     const size_t n = (size_t)sp.f32.n;
-    std::vector<double> R(n), Z(n), VR(n), VP(n), VZ(n);
-    pdp3g_status gs = pdp3g_get_species(ctx, id, R.data(), Z.data(), VR.data(), VP.data(),
-                                        VZ.data(), nullptr, nullptr);
-    if (gs != PDP3G_OK) return gs;
-    if (r) memcpy(R.data(), r, n * sizeof(double));
-    if (z) memcpy(Z.data(), z, n * sizeof(double));
-    if (vr) memcpy(VR.data(), vr, n * sizeof(double));
-    if (vphi) memcpy(VP.data(), vphi, n * sizeof(double));
-    if (vz) memcpy(VZ.data(), vz, n * sizeof(double));
-    gs = upload_f32(ctx, sp, (int64_t)n, R.data(), Z.data(), VR.data(), VP.data(), VZ.data());
-    if (gs != PDP3G_OK) return gs;
+    pdp3g_status rs = stage_reserve(ctx, n);
+    if (rs != PDP3G_OK) return rs;
+    double *S = ctx->d_stage;
+    cudaStream_t st = ctx->stream;
+    const double *ins[5] = {r, z, vr, vphi, vz};
+    if (!(r && z && vr && vphi && vz)) {
+      launch_cell_to_f64(sp.f32, ctx->dr, ctx->dz, ctx->cfg.n_grid_z - 1, S, S + n, S + 2 * n,
+                         S + 3 * n, S + 4 * n, nullptr, st);
+      ctx->launches++;
+    }
+    for (int j = 0; j < 5; j++)
+      if (ins[j]) CK(cudaMemcpyAsync(S + j * n, ins[j], sizeof(double) * n, cudaMemcpyHostToDevice, st));
+    if (r || z || vr || vphi || vz) {
+      rs = convert_staged_f32(ctx, sp, false);
+      if (rs != PDP3G_OK) return rs;
+    }
     if (alive) {
       if (!sp.f32.alive) CK(dalloc(ctx, &sp.f32.alive, n));
-      CK(cudaMemcpy(sp.f32.alive, alive, n, cudaMemcpyHostToDevice));
+      CK(cudaMemcpyAsync(sp.f32.alive, alive, n, cudaMemcpyHostToDevice, st));
+      CK(cudaStreamSynchronize(st));
     }
     return PDP3G_OK;
   }
@@ -943,5 +938,278 @@ pdp3g_status pdp3g_get_timing(pdp3g_ctx *ctx, pdp3g_timing *out) {
 double pdp3g_current_time(pdp3g_ctx *ctx) { return ctx ? ctx->t : 0.0; }
 void *pdp3g_stream(pdp3g_ctx *ctx) { return ctx ? (void *)ctx->stream : nullptr; }
 int64_t pdp3g_device_bytes(pdp3g_ctx *ctx) { return ctx ? ctx->bytes : 0; }
+
+
+// ------------------------------------------------------------ batched ensemble
+
+struct pdp3g_ensemble {
+  std::vector<pdp3g_ctx *> runs;
+  int device = 0;
+  int n_sm = 148;
+  cudaStream_t stream = nullptr;
+  EnsRun *d_runs = nullptr;
+  EnsSpecies *d_species = nullptr;
+  int *d_status = nullptr;
+  int *h_cancel = nullptr;  // host-mapped
+  int *d_cancel = nullptr;
+  EnsembleDev dev{};
+  std::vector<EnsRun> h_runs;
+  int blocks_per_sm = 0;
+  int max_blocks_per_sm = 0;
+  double budget_ms = 0;
+  long long clock_khz = 0;
+  cudaGraph_t graph = nullptr;
+  cudaGraphExec_t exec = nullptr;
+  int graph_steps = -1, graph_blocks = -1;
+  bool graph_ok = true;
+  bool last_used_graph = false;
+  double last_ms = 0;
+  int64_t last_steps_done = 0;
+  int64_t total_particles = 0;
+  std::string last_error;
+};
+
+static pdp3g_status ens_fail(pdp3g_ensemble *e, pdp3g_status st, const std::string &m) {
+  if (e) e->last_error = m;
+  return st;
+}
+
+#define EK(call)                                                                  \
+  do {                                                                            \
+    cudaError_t _e = (call);                                                      \
+    if (_e != cudaSuccess)                                                        \
+      return ens_fail(e, _e == cudaErrorMemoryAllocation ? PDP3G_NO_MEMORY : PDP3G_CUDA_ERROR, \
+                      std::string(#call) + ": " + cudaGetErrorString(_e));      \
+  } while (0)
+
+void pdp3g_ensemble_destroy(pdp3g_ensemble *e) {
+  if (!e) return;
+  cudaSetDevice(e->device);
+  if (e->stream) cudaStreamSynchronize(e->stream);
+  if (e->exec) cudaGraphExecDestroy(e->exec);
+  if (e->graph) cudaGraphDestroy(e->graph);
+  cudaFree(e->d_runs);
+  cudaFree(e->d_species);
+  cudaFree(e->d_status);
+  if (e->h_cancel) cudaFreeHost(e->h_cancel);
+  if (e->stream) cudaStreamDestroy(e->stream);
+  delete e;
+}
+
+pdp3g_status pdp3g_ensemble_create(pdp3g_ctx *const *runs, int32_t n_runs, pdp3g_ensemble **out) {
+  if (!runs || n_runs <= 0 || !out) return PDP3G_INVALID_ARG;
+  *out = nullptr;
+  pdp3g_ensemble *e = new pdp3g_ensemble();
+  e->device = runs[0]->device;
+  auto bail = [&](pdp3g_status st, const std::string &m) {
+    if (runs[0]) runs[0]->last_error = m;
+    pdp3g_ensemble_destroy(e);
+    return st;
+  };
+  std::vector<EnsSpecies> hs;
+  long long h = 0, ee = 0, j = 0, ch = 0;
+  for (int r = 0; r < n_runs; r++) {
+    pdp3g_ctx *c = runs[r];
+    if (!c || c->device != e->device)
+      return bail(PDP3G_INVALID_ARG, "ensemble runs must share one device");
+    if (c->cfg.precision != PDP3G_FP32_CELL)
+      return bail(PDP3G_NOT_SUPPORTED, "ensemble runs use the FP32 cell-local form");
+    e->runs.push_back(c);
+    EnsRun er{};
+    er.g = c->g;
+    er.t = c->t;
+    er.pusher = c->cfg.pusher;
+    er.h_begin = h;
+    er.e_begin = ee;
+    er.j_begin = j;
+    er.chunk_begin = ch;
+    h += (long long)c->g.nr * (c->g.nz - 1);
+    ee += (long long)(c->g.nr - 1) * (c->g.nz - 1);
+    j += (long long)c->g.nr * c->g.nz;
+    for (auto &sp : c->species) {
+      EnsSpecies es{};
+      es.s = sp.f32;
+      es.run = r;
+      es.chunk_begin = ch;
+      es.is_bunch = sp.is_bunch ? 1 : 0;
+      es.duration = sp.duration;
+      es.bunch_number = sp.bunch_number;
+      es.hole_duration = sp.hole_duration;
+      es.velocity = sp.velocity;
+      if (sp.is_bunch)
+        es.uz_beam = (float)(sp.velocity / (LIGHT_SPEED * std::sqrt(1.0 - sp.velocity * sp.velocity /
+                                                                           LIGHT_SPEED_POW_2)));
+      ch += (sp.f32.n + 255) / 256;
+      e->total_particles += sp.f32.n;
+      hs.push_back(es);
+    }
+    e->h_runs.push_back(er);
+  }
+  cudaError_t ce = cudaSetDevice(e->device);
+  if (ce != cudaSuccess) return bail(PDP3G_CUDA_ERROR, "cudaSetDevice");
+  cudaDeviceGetAttribute(&e->n_sm, cudaDevAttrMultiProcessorCount, e->device);
+  int khz = 0;
+  cudaDeviceGetAttribute(&khz, cudaDevAttrClockRate, e->device);
+  e->clock_khz = khz;
+  if (cudaStreamCreateWithFlags(&e->stream, cudaStreamNonBlocking) != cudaSuccess ||
+      cudaMalloc(&e->d_runs, sizeof(EnsRun) * n_runs) != cudaSuccess ||
+      cudaMalloc(&e->d_species, sizeof(EnsSpecies) * std::max<size_t>(hs.size(), 1)) !=
+          cudaSuccess ||
+      cudaMalloc(&e->d_status, sizeof(int) * 4) != cudaSuccess ||
+      cudaHostAlloc(&e->h_cancel, sizeof(int), cudaHostAllocMapped) != cudaSuccess ||
+      cudaHostGetDevicePointer((void **)&e->d_cancel, e->h_cancel, 0) != cudaSuccess)
+    return bail(PDP3G_CUDA_ERROR, "ensemble allocation");
+  *e->h_cancel = 0;
+  cudaMemcpy(e->d_runs, e->h_runs.data(), sizeof(EnsRun) * n_runs, cudaMemcpyHostToDevice);
+  if (!hs.empty())
+    cudaMemcpy(e->d_species, hs.data(), sizeof(EnsSpecies) * hs.size(), cudaMemcpyHostToDevice);
+  EnsembleDev &d = e->dev;
+  d.runs = e->d_runs;
+  d.nruns = n_runs;
+  d.species = e->d_species;
+  d.nspecies = (int)hs.size();
+  d.total_h = h;
+  d.total_e = ee;
+  d.total_j = j;
+  d.total_chunks = ch;
+  d.inv_pow11 = runs[0]->d_inv_pow11;
+  d.cancel = e->d_cancel;
+  d.status = e->d_status;
+  d.budget_cycles = 0;
+  e->max_blocks_per_sm = ensemble_max_blocks_per_sm();
+  if (e->max_blocks_per_sm <= 0) return bail(PDP3G_CUDA_ERROR, "ensemble kernel does not fit");
+  e->blocks_per_sm = e->max_blocks_per_sm;
+  *out = e;
+  return PDP3G_OK;
+}
+
+static pdp3g_status ens_launch(pdp3g_ensemble *e, int nsteps, bool allow_graph) {
+  const int blocks = e->n_sm * e->blocks_per_sm;
+  e->dev.budget_cycles = e->budget_ms > 0 ? (long long)(e->budget_ms * e->clock_khz) : 0;
+  e->last_used_graph = false;
+  if (allow_graph && e->graph_ok) {
+    if (e->exec && (e->graph_steps != nsteps || e->graph_blocks != blocks)) {
+      cudaGraphExecDestroy(e->exec);
+      cudaGraphDestroy(e->graph);
+      e->exec = nullptr;
+      e->graph = nullptr;
+    }
+    if (!e->exec) {
+      cudaError_t c1 = cudaStreamBeginCapture(e->stream, cudaStreamCaptureModeThreadLocal);
+      cudaError_t c2 = c1 == cudaSuccess ? ensemble_launch(e->dev, nsteps, blocks, e->stream) : c1;
+      cudaGraph_t g = nullptr;
+      cudaError_t c3 = c1 == cudaSuccess ? cudaStreamEndCapture(e->stream, &g) : c1;
+      cudaError_t c4 = (c2 == cudaSuccess && c3 == cudaSuccess)
+                           ? cudaGraphInstantiate(&e->exec, g, 0)
+                           : cudaErrorUnknown;
+      if (c4 == cudaSuccess) {
+        e->graph = g;
+        e->graph_steps = nsteps;
+        e->graph_blocks = blocks;
+      } else {
+        if (g) cudaGraphDestroy(g);
+        e->exec = nullptr;
+        e->graph_ok = false;  // capture of a cooperative launch refused: launch directly
+        cudaGetLastError();
+      }
+    }
+    if (e->exec) {
+      EK(cudaGraphLaunch(e->exec, e->stream));
+      e->last_used_graph = true;
+      return PDP3G_OK;
+    }
+  }
+  EK(ensemble_launch(e->dev, nsteps, blocks, e->stream));
+  return PDP3G_OK;
+}
+
+static pdp3g_status ens_run(pdp3g_ensemble *e, int nsteps, bool allow_graph, float *ms_out) {
+  EK(cudaSetDevice(e->device));
+  for (size_t r = 0; r < e->runs.size(); r++) {
+    EK(cudaStreamSynchronize(e->runs[r]->stream));
+    e->h_runs[r].t = e->runs[r]->t;
+  }
+  EK(cudaMemcpyAsync(e->d_runs, e->h_runs.data(), sizeof(EnsRun) * e->h_runs.size(),
+                     cudaMemcpyHostToDevice, e->stream));
+  EK(cudaMemsetAsync(e->d_status, 0, sizeof(int) * 4, e->stream));
+  cudaEvent_t a, b;
+  cudaEventCreate(&a);
+  cudaEventCreate(&b);
+  cudaEventRecord(a, e->stream);
+  pdp3g_status st = ens_launch(e, nsteps, allow_graph);
+  cudaEventRecord(b, e->stream);
+  cudaError_t sync = cudaStreamSynchronize(e->stream);
+  float ms = 0;
+  cudaEventElapsedTime(&ms, a, b);
+  cudaEventDestroy(a);
+  cudaEventDestroy(b);
+  if (st != PDP3G_OK) return st;
+  if (sync != cudaSuccess) return ens_fail(e, PDP3G_CUDA_ERROR, cudaGetErrorString(sync));
+  int status[4] = {0, 0, 0, 0};
+  EK(cudaMemcpy(status, e->d_status, sizeof(status), cudaMemcpyDeviceToHost));
+  const int done = status[0];
+  for (auto *c : e->runs) {
+    for (int i = 0; i < done; i++) c->t = c->t + c->cfg.dt;
+    c->steps += done;
+  }
+  e->last_ms = ms;
+  e->last_steps_done = done;
+  if (ms_out) *ms_out = ms;
+  if (status[1] == 1) return ens_fail(e, PDP3G_TIMEOUT, "ensemble cancelled");
+  if (status[1] == 2) return ens_fail(e, PDP3G_TIMEOUT, "ensemble time budget exhausted");
+  return PDP3G_OK;
+}
+
+pdp3g_status pdp3g_ensemble_run(pdp3g_ensemble *e, int32_t nsteps) {
+  if (!e || nsteps < 0) return PDP3G_INVALID_ARG;
+  if (nsteps == 0) return PDP3G_OK;
+  return ens_run(e, nsteps, true, nullptr);
+}
+
+pdp3g_status pdp3g_ensemble_autotune(pdp3g_ensemble *e, int32_t steps_per_trial,
+                                     int32_t *blocks_per_sm) {
+  if (!e || steps_per_trial <= 0) return PDP3G_INVALID_ARG;
+  float best = 0;
+  int best_b = e->blocks_per_sm;
+  for (int b = 1; b <= e->max_blocks_per_sm; b++) {
+    e->blocks_per_sm = b;
+    float ms = 0;
+    pdp3g_status st = ens_run(e, steps_per_trial, false, &ms);
+    if (st != PDP3G_OK) return st;
+    if (b == 1 || ms < best) {
+      best = ms;
+      best_b = b;
+    }
+  }
+  e->blocks_per_sm = best_b;
+  if (blocks_per_sm) *blocks_per_sm = best_b;
+  return PDP3G_OK;
+}
+
+pdp3g_status pdp3g_ensemble_set_budget(pdp3g_ensemble *e, double max_ms) {
+  if (!e || max_ms < 0) return PDP3G_INVALID_ARG;
+  e->budget_ms = max_ms;
+  return PDP3G_OK;
+}
+
+pdp3g_status pdp3g_ensemble_cancel(pdp3g_ensemble *e, int32_t cancel) {
+  if (!e) return PDP3G_INVALID_ARG;
+  *(volatile int *)e->h_cancel = cancel ? 1 : 0;
+  return PDP3G_OK;
+}
+
+pdp3g_status pdp3g_ensemble_info(pdp3g_ensemble *e, pdp3g_ensemble_stats *out) {
+  if (!e || !out) return PDP3G_INVALID_ARG;
+  out->runs = (int32_t)e->runs.size();
+  out->blocks_per_sm = e->blocks_per_sm;
+  out->blocks = e->n_sm * e->blocks_per_sm;
+  out->used_graph = e->last_used_graph ? 1 : 0;
+  out->last_ms = e->last_ms;
+  out->last_steps_done = e->last_steps_done;
+  out->particles = e->total_particles;
+  return PDP3G_OK;
+}
+
+const char *pdp3g_ensemble_last_error(pdp3g_ensemble *e) { return e ? e->last_error.c_str() : ""; }
 
 }  // extern "C"

@@ -1,0 +1,159 @@
+// Batched ensemble: many independent runs (different grids, species and
+// bunches, FP32 cell-local form) advanced together by ONE persistent
+// cooperative kernel per launch, replayed from a captured CUDA graph.
+//
+// Every step has three phases separated by grid-wide barriers:
+//   A  bunch injection, H update and J clear of every run
+//   B  push + deposition of every chunk of every species of every run
+//   C  E update of every run, t += dt
+// Work items are global index spaces (nodes of all runs, 256-particle chunks
+// of all species) dealt to CTAs round-robin, so runs of very different sizes
+// share the GPU without per-run launches.  Each run's step is the same as
+// pdp3g_step on that run alone (same device functions, fields_body.cuh and
+// particles_f32.cuh).
+//
+// Stop path: at the top of each step one thread reads a host-mapped cancel
+// flag and compares clock64() with a cycle budget; the decision is published
+// through device memory before the barrier, so every CTA leaves together and
+// the kernel never spins on the host.
+#include <cooperative_groups.h>
+
+#include "fields_body.cuh"
+#include "particles_f32.cuh"
+
+namespace cg = cooperative_groups;
+
+namespace pdp3g {
+
+// largest index j with prefix[j] <= x (prefix ascending, prefix[0] = 0)
+template <typename F>
+__device__ __forceinline__ int find_owner(long long x, int n, F prefix) {
+  int lo = 0, hi = n - 1;
+  while (lo < hi) {
+    const int mid = (lo + hi + 1) >> 1;
+    if (prefix(mid) <= x) lo = mid; else hi = mid - 1;
+  }
+  return lo;
+}
+
+// Bunch::bunch_inject (src/bunch.cpp:87-124) for one bunch species, by one CTA
+__device__ void ens_inject(const EnsembleDev &E, const EnsSpecies &sp) {
+  const EnsRun &run = E.runs[sp.run];
+  const double dt = run.g.dt, t = run.t;
+  const double begin = sp.duration * sp.bunch_number + sp.hole_duration * sp.bunch_number;
+  const double end = begin + sp.duration;
+  const double dl = sp.velocity * dt;
+  const int steps_amount = (int)ceil(sp.duration / dt);
+  const unsigned number = (unsigned)sp.s.n;
+  const unsigned particles_in_step = number / steps_amount;
+  const int start_number = (t - begin) / dt * particles_in_step;
+  if (!(t >= begin && t < end) || particles_in_step == 0) return;
+  const long long start = (long long)(unsigned)start_number;
+  const int ncz = run.g.nz - 1;
+  const double dz = run.g.dz;
+  for (long long j = threadIdx.x; j < particles_in_step; j += blockDim.x) {
+    const long long idx = start + j;
+    if (idx >= (long long)number) break;
+    int int_vel = (int)floor((double)(unsigned)idx);
+    double ost = 0, rr = 0;
+    int order = 1;
+    while (int_vel >= 1 && order < 40) {
+      ost = int_vel % 11;
+      rr = rr + ost * E.inv_pow11[order];
+      int_vel = (int)((int_vel - ost) / 11);
+      order = order + 1;
+    }
+    const double z = dl * rr + dz / 2.0;
+    int k = (int)ceil(z / dz) - 1;
+    k = max(0, min(k, ncz - 1));
+    const int i = sp.s.cell[idx] / ncz;
+    sp.s.cell[idx] = i * ncz + k;
+    sp.s.fz[idx] = (float)(z / dz - k);
+    sp.s.uz[idx] = sp.uz_beam;
+    sp.s.alive[idx] = 1;
+  }
+}
+
+__global__ void __launch_bounds__(F32_THREADS, 3) k_ensemble(EnsembleDev E, int nsteps) {
+  cg::grid_group grid = cg::this_grid();
+  __shared__ F32Shared sm;
+  for (int idx = threadIdx.x; idx < 3 * TILE_CAP; idx += F32_THREADS) sm.acc[idx] = 0.0f;
+  __syncthreads();
+  const long long gtid = (long long)blockIdx.x * blockDim.x + threadIdx.x;
+  const long long gstride = (long long)gridDim.x * blockDim.x;
+  const long long t_start = clock64();
+  for (int step = 0; step < nsteps; step++) {
+    if (gtid == 0) {
+      int stop = 0;
+      if (*E.cancel) stop = 1;
+      else if (E.budget_cycles > 0 && clock64() - t_start > E.budget_cycles) stop = 2;
+      E.status[1] = stop;
+      __threadfence();
+    }
+    grid.sync();
+    if (*(volatile int *)&E.status[1] != 0) return;
+    // ---- phase A: injection, H update, J clear
+    for (int sp = blockIdx.x; sp < E.nspecies; sp += gridDim.x)
+      if (E.species[sp].is_bunch) ens_inject(E, E.species[sp]);
+    for (long long x = gtid; x < E.total_h; x += gstride) {
+      const int r = find_owner(x, E.nruns, [&](int j) { return E.runs[j].h_begin; });
+      const GridDev &g = E.runs[r].g;
+      const long long l = x - E.runs[r].h_begin;
+      const int i = (int)(l / (g.nz - 1));
+      yee_h_node(g, i, (int)(l - (long long)i * (g.nz - 1)));
+    }
+    for (long long x = gtid; x < E.total_j; x += gstride) {
+      const int r = find_owner(x, E.nruns, [&](int j) { return E.runs[j].j_begin; });
+      const GridDev &g = E.runs[r].g;
+      const long long l = x - E.runs[r].j_begin;
+      g.jr[l] = 0.0;
+      g.jphi[l] = 0.0;
+      g.jz[l] = 0.0;
+    }
+    grid.sync();
+    // ---- phase B: particles
+    for (long long c = blockIdx.x; c < E.total_chunks; c += gridDim.x) {
+      const int sp = find_owner(c, E.nspecies, [&](int j) { return E.species[j].chunk_begin; });
+      const EnsSpecies &S = E.species[sp];
+      const EnsRun &run = E.runs[S.run];
+      f32_chunk(run.g, S.s, run.pusher, c - S.chunk_begin, sm);
+    }
+    grid.sync();
+    // ---- phase C: E update, t += dt
+    for (long long x = gtid; x < E.total_e; x += gstride) {
+      const int r = find_owner(x, E.nruns, [&](int j) { return E.runs[j].e_begin; });
+      const GridDev &g = E.runs[r].g;
+      const long long l = x - E.runs[r].e_begin;
+      const int i = (int)(l / (g.nz - 1));
+      yee_e_node(g, i, (int)(l - (long long)i * (g.nz - 1)));
+    }
+    if (gtid < E.nruns) E.runs[gtid].t = E.runs[gtid].t + E.runs[gtid].g.dt;
+    if (gtid == 0) E.status[0] = step + 1;
+  }
+}
+
+int ensemble_max_blocks_per_sm() {
+  int nb = 0;
+  if (cudaOccupancyMaxActiveBlocksPerMultiprocessor(&nb, k_ensemble, F32_THREADS, 0) !=
+      cudaSuccess)
+    return 0;
+  return nb;
+}
+
+// One cooperative launch of nsteps steps (graph capture of this call is done
+// by the caller).
+cudaError_t ensemble_launch(const EnsembleDev &E, int nsteps, int blocks, cudaStream_t st) {
+  cudaLaunchConfig_t cfg = {};
+  cfg.gridDim = dim3(blocks);
+  cfg.blockDim = dim3(F32_THREADS);
+  cfg.dynamicSmemBytes = 0;
+  cfg.stream = st;
+  cudaLaunchAttribute attr[1];
+  attr[0].id = cudaLaunchAttributeCooperative;
+  attr[0].val.cooperative = 1;
+  cfg.attrs = attr;
+  cfg.numAttrs = 1;
+  return cudaLaunchKernelEx(&cfg, k_ensemble, E, nsteps);
+}
+
+}  // namespace pdp3g

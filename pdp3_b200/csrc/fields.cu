@@ -8,80 +8,29 @@
 // from L2).  Algorithmic bytes per node: H update reads E (3) and H (3),
 // writes H (3) and H_half (3): 96 B; E update reads E (3), H (3), J (3),
 // sigma, writes E (3): 104 B.
-#include "pdp3g_internal.cuh"
+#include "fields_body.cuh"
 
 namespace pdp3g {
 
-#define IDX(i, k) ((size_t)(i) * (size_t)nz + (size_t)(k))
-
-// HField::calc_field, src/hField.cpp:93-157.  H_r is updated for
-// i in [0, nr-1], H_phi and H_z for i in [0, nr-2]; k in [0, nz-2].
-// H_half = H_old + dH/2 (H_z: H_old - dH/2, the upstream sign convention).
+// H update over i in [0, nr-1], k in [0, nz-2]
 __global__ void __launch_bounds__(256) k_yee_h(GridDev g) {
-  const int nr = g.nr, nz = g.nz;
-  const double dr = g.dr, dz = g.dz, dt = g.dt;
-  const long long total = (long long)nr * (nz - 1);
+  const int nz = g.nz;
+  const long long total = (long long)g.nr * (nz - 1);
   for (long long t = blockIdx.x * (long long)blockDim.x + threadIdx.x; t < total;
        t += (long long)gridDim.x * blockDim.x) {
     const int i = (int)(t / (nz - 1));
-    const int k = (int)(t - (long long)i * (nz - 1));
-    const double ephi_ik = g.ephi[IDX(i, k)];
-    const double ephi_ik1 = g.ephi[IDX(i, k + 1)];
-    const double a = dt * (ephi_ik1 - ephi_ik) / (dz * MAGN_CONST);
-    const double hr = g.hr[IDX(i, k)];
-    g.hrh[IDX(i, k)] = hr + a / 2;
-    g.hr[IDX(i, k)] = hr + a;
-    if (i < nr - 1) {
-      const double b = dt * ((g.ez[IDX(i + 1, k)] - g.ez[IDX(i, k)]) / dr -
-                             (g.er[IDX(i, k + 1)] - g.er[IDX(i, k)]) / dz) / MAGN_CONST;
-      const double hphi = g.hphi[IDX(i, k)];
-      g.hphih[IDX(i, k)] = hphi + b / 2;
-      g.hphi[IDX(i, k)] = hphi + b;
-      const double ephi_i1k = g.ephi[IDX(i + 1, k)];
-      const double c = dt * ((ephi_i1k + ephi_ik) / (2.0 * dr * (i + 0.5)) +
-                             (ephi_i1k - ephi_ik) / dr) / MAGN_CONST;
-      const double hz = g.hz[IDX(i, k)];
-      g.hzh[IDX(i, k)] = hz - c / 2;
-      g.hz[IDX(i, k)] = hz - c;
-    }
+    yee_h_node(g, i, (int)(t - (long long)i * (nz - 1)));
   }
 }
 
-// EField::calc_field, src/eField.cpp:85-170 (epsilon == 1):
-//   E_r   i in [0, nr-2], k in [1, nz-2]
-//   E_phi i in [1, nr-2], k in [1, nz-2]
-//   E_z   i = 0 (on-axis form, 4/dr * H_phi), k in [0, nz-2];
-//         i in [1, nr-2], k in [0, nz-2] (interior form, also the k = 0 row)
+// E update over i in [0, nr-2], k in [0, nz-2]
 __global__ void __launch_bounds__(256) k_yee_e(GridDev g) {
-  const int nr = g.nr, nz = g.nz;
-  const double dr = g.dr, dz = g.dz, dt = g.dt;
-  const long long total = (long long)(nr - 1) * (nz - 1);
+  const int nz = g.nz;
+  const long long total = (long long)(g.nr - 1) * (nz - 1);
   for (long long t = blockIdx.x * (long long)blockDim.x + threadIdx.x; t < total;
        t += (long long)gridDim.x * blockDim.x) {
     const int i = (int)(t / (nz - 1));
-    const int k = (int)(t - (long long)i * (nz - 1));
-    const double epsx2 = 2 * 1.0 * EPSILON0;
-    const double sigma_t = g.sigma[IDX(i, k)] * dt;
-    const double koef_e = (epsx2 - sigma_t) / (epsx2 + sigma_t);
-    const double koef_h = 2 * dt / (epsx2 + sigma_t);
-    const double hphi_ik = g.hphi[IDX(i, k)];
-    if (k >= 1) {
-      g.er[IDX(i, k)] = g.er[IDX(i, k)] * koef_e -
-                        (g.jr[IDX(i, k)] + (hphi_ik - g.hphi[IDX(i, k - 1)]) / dz) * koef_h;
-    }
-    if (i == 0) {
-      g.ez[IDX(i, k)] = g.ez[IDX(i, k)] * koef_e - (g.jz[IDX(i, k)] - 4.0 / dr * hphi_ik) * koef_h;
-    } else {
-      const double hphi_m = g.hphi[IDX(i - 1, k)];
-      g.ez[IDX(i, k)] = g.ez[IDX(i, k)] * koef_e -
-                        (g.jz[IDX(i, k)] - (hphi_ik - hphi_m) / dr -
-                         (hphi_ik + hphi_m) / (2.0 * dr * i)) * koef_h;
-      if (k >= 1) {
-        g.ephi[IDX(i, k)] = g.ephi[IDX(i, k)] * koef_e -
-                            (g.jphi[IDX(i, k)] - (g.hr[IDX(i, k)] - g.hr[IDX(i, k - 1)]) / dz +
-                             (g.hz[IDX(i, k)] - g.hz[IDX(i - 1, k)]) / dr) * koef_h;
-      }
-    }
+    yee_e_node(g, i, (int)(t - (long long)i * (nz - 1)));
   }
 }
 

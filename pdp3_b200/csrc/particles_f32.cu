@@ -36,464 +36,18 @@
 // bounding box of the CTA's particles (particles sorted by cell keep the box
 // small) and flushed into the FP64 grid currents with FP64 atomics; a CTA
 // whose box does not fit adds straight into the FP64 grid.
-#include "pdp3g_internal.cuh"
+#include "particles_f32.cuh"
 
 namespace pdp3g {
 
-#define GIDX(i, k) ((size_t)(i) * (size_t)g.nz + (size_t)(k))
-
-constexpr int F32_THREADS = 256;
-constexpr int TILE_CAP = 1536;  // nodes per component in the shared accumulator
-
-__device__ __forceinline__ void flag32(const GridDev &g, unsigned bit) { atomicOr(g.err, bit); }
-
-// moves (i, f) so that f is in (0, 1] (CELL_NUMBER semantics); cells below
-// 0 clamp to 0 like the upstream "sometimes it gives -1" workaround.
-__device__ __forceinline__ void renorm(int &i, float &f) {
-#pragma unroll 1
-  for (int it = 0; it < 4 && f > 1.0f; it++) { f -= 1.0f; i += 1; }
-#pragma unroll 1
-  for (int it = 0; it < 4 && f <= 0.0f; it++) { f += 1.0f; i -= 1; }
-  if (i < 0) { f = f + (float)i; i = 0; }
-}
-
-struct Tile {
-  float *acc;  // [3][TILE_CAP]: j_r, j_phi, j_z
-  int r0, z0, nzb, nrb;
-  bool on;
-};
-
-// adds v into component comp (0 j_r, 1 j_phi, 2 j_z) at node (i, k)
-__device__ __forceinline__ void dep(const GridDev &g, const Tile &t, int comp, int i, int k,
-                                    float v) {
-  const int li = i - t.r0, lk = k - t.z0;
-  if (t.on && (unsigned)li < (unsigned)t.nrb && (unsigned)lk < (unsigned)t.nzb) {
-    atomicAdd(&t.acc[comp * TILE_CAP + li * t.nzb + lk], v);
-    return;
-  }
-  if ((unsigned)i >= (unsigned)g.nr || (unsigned)k >= (unsigned)g.nz) {
-    flag32(g, ERR_OUT_OF_GRID);
-    return;
-  }
-  double *base = comp == 0 ? g.jr : (comp == 1 ? g.jphi : g.jz);
-  atomicAdd(base + GIDX(i, k), (double)v);
-}
-
-// eps(s) = atanh(s)/s - 1
-__device__ __forceinline__ float atanh_ratio_m1(float s) {
-  const float s2 = s * s;
-  if (s2 < 0.01f) return s2 * (1.0f / 3.0f + s2 * (0.2f + s2 * (1.0f / 7.0f + s2 * (1.0f / 9.0f))));
-  return atanhf(s) / s - 1.0f;
-}
-
-// One straight piece of the step inside cell (ci, ck), endpoints given as
-// offsets (ao, co) -> (an, cn) relative to that cell (each in [0, 1]).
-// out = {j_z(ci, ck), j_z(ci+1, ck), j_r(ci, ck), j_r(ci, ck+1)}.
-__device__ __forceinline__ void piece_values(int ci, float ao, float co, float an, float cn,
-                                             float kz, float kr, float out[4]) {
-  const float drho = an - ao, dzeta = cn - co;
-  const float fi = (float)ci;
-  const float fm = 0.5f * (ao + an);
-  const float rho_m = fi + fm;
-  const float beta = 1.0f - co;  // ((k+1) dz - z_o)/dz
-  if (ci >= 1) {
-    const float s = 0.5f * drho / rho_m;
-    const float eps = atanh_ratio_m1(s);
-    const float ii1 = fi * (fi + 1.0f);
-    const float inv_rm = 1.0f / rho_m;
-    out[0] = kz * dzeta * ((1.0f - fm) * (2.0f * fi + fm) + ii1 * eps) * inv_rm / fi;
-    out[1] = kz * dzeta * (fm * (2.0f * fi + 1.0f + fm) - ii1 * eps) * inv_rm / (fi + 1.0f);
-    const float rho_o = fi + ao, rho_n = fi + an;
-    const float q1 = drho / (rho_o * rho_n);
-    const float q2 = dzeta * drho * 0.5f * inv_rm / rho_n;
-    const float q3 = dzeta * eps * inv_rm;
-    const float h = 0.5f * ii1;
-    const float inv_r0 = kr / (fi + 0.5f);
-    out[2] = inv_r0 * (0.5f * drho * beta - 0.25f * dzeta * drho + h * (q1 * beta - q2 - q3));
-    out[3] = inv_r0 * (0.5f * drho * co + 0.25f * dzeta * drho + h * (q1 * co + q2 + q3));
-  } else {
-    // i = 0: src/particles.cpp:415-473 (no log terms; i(i+1) = 0)
-    out[0] = 8.0f * kz * dzeta * (1.0f - fm);
-    out[1] = kz * dzeta * (1.0f + fm);
-    out[2] = 2.0f * kr * (0.5f * drho * beta - 0.25f * dzeta * drho);
-    out[3] = 2.0f * kr * (0.5f * drho * co + 0.25f * dzeta * drho);
-  }
-}
-
-__device__ __forceinline__ void dep_rz(const GridDev &g, const Tile &t, int ci, int ck,
-                                       const float v[4]) {
-  dep(g, t, 2, ci, ck, v[0]);
-  dep(g, t, 2, ci + 1, ck, v[1]);
-  dep(g, t, 0, ci, ck, v[2]);
-  dep(g, t, 0, ci, ck + 1, v[3]);
-}
-
-// The step's straight path from (i, a, k, b) to (in, an, kn, bn) split at the
-// cell faces it crosses (at most one r face and one z face).  The first
-// piece's cell and values are returned (the caller reduces them across the
-// warp); further pieces are deposited directly.  Returns false when the
-// path spans more than one cell in r or z (nothing is deposited, as upstream).
-__device__ __forceinline__ bool deposit_path(const GridDev &g, const Tile &t, int i, float a,
-                                             int k, float b, int in, float an, int kn, float bn,
-                                             float kz, float kr, int &c0i, int &c0k,
-                                             float first[4]) {
-  const int di = in - i, dk = kn - k;
-  if (di < -1 || di > 1 || dk < -1 || dk > 1) return false;
-  // end point relative to the start cell
-  const float A = (float)di + an, B = (float)dk + bn;
-  float tr = 2.0f, tz = 2.0f;
-  if (di != 0) tr = ((di > 0 ? 1.0f : 0.0f) - a) / (A - a);
-  if (dk != 0) tz = ((dk > 0 ? 1.0f : 0.0f) - b) / (B - b);
-  float ts[2];
-  int kind[2];  // 0: r face, 1: z face
-  int np = 0;
-  if (tr <= 1.0f && tz <= 1.0f) {
-    if (tr <= tz) { ts[0] = tr; kind[0] = 0; ts[1] = tz; kind[1] = 1; }
-    else { ts[0] = tz; kind[0] = 1; ts[1] = tr; kind[1] = 0; }
-    np = 2;
-  } else if (tr <= 1.0f) {
-    ts[0] = tr; kind[0] = 0; np = 1;
-  } else if (tz <= 1.0f) {
-    ts[0] = tz; kind[0] = 1; np = 1;
-  }
-  int ci = i, ck = k;
-  float pa = a, pb = b;  // current point relative to (i, k)
-  c0i = i;
-  c0k = k;
-#pragma unroll 1
-  for (int p = 0; p <= np; p++) {
-    float qa, qb;
-    if (p < np) {
-      // crossing point: the crossed coordinate sits exactly on the face
-      const float tt = ts[p];
-      if (kind[p] == 0) {
-        qa = di > 0 ? 1.0f : 0.0f;
-        qb = b + tt * (B - b);
-      } else {
-        qa = a + tt * (A - a);
-        qb = dk > 0 ? 1.0f : 0.0f;
-      }
-    } else {
-      qa = A;
-      qb = B;
-    }
-    const float oi = (float)(ci - i), ok = (float)(ck - k);
-    if (p == 0) {
-      piece_values(ci, pa - oi, pb - ok, qa - oi, qb - ok, kz, kr, first);
-    } else {
-      float v[4];
-      piece_values(ci, pa - oi, pb - ok, qa - oi, qb - ok, kz, kr, v);
-      dep_rz(g, t, ci, ck, v);
-    }
-    if (p < np) {
-      if (kind[p] == 0) ci += di; else ck += dk;
-    }
-    pa = qa;
-    pb = qb;
-  }
-  return true;
-}
-
-// Warp-level segmented sum of the 4 deposits of each run of consecutive
-// lanes with the same key (particles sorted by cell form long runs); the
-// last lane of a run adds the run's totals.  Lanes with key < 0 hold nothing.
-// node layout: MODE 0 = j_phi at (i,k), (i+1,k), (i,k+1), (i+1,k+1);
-//              MODE 1 = j_z at (i,k), (i+1,k), j_r at (i,k), (i,k+1).
-template <int MODE>
-__device__ __forceinline__ void warp_run_deposit(const GridDev &g, const Tile &t, int key, int i,
-                                                 int k, float v[4]) {
-  const unsigned FULL = 0xffffffffu;
-  const int lane = threadIdx.x & 31;
-  const int prev = __shfl_up_sync(FULL, key, 1);
-  const int next = __shfl_down_sync(FULL, key, 1);
-  const bool head = lane == 0 || prev != key;
-  const bool tail = lane == 31 || next != key;
-  const unsigned heads = __ballot_sync(FULL, head);
-  const unsigned le = lane == 31 ? FULL : ((2u << lane) - 1u);
-  const int seg_start = 31 - __clz(heads & le);
-#pragma unroll
-  for (int j = 0; j < 4; j++) {
-    float x = v[j];
-#pragma unroll
-    for (int off = 1; off < 32; off <<= 1) {
-      const float y = __shfl_up_sync(FULL, x, off);
-      if (lane >= seg_start + off) x += y;
-    }
-    v[j] = x;
-  }
-  if (tail && key >= 0) {
-    if (MODE == 0) {
-      dep(g, t, 1, i, k, v[0]);
-      dep(g, t, 1, i + 1, k, v[1]);
-      dep(g, t, 1, i, k + 1, v[2]);
-      dep(g, t, 1, i + 1, k + 1, v[3]);
-    } else {
-      dep_rz(g, t, i, k, v);
-    }
-  }
-}
-
-__device__ __forceinline__ void weights_rhalf(int i, float a, int &ir, float &w0, float &w1) {
-  // E_r / H_z / H_phi radial part: i_r = CELL_NUMBER(r - dr/2), volumes
-  // CELL_VOLUME(i_r+1), CELL_VOLUME(i_r+3) (src/eField.cpp:225-248)
-  ir = a > 0.5f ? i : i - 1;
-  if (ir < 0) ir = 0;
-  const float d21 = (float)(ir - i) + 1.5f - a;
-  const float s21 = (float)(ir + i) + 0.5f + a;
-  const float d32 = (float)(i - ir) + a - 0.5f;
-  const float s32 = (float)(i + ir) + 1.5f + a;
-  w0 = d21 * s21 / (2.0f * (float)(ir + 1));
-  w1 = d32 * s32 / (2.0f * (float)(ir + 3));
-}
-
-__device__ __forceinline__ void weights_rnode(int i, float a, float &w0, float &w1) {
-  // E_z / E_phi / H_r radial part: i_r = CELL_NUMBER(r), volume CELL_VOLUME(i)
-  // or CYL_VOL for r <= dr, and CELL_VOLUME(i+2) (src/eField.cpp:252-279)
-  const float fi = (float)i;
-  const float v1 = i >= 1 ? 2.0f * fi : 0.25f;
-  w0 = (1.0f - a) * (2.0f * fi + a) / v1;
-  w1 = a * (2.0f * fi + 1.0f + a) / (2.0f * (fi + 2.0f));
-}
-
-__device__ __forceinline__ void weights_zhalf(int k, float b, int &kz, float &w0, float &w1) {
-  kz = b > 0.5f ? k : k - 1;
-  if (kz < 0) kz = 0;
-  w0 = (float)(kz - k) + 1.5f - b;
-  w1 = (float)(k - kz) + b - 0.5f;
-}
-
-__device__ __forceinline__ float gather4(const GridDev &g, const double *__restrict__ f, int ir,
-                                         int kz, float wr0, float wr1, float wz0, float wz1) {
-  if (ir > g.nr - 2) { flag32(g, ERR_OUT_OF_GRID); ir = g.nr - 2; }
-  if (kz > g.nz - 2) { flag32(g, ERR_OUT_OF_GRID); kz = g.nz - 2; }
-  const float f00 = (float)__ldg(f + GIDX(ir, kz)), f10 = (float)__ldg(f + GIDX(ir + 1, kz));
-  const float f01 = (float)__ldg(f + GIDX(ir, kz + 1));
-  const float f11 = (float)__ldg(f + GIDX(ir + 1, kz + 1));
-  return wz0 * (f00 * wr0 + f10 * wr1) + wz1 * (f01 * wr0 + f11 * wr1);
-}
-
 __global__ void __launch_bounds__(F32_THREADS, 4) k_push_deposit_f32(GridDev g, SpeciesF32 s,
                                                                    int pusher) {
-  __shared__ float acc[3 * TILE_CAP];
-  __shared__ int red[4][F32_THREADS / 32];
-  __shared__ int box[4];
-  const int ncz = g.nz - 1;
+  __shared__ F32Shared sm;
   const long long nchunks = (s.n + F32_THREADS - 1) / F32_THREADS;
-  for (int idx = threadIdx.x; idx < 3 * TILE_CAP; idx += F32_THREADS) acc[idx] = 0.0f;
-  for (long long chunk = blockIdx.x; chunk < nchunks; chunk += gridDim.x) {
-    const long long p = chunk * F32_THREADS + threadIdx.x;
-    bool live = p < s.n;
-    if (live && s.alive != nullptr && !s.alive[p]) live = false;
-    int c = live ? s.cell[p] : 0;
-    if (live && (c < 0 || c >= (g.nr - 1) * ncz)) {
-      flag32(g, ERR_OUT_OF_GRID);
-      live = false;
-    }
-    const int i = c / ncz, k = c - (c / ncz) * ncz;
-    // bounding box of the chunk's start cells (block min/max reduction)
-    int v4[4] = {live ? i : INT_MAX, live ? -i : INT_MAX, live ? k : INT_MAX,
-                 live ? -k : INT_MAX};
-#pragma unroll
-    for (int j = 0; j < 4; j++) {
-#pragma unroll
-      for (int o = 16; o > 0; o >>= 1) v4[j] = min(v4[j], __shfl_xor_sync(0xffffffffu, v4[j], o));
-    }
-    if ((threadIdx.x & 31) == 0)
-#pragma unroll
-      for (int j = 0; j < 4; j++) red[j][threadIdx.x >> 5] = v4[j];
-    __syncthreads();
-    if (threadIdx.x < 4) {
-      int m = INT_MAX;
-      for (int w = 0; w < F32_THREADS / 32; w++) m = min(m, red[threadIdx.x][w]);
-      box[threadIdx.x] = m;
-    }
-    __syncthreads();
-    Tile t;
-    t.acc = acc;
-    t.r0 = box[0] - 1;
-    t.z0 = box[2] - 1;
-    t.nrb = -box[1] - box[0] + 4;
-    t.nzb = -box[3] - box[2] + 4;
-    t.on = box[0] != INT_MAX && t.nrb * t.nzb <= TILE_CAP;
-    // this lane's j_phi and first r-z piece, reduced across the warp below
-    int key_phi = -1, key_rz = -1, phi_i = 0, phi_k = 0, rz_i = 0, rz_k = 0;
-    float vphi4[4] = {0.f, 0.f, 0.f, 0.f}, vrz4[4] = {0.f, 0.f, 0.f, 0.f};
-    if (live) {
-      const float a = s.fr[p], b = s.fz[p];
-      float u[3] = {s.ur[p], s.uphi[p], s.uz[p]};
-      const float w = s.w[p];
-      // ---- gather E (time n) and H (time n+1/2)
-      int ir_h, kz_h;
-      float wrh0, wrh1, wrn0, wrn1, wzh0, wzh1;
-      weights_rhalf(i, a, ir_h, wrh0, wrh1);
-      weights_rnode(i, a, wrn0, wrn1);
-      weights_zhalf(k, b, kz_h, wzh0, wzh1);
-      const float wzn0 = 1.0f - b, wzn1 = b;
-      const int ir_n = i, kz_n = k;
-      float e[3], h[3];
-      e[0] = gather4(g, g.er, ir_h, kz_n, wrh0, wrh1, wzn0, wzn1);
-      e[1] = gather4(g, g.ephi, ir_n, kz_n, wrn0, wrn1, wzn0, wzn1);
-      e[2] = gather4(g, g.ez, ir_n, kz_h, wrn0, wrn1, wzh0, wzh1);
-      h[0] = gather4(g, g.hrh, ir_n, kz_h, wrn0, wrn1, wzh0, wzh1);
-      h[1] = gather4(g, g.hphih, ir_h, kz_h, wrh0, wrh1, wzh0, wzh1);
-      h[2] = gather4(g, g.hzh, ir_h, kz_n, wrh0, wrh1, wzn0, wzn1);
-      // ---- push
-      float inv_g = 1.0f;
-      if (pusher == 1) {
-        // Vay as the upstream code writes it (src/particles.cpp:1152-1254), in
-        // SI velocity units (gamma v in m/s) because its alpha/us2 terms mix
-        // units and so depend on them.
-        const float C = (float)LIGHT_SPEED;
-        float vel[3] = {u[0] * C, u[1] * C, u[2] * C};
-        float ee[3], bb[3], vt[3];
-#pragma unroll
-        for (int j = 0; j < 3; j++) {
-          ee[j] = e[j] * s.vay_e;
-          bb[j] = h[j] * s.vay_b;
-          vt[j] = vel[j];
-          vel[j] += ee[j];
-        }
-        float gm = rsqrtf(1.0f + (vt[0] * vt[0] + vt[1] * vt[1] + vt[2] * vt[2]) * s.inv_c2);
-        vel[0] += gm * (vt[1] * bb[2] - vt[2] * bb[1]);
-        vel[1] += gm * (vt[2] * bb[0] - vt[0] * bb[2]);
-        vel[2] += gm * (vt[0] * bb[1] - vt[1] * bb[0]);
-        gm = rsqrtf(1.0f + (vel[0] * vel[0] + vel[1] * vel[1] + vel[2] * vel[2]) * s.inv_c2);
-        float alpha = 1.0f / gm / gm;
-        const float B2 = bb[0] * bb[0] + bb[1] * bb[1] + bb[2] * bb[2];
-        float sg = alpha - B2;
-        const float vb = vel[0] * bb[0] + vel[1] * bb[1] + vel[2] * bb[2];
-        alpha = rsqrtf(0.5f * (sg + sqrtf(sg * sg + 4.0f * (B2 + vb * vb))));
-#pragma unroll
-        for (int j = 0; j < 3; j++) bb[j] *= alpha;
-        sg = 1.0f / (1.0f + bb[0] * bb[0] + bb[1] * bb[1] + bb[2] * bb[2]);
-        alpha = vel[0] * bb[0] + vel[1] * bb[1] + vel[2] * bb[2];
-        vt[0] = sg * (vel[0] + alpha * bb[0] + bb[2] * vel[1] - bb[1] * vel[2]);
-        vt[1] = sg * (vel[1] + alpha * bb[1] + bb[0] * vel[2] - bb[2] * vel[0]);
-        vt[2] = sg * (vel[2] + alpha * bb[2] + bb[1] * vel[0] - bb[0] * vel[1]);
-#pragma unroll
-        for (int j = 0; j < 3; j++) u[j] = vt[j] / C;
-        inv_g = rsqrtf(1.0f + u[0] * u[0] + u[1] * u[1] + u[2] * u[2]);
-      } else {
-        // Boris (src/particles.cpp:1025-1150) on u = gamma v / c
-        float um[3];
-#pragma unroll
-        for (int j = 0; j < 3; j++) um[j] = u[j] + s.ke * e[j];
-        const float gi = pusher == 0 ? rsqrtf(1.0f + um[0] * um[0] + um[1] * um[1] + um[2] * um[2])
-                                     : 1.0f;
-        float tb[3];
-#pragma unroll
-        for (int j = 0; j < 3; j++) tb[j] = s.kb * h[j] * gi;
-        const float c2 = 2.0f / (1.0f + tb[0] * tb[0] + tb[1] * tb[1] + tb[2] * tb[2]);
-        const float w0 = um[0] + (um[1] * tb[2] - um[2] * tb[1]);
-        const float w1 = um[1] + (um[2] * tb[0] - um[0] * tb[2]);
-        const float w2 = um[2] + (um[0] * tb[1] - um[1] * tb[0]);
-        u[0] = um[0] + c2 * (w1 * tb[2] - w2 * tb[1]) + s.ke * e[0];
-        u[1] = um[1] + c2 * (w2 * tb[0] - w0 * tb[2]) + s.ke * e[1];
-        u[2] = um[2] + c2 * (w0 * tb[1] - w1 * tb[0]) + s.ke * e[2];
-        inv_g = pusher == 0 ? rsqrtf(1.0f + u[0] * u[0] + u[1] * u[1] + u[2] * u[2]) : 1.0f;
-      }
-      if (!(inv_g == inv_g)) flag32(g, ERR_NAN);
-      // ---- first half move and rz rotation (cells of r and z units)
-      const float dr_h = u[0] * inv_g * s.cr, dy = u[1] * inv_g * s.cr;
-      const float dz_h = u[2] * inv_g * s.cz;
-      float xa = a + dr_h;
-      float x = (float)i + xa;
-      float rr = sqrtf(x * x + dy * dy);
-      float a1 = xa + (x > 0.0f ? dy * dy / (x + rr) : rr - x);
-      float b1 = b + dz_h;
-      // ---- azimuthal current at the mid-step position (src/particles.cpp:688-784)
-      {
-        int i1 = i, k1 = k;
-        float f1 = a1, g1 = b1;
-        renorm(i1, f1);
-        renorm(k1, g1);
-        const float fi1 = (float)i1;
-        const float rho1 = fi1 + f1;
-        const float v1 = i1 >= 1 ? 2.0f * fi1 : 0.25f;
-        const float wa = (1.0f - f1) * (2.0f * fi1 + f1) / (rho1 * v1);
-        const float wb = f1 * (2.0f * fi1 + 1.0f + f1) / (rho1 * 2.0f * (fi1 + 1.0f));
-        const float pref = s.kphi * w * u[1] * inv_g;
-        vphi4[0] = pref * (1.0f - g1) * wa;
-        vphi4[1] = pref * (1.0f - g1) * wb;
-        vphi4[2] = pref * g1 * wa;
-        vphi4[3] = pref * g1 * wb;
-        phi_i = i1;
-        phi_k = k1;
-        key_phi = i1 * g.nz + k1;
-      }
-      // ---- second half move, walls, rz rotation (src/particles.cpp:1355-1365)
-      float xa2 = a1 + dr_h;
-      float b2 = b1 + dz_h;
-      bool alive_now = true;
-      const float wr_rel = (float)(g.nr - 1) - 0.5f - (float)i;
-      const float wz_rel = (float)(g.nz - 1) - 0.5f - (float)k;
-      if (s.kind == KIND_PLASMA) {
-        if (xa2 > wr_rel) { xa2 = 2.0f * wr_rel - xa2; u[0] = -u[0]; }
-        if (b2 > wz_rel) { b2 = 2.0f * wz_rel - b2; u[2] = -u[2]; }
-      } else {
-        if (xa2 > wr_rel) alive_now = false;
-        if (b2 > wz_rel) alive_now = false;
-      }
-      if (xa2 < 0.5f - (float)i) { xa2 = 1.0f - 2.0f * (float)i - xa2; u[0] = -u[0]; }
-      if (b2 < 0.5f - (float)k) { b2 = 1.0f - 2.0f * (float)k - b2; u[2] = -u[2]; }
-      const float x2 = (float)i + xa2;
-      const float r2 = sqrtf(x2 * x2 + dy * dy);
-      float an = xa2 + (x2 > 0.0f ? dy * dy / (x2 + r2) : r2 - x2);
-      float bn = b2;
-      int in = i, kn = k;
-      renorm(in, an);
-      renorm(kn, bn);
-      if (alive_now) {
-        if (deposit_path(g, t, i, a, k, b, in, an, kn, bn, s.kz * w, s.kr * w, rz_i, rz_k, vrz4))
-          key_rz = rz_i * g.nz + rz_k;
-        // back_velocity_to_rz (src/particles.cpp:1005-1015): cos = x/r, sin = y/r
-        const float inv_r2 = 1.0f / r2;
-        const float st = dy * inv_r2, ct = x2 * inv_r2;
-        const float u0 = ct * u[0] - st * u[1];
-        const float u1 = st * u[0] + ct * u[1];
-        u[0] = u0;
-        u[1] = u1;
-      } else {
-        s.alive[p] = 0;
-      }
-      if (in > g.nr - 2 || kn > g.nz - 2) {
-        flag32(g, ERR_OUT_OF_GRID);
-        in = min(in, g.nr - 2);
-        kn = min(kn, g.nz - 2);
-      }
-      s.cell[p] = in * ncz + kn;
-      s.fr[p] = an;
-      s.fz[p] = bn;
-      s.ur[p] = u[0];
-      s.uphi[p] = u[1];
-      s.uz[p] = u[2];
-    }
-    warp_run_deposit<0>(g, t, key_phi, phi_i, phi_k, vphi4);
-    warp_run_deposit<1>(g, t, key_rz, rz_i, rz_k, vrz4);
-    __syncthreads();
-    // ---- flush the tile into the FP64 grid currents
-    if (t.on) {
-      const int nb = t.nrb * t.nzb;
-      for (int idx = threadIdx.x; idx < nb; idx += F32_THREADS) {
-        const int li = idx / t.nzb, lk = idx - li * t.nzb;
-        const int gi = t.r0 + li, gk = t.z0 + lk;
-#pragma unroll
-        for (int comp = 0; comp < 3; comp++) {
-          const float v = acc[comp * TILE_CAP + idx];
-          if (v != 0.0f) {
-            acc[comp * TILE_CAP + idx] = 0.0f;
-            if ((unsigned)gi < (unsigned)g.nr && (unsigned)gk < (unsigned)g.nz) {
-              double *base = comp == 0 ? g.jr : (comp == 1 ? g.jphi : g.jz);
-              atomicAdd(base + GIDX(gi, gk), (double)v);
-            } else {
-              flag32(g, ERR_OUT_OF_GRID);
-            }
-          }
-        }
-      }
-    }
-    __syncthreads();
-  }
+  for (int idx = threadIdx.x; idx < 3 * TILE_CAP; idx += F32_THREADS) sm.acc[idx] = 0.0f;
+  __syncthreads();
+  for (long long chunk = blockIdx.x; chunk < nchunks; chunk += gridDim.x)
+    f32_chunk(g, s, pusher, chunk, sm);
 }
 
 // Bunch::bunch_inject in the cell-local form: z = dl * random_reverse(idx, 11)
@@ -568,6 +122,79 @@ __global__ void k_kinetic_f32(SpeciesF32 s, double mass, double *partials) {
     for (int w = 0; w < F32_THREADS / 32; w++) sum += sh[threadIdx.x][w];
     partials[(size_t)blockIdx.x * 2 + threadIdx.x] = sum;
   }
+}
+
+// cell-local FP32 state -> FP64 r, z, v (and w when w_out is given)
+__global__ void k_cell_to_f64(SpeciesF32 s, double dr, double dz, int ncz, double *r, double *z,
+                              double *vr, double *vphi, double *vz, double *w_out) {
+  for (long long p = blockIdx.x * (long long)blockDim.x + threadIdx.x; p < s.n;
+       p += (long long)gridDim.x * blockDim.x) {
+    const int c = s.cell[p];
+    const int i = c / ncz, k = c - (c / ncz) * ncz;
+    r[p] = (i + (double)s.fr[p]) * dr;
+    z[p] = (k + (double)s.fz[p]) * dz;
+    const double ur = s.ur[p], up = s.uphi[p], uz = s.uz[p];
+    const double c_over_g = LIGHT_SPEED / sqrt(1.0 + (ur * ur + up * up + uz * uz));
+    vr[p] = ur * c_over_g;
+    vphi[p] = up * c_over_g;
+    vz[p] = uz * c_over_g;
+    if (w_out) w_out[p] = s.w[p];
+  }
+}
+
+// FP64 r, z, v (and w when given) -> cell-local FP32 state; a NaN position,
+// a cell outside the grid or v >= c raises the matching error flag.
+__global__ void k_f64_to_cell(SpeciesF32 s, const double *r, const double *z, const double *vr,
+                              const double *vphi, const double *vz, const double *w_in,
+                              double dr, double dz, int nr, int nz, unsigned *err) {
+  const int ncz = nz - 1;
+  for (long long p = blockIdx.x * (long long)blockDim.x + threadIdx.x; p < s.n;
+       p += (long long)gridDim.x * blockDim.x) {
+    const double rp = r[p], zp = z[p];
+    if (!isfinite(rp) || !isfinite(zp)) {
+      atomicOr(err, ERR_NAN);
+      continue;
+    }
+    int i = (int)ceil(rp / dr) - 1, k = (int)ceil(zp / dz) - 1;
+    if (i < 0) i = 0;
+    if (k < 0) k = 0;
+    if (i > nr - 2 || k > nz - 2) {
+      atomicOr(err, ERR_OUT_OF_GRID);
+      i = min(i, nr - 2);
+      k = min(k, nz - 2);
+    }
+    s.cell[p] = i * ncz + k;
+    s.fr[p] = (float)(rp / dr - i);
+    s.fz[p] = (float)(zp / dz - k);
+    const double v2 = __dadd_rn(__dadd_rn(__dmul_rn(vr[p], vr[p]), __dmul_rn(vphi[p], vphi[p])),
+                                __dmul_rn(vz[p], vz[p]));
+    if (!(v2 < LIGHT_SPEED_POW_2)) {
+      atomicOr(err, ERR_V_GE_C);
+      continue;
+    }
+    const double gc = 1.0 / (LIGHT_SPEED * sqrt(1.0 - v2 / LIGHT_SPEED_POW_2));
+    s.ur[p] = (float)(vr[p] * gc);
+    s.uphi[p] = (float)(vphi[p] * gc);
+    s.uz[p] = (float)(vz[p] * gc);
+    if (w_in) ((float *)s.w)[p] = (float)w_in[p];
+  }
+}
+
+void launch_cell_to_f64(const SpeciesF32 &s, double dr, double dz, int ncz, double *r, double *z,
+                        double *vr, double *vphi, double *vz, double *w_out, cudaStream_t st) {
+  if (s.n <= 0) return;
+  long long blocks = (s.n + 255) / 256;
+  if (blocks > 148 * 16) blocks = 148 * 16;
+  k_cell_to_f64<<<(int)blocks, 256, 0, st>>>(s, dr, dz, ncz, r, z, vr, vphi, vz, w_out);
+}
+
+void launch_f64_to_cell(const SpeciesF32 &s, const double *r, const double *z, const double *vr,
+                        const double *vphi, const double *vz, const double *w_in, double dr,
+                        double dz, int nr, int nz, unsigned *err, cudaStream_t st) {
+  if (s.n <= 0) return;
+  long long blocks = (s.n + 255) / 256;
+  if (blocks > 148 * 16) blocks = 148 * 16;
+  k_f64_to_cell<<<(int)blocks, 256, 0, st>>>(s, r, z, vr, vphi, vz, w_in, dr, dz, nr, nz, err);
 }
 
 void launch_push_deposit_f32(const GridDev &g, const SpeciesF32 &s, int pusher, int n_sm,

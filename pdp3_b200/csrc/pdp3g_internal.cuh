@@ -117,6 +117,38 @@ __device__ __forceinline__ void charge_weight_one(const GridDev &g, double *rho,
   }
 }
 
+// batched ensemble (ensemble.cu)
+struct EnsRun {
+  GridDev g;
+  double t;
+  long long h_begin, e_begin, j_begin, chunk_begin;  // prefixes of the index spaces
+  int pusher;
+};
+
+struct EnsSpecies {
+  SpeciesF32 s;
+  int run;
+  long long chunk_begin;
+  int is_bunch;
+  double duration, bunch_number, hole_duration, velocity;
+  float uz_beam;
+};
+
+struct EnsembleDev {
+  EnsRun *runs;
+  int nruns;
+  EnsSpecies *species;
+  int nspecies;
+  long long total_h, total_e, total_j, total_chunks;
+  const double *inv_pow11;
+  volatile int *cancel;  // host-mapped
+  int *status;           // [0] steps done, [1] stop (0 run, 1 cancelled, 2 budget)
+  long long budget_cycles;
+};
+
+int ensemble_max_blocks_per_sm();
+cudaError_t ensemble_launch(const EnsembleDev &E, int nsteps, int blocks, cudaStream_t st);
+
 // byte offsets of the radix sort's scratch (sort.cu)
 struct SortLayout {
   long long nsub, m, nb;
@@ -144,6 +176,11 @@ void launch_bunch_inject_f32(const SpeciesF32 &s, long long start, long long cou
                              const double *inv_pow11, cudaStream_t st);
 void launch_charge_density_f32(const GridDev &g, const SpeciesF32 &s, double charge,
                                double *rho, cudaStream_t st);
+void launch_cell_to_f64(const SpeciesF32 &s, double dr, double dz, int ncz, double *r, double *z,
+                        double *vr, double *vphi, double *vz, double *w_out, cudaStream_t st);
+void launch_f64_to_cell(const SpeciesF32 &s, const double *r, const double *z, const double *vr,
+                        const double *vphi, const double *vz, const double *w_in, double dr,
+                        double dz, int nr, int nz, unsigned *err, cudaStream_t st);
 void launch_kinetic_f32(const SpeciesF32 &s, double mass, double *partials, double *out,
                         cudaStream_t st);
 void launch_grid_diag(const GridDev &g, const double *rho, const double *rho0, double *partials,
