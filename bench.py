@@ -230,7 +230,8 @@ def main():
     ap.add_argument("--impl", default="ours", choices=["ours", "reference"])
     ap.add_argument("--precision", default="fp32", choices=["fp64", "fp32"],
                     help="the form reported as value (the other is measured beside it)")
-    ap.add_argument("--workload", default="wake", choices=["wake", "thermal"])
+    ap.add_argument("--workload", default="wake", choices=["wake", "thermal", "ensemble"])
+    ap.add_argument("--ensemble-runs", type=int, default=64)
     ap.add_argument("--ppc", type=int, default=None,
                     help="macroparticles per cell (profiling runs on a smaller case)")
     ap.add_argument("--e2e-steps", type=int, default=3)
@@ -245,6 +246,8 @@ def main():
 
     if args.impl == "reference":
         return run_reference(args, rank, world)
+    if args.workload == "ensemble":
+        return run_ensemble(args, rank, world, local_rank)
 
     import torch
     dist = None
@@ -390,6 +393,71 @@ def main():
     if dist is not None:
         dist.barrier()
         dist.destroy_process_group()
+    return 0
+
+
+def run_ensemble(args, rank, world, local_rank):
+    """Batched ensemble: independent FP32 runs of uneven grids advanced by one
+    persistent kernel (pdp3g_ensemble_run), against the same runs stepped one
+    after another with their own launches.  value = ensemble particle-steps/s."""
+    import torch
+    from pdp3_b200 import api
+    from pdp3_b200 import workloads as W
+    torch.cuda.set_device(local_rank)
+    params = W.ensemble_params(seed=1005 + 100 * rank, n_runs=args.ensemble_runs)
+    sims, n_slots = [], 0
+    for p in params:
+        wl = W.ensemble_run_workload(p, steps=500)
+        sims.append(api.from_workload(wl, precision="fp32", device=local_rank))
+        n_slots += wl.n_particles
+    # sequential reference: every run on its own, its own launches
+    for s_ in sims:
+        s_.step(args.warmup)
+        s_.sync()
+    seq_ms = 0.0
+    for s_ in sims:
+        s_.reset_timing()
+        s_.set_timing(True)
+        s_.step(args.steps)
+        s_.sync()
+        seq_ms += s_.timing()["ms_step_total"]
+        s_.set_timing(False)
+    ens = api.Ensemble(sims)
+    bpsm = ens.autotune(2)
+    ens.run(args.warmup)
+    clocks = ClockSampler(local_rank)
+    clocks.start()
+    time.sleep(0.3)
+    ens.run(args.steps)
+    clk = clocks.stop()
+    info = ens.info()
+    ms = info["last_ms"]
+    alive = 0
+    for s_ in sims:
+        for sid in range(3):
+            n = s_.species_size(sid)
+            alive += n if sid < 2 else int(s_.species(sid)["alive"].sum())
+    value = alive * args.steps / (ms / 1000.0)
+    seq_value = alive * args.steps / (seq_ms / 1000.0)
+    if rank == 0:
+        print(json.dumps({
+            "metric": METRIC, "value": value * world, "unit": UNIT, "n_gpus": world,
+            "steps": args.steps, "warmup": args.warmup, "ms_per_step": ms / args.steps,
+            "higher_is_better": True, "scaling": "weak", "vs_baseline": None,
+            "dtype": "f32+f64acc", "data": "synthetic (seeded)",
+            "config": {"workload": "ensemble_%druns" % len(sims), "runs": len(sims),
+                       "particle_slots": n_slots, "alive_particles": alive,
+                       "grids": "r in {64,128,256} x z in {256,512,1024} cells",
+                       "parallelism": "replicas x%d" % world},
+            "ensemble": {"blocks_per_sm": bpsm, "blocks": info["blocks"],
+                         "cuda_graph": bool(info["used_graph"]), "ms_per_step": ms / args.steps},
+            "sequential": {"value": seq_value, "ms_per_step": seq_ms / args.steps,
+                           "note": "same runs, each stepped alone with per-run launches"},
+            "ensemble_over_sequential": value / seq_value,
+            "clocks": clk}), flush=True)
+    ens.close()
+    for s_ in sims:
+        s_.close()
     return 0
 
 

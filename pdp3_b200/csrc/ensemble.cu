@@ -25,17 +25,6 @@ namespace cg = cooperative_groups;
 
 namespace pdp3g {
 
-// largest index j with prefix[j] <= x (prefix ascending, prefix[0] = 0)
-template <typename F>
-__device__ __forceinline__ int find_owner(long long x, int n, F prefix) {
-  int lo = 0, hi = n - 1;
-  while (lo < hi) {
-    const int mid = (lo + hi + 1) >> 1;
-    if (prefix(mid) <= x) lo = mid; else hi = mid - 1;
-  }
-  return lo;
-}
-
 // Bunch::bunch_inject (src/bunch.cpp:87-124) for one bunch species, by one CTA
 __device__ void ens_inject(const EnsembleDev &E, const EnsSpecies &sp) {
   const EnsRun &run = E.runs[sp.run];
@@ -74,9 +63,14 @@ __device__ void ens_inject(const EnsembleDev &E, const EnsSpecies &sp) {
   }
 }
 
-__global__ void __launch_bounds__(F32_THREADS, 3) k_ensemble(EnsembleDev E, int nsteps) {
+__global__ void __launch_bounds__(F32_THREADS, 4) k_ensemble(EnsembleDev E, int nsteps) {
   cg::grid_group grid = cg::this_grid();
   __shared__ F32Shared sm;
+  __shared__ struct {
+    GridDev g;
+    SpeciesF32 s;
+    int pusher;
+  } desc;
   for (int idx = threadIdx.x; idx < 3 * TILE_CAP; idx += F32_THREADS) sm.acc[idx] = 0.0f;
   __syncthreads();
   const long long gtid = (long long)blockIdx.x * blockDim.x + threadIdx.x;
@@ -95,37 +89,54 @@ __global__ void __launch_bounds__(F32_THREADS, 3) k_ensemble(EnsembleDev E, int 
     // ---- phase A: injection, H update, J clear
     for (int sp = blockIdx.x; sp < E.nspecies; sp += gridDim.x)
       if (E.species[sp].is_bunch) ens_inject(E, E.species[sp]);
-    for (long long x = gtid; x < E.total_h; x += gstride) {
-      const int r = find_owner(x, E.nruns, [&](int j) { return E.runs[j].h_begin; });
-      const GridDev &g = E.runs[r].g;
-      const long long l = x - E.runs[r].h_begin;
-      const int i = (int)(l / (g.nz - 1));
-      yee_h_node(g, i, (int)(l - (long long)i * (g.nz - 1)));
-    }
-    for (long long x = gtid; x < E.total_j; x += gstride) {
-      const int r = find_owner(x, E.nruns, [&](int j) { return E.runs[j].j_begin; });
-      const GridDev &g = E.runs[r].g;
-      const long long l = x - E.runs[r].j_begin;
-      g.jr[l] = 0.0;
-      g.jphi[l] = 0.0;
-      g.jz[l] = 0.0;
+    for (int r = 0; r < E.nruns; r++) {
+      __syncthreads();
+      if (threadIdx.x == 0) desc.g = E.runs[r].g;
+      __syncthreads();
+      const GridDev &g = desc.g;
+      const long long nh = (long long)g.nr * (g.nz - 1);
+      for (long long l = gtid; l < nh; l += gstride) {
+        const int i = (int)(l / (g.nz - 1));
+        yee_h_node(g, i, (int)(l - (long long)i * (g.nz - 1)));
+      }
+      const long long nj = (long long)g.nr * g.nz;
+      for (long long l = gtid; l < nj; l += gstride) {
+        g.jr[l] = 0.0;
+        g.jphi[l] = 0.0;
+        g.jz[l] = 0.0;
+      }
     }
     grid.sync();
-    // ---- phase B: particles
-    for (long long c = blockIdx.x; c < E.total_chunks; c += gridDim.x) {
-      const int sp = find_owner(c, E.nspecies, [&](int j) { return E.species[j].chunk_begin; });
-      const EnsSpecies &S = E.species[sp];
-      const EnsRun &run = E.runs[S.run];
-      f32_chunk(run.g, S.s, run.pusher, c - S.chunk_begin, sm);
+    // ---- phase B: particles.  Global chunk j goes to CTA j mod gridDim.x;
+    // the CTA walks the species in order and keeps the current run's grid
+    // and species descriptors in shared memory, where they cannot alias the
+    // grids and particle arrays that the chunk loop writes.
+    for (int sp = 0; sp < E.nspecies; sp++) {
+      const long long cb = E.species[sp].chunk_begin;
+      const long long ce = sp + 1 < E.nspecies ? E.species[sp + 1].chunk_begin : E.total_chunks;
+      long long first = cb + (((long long)blockIdx.x - cb) % gridDim.x + gridDim.x) % gridDim.x;
+      if (first >= ce) continue;
+      __syncthreads();
+      if (threadIdx.x == 0) {
+        desc.g = E.runs[E.species[sp].run].g;
+        desc.s = E.species[sp].s;
+        desc.pusher = E.runs[E.species[sp].run].pusher;
+      }
+      __syncthreads();
+      for (long long c = first; c < ce; c += gridDim.x) f32_chunk(desc.g, desc.s, desc.pusher, c - cb, sm);
     }
     grid.sync();
     // ---- phase C: E update, t += dt
-    for (long long x = gtid; x < E.total_e; x += gstride) {
-      const int r = find_owner(x, E.nruns, [&](int j) { return E.runs[j].e_begin; });
-      const GridDev &g = E.runs[r].g;
-      const long long l = x - E.runs[r].e_begin;
-      const int i = (int)(l / (g.nz - 1));
-      yee_e_node(g, i, (int)(l - (long long)i * (g.nz - 1)));
+    for (int r = 0; r < E.nruns; r++) {
+      __syncthreads();
+      if (threadIdx.x == 0) desc.g = E.runs[r].g;
+      __syncthreads();
+      const GridDev &g = desc.g;
+      const long long ne = (long long)(g.nr - 1) * (g.nz - 1);
+      for (long long l = gtid; l < ne; l += gstride) {
+        const int i = (int)(l / (g.nz - 1));
+        yee_e_node(g, i, (int)(l - (long long)i * (g.nz - 1)));
+      }
     }
     if (gtid < E.nruns) E.runs[gtid].t = E.runs[gtid].t + E.runs[gtid].g.dt;
     if (gtid == 0) E.status[0] = step + 1;

@@ -1,0 +1,94 @@
+"""The batched ensemble: independent FP32 runs of different grid sizes
+advanced by one persistent kernel (graph-replayed), against the same runs
+stepped one by one; the cancel flag and the time budget stop it with
+PDP3G_TIMEOUT without hanging, and the autotuner picks a feasible shape.
+
+Tolerance: each run's grids within 1e-4 of max|x| of the run stepped alone
+(same arithmetic; the FP32 tile sums and FP64 atomics add in a different
+order)."""
+import numpy as np
+import pytest
+
+from helpers import rel_inf
+from pdp3_b200 import api
+from pdp3_b200 import workloads as W
+
+pytestmark = pytest.mark.gpu
+
+
+def small_runs(n=4):
+    params = W.ensemble_params(seed=77, n_runs=n, cell=1e-3)
+    out = []
+    for i, p in enumerate(params):
+        p = dict(p)
+        p["n_grid_r"] = 17 + 8 * (i % 2)
+        p["n_grid_z"] = 65 + 32 * (i % 3)
+        p["r_size"] = (p["n_grid_r"] - 1) * 1e-3
+        p["z_size"] = (p["n_grid_z"] - 1) * 1e-3
+        p["ppc"] = 4 + 2 * i
+        out.append(W.ensemble_run_workload(p, steps=10))
+    return out
+
+
+def test_ensemble_matches_runs_stepped_alone():
+    wls = small_runs()
+    alone = [api.from_workload(wl, precision="fp32") for wl in wls]
+    batch = [api.from_workload(wl, precision="fp32") for wl in wls]
+    for s in alone:
+        s.step(10)
+        s.sync()
+    ens = api.Ensemble(batch)
+    ens.run(10)
+    info = ens.info()
+    assert info["last_steps_done"] == 10
+    assert info["runs"] == len(wls)
+    for a, b in zip(alone, batch):
+        b.sync()
+        assert a.time == b.time
+        for c in ("E_r", "E_z", "H_phi", "J_z", "J_r", "J_phi"):
+            assert rel_inf(b.field(c), a.field(c)) <= 1e-4, c
+        assert np.array_equal(a.species(2)["alive"], b.species(2)["alive"])
+    ens.close()
+
+
+def test_ensemble_cancel_and_budget_stop_without_hanging():
+    wls = small_runs(2)
+    sims = [api.from_workload(wl, precision="fp32") for wl in wls]
+    ens = api.Ensemble(sims)
+    t0 = [s.time for s in sims]
+    ens.cancel(True)
+    assert ens.run_status(5) == 6  # PDP3G_TIMEOUT
+    assert ens.info()["last_steps_done"] == 0
+    assert [s.time for s in sims] == t0
+    ens.cancel(False)
+    ens.set_budget(1e-9)  # milliseconds: exhausted right away
+    st = ens.run_status(1000)
+    assert st == 6
+    done = ens.info()["last_steps_done"]
+    assert 0 <= done < 1000
+    ens.set_budget(0)
+    ens.run(3)
+    assert ens.info()["last_steps_done"] == 3
+    for s in sims:
+        s.sync()
+    ens.close()
+
+
+def test_ensemble_autotune_and_graph():
+    sims = [api.from_workload(wl, precision="fp32") for wl in small_runs(3)]
+    ens = api.Ensemble(sims)
+    b = ens.autotune(2)
+    assert b >= 1
+    ens.run(4)
+    ens.run(4)  # second call replays the captured graph
+    info = ens.info()
+    assert info["blocks_per_sm"] == b and info["last_steps_done"] == 4
+    assert info["used_graph"] in (0, 1)
+    ens.close()
+
+
+def test_ensemble_rejects_fp64_runs():
+    wl = small_runs(1)[0]
+    sim = api.from_workload(wl, precision="fp64")
+    with pytest.raises(api.Pdp3gError):
+        api.Ensemble([sim])
