@@ -236,6 +236,50 @@ pdp3g_status pdp3g_ensemble_info(pdp3g_ensemble *e, pdp3g_ensemble_stats *out);
 const char *pdp3g_ensemble_last_error(pdp3g_ensemble *e);
 void pdp3g_ensemble_destroy(pdp3g_ensemble *e);
 
+/* ---- Adjoint window (no upstream counterpart: the upstream has no
+   derivatives).  A forward/backward vector-Jacobian pair over window_steps
+   steps of a PDP3G_FP32_CELL context with the relativistic Boris pusher.
+   Loss: sum over the probe nodes i in [probe_r0, probe_r1), k in
+   [probe_z0, probe_z1) of E_z(i, k)^2 V_i after the window, with V_i the
+   node's ring volume 2 pi i dr^2 dz (pi dr^2 dz / 4 on the axis).
+   pdp3g_forward_window steps the context window_steps steps (no re-sorting,
+   so every particle keeps its slot), storing E, H and the particle state
+   every checkpoint_interval steps and at the end, and returns the loss.
+   pdp3g_backward_window recomputes each interval from its checkpoint
+   (storing every step's particle-phase input) and runs the hand-written
+   reverse of each step, last to first; it leaves the context in the state
+   that the forward ended in.  Results, all with respect to the state at the
+   start of the forward window: per particle dL/dr and dL/dz (per metre),
+   dL/du for u = gamma v / c (r, phi, z) and dL/dw (weight); per grid node
+   dL/dE and dL/dH; per bunch dL/dv for the beam velocity through the
+   injected z offsets and u_z. */
+typedef struct pdp3g_adjoint pdp3g_adjoint;
+pdp3g_status pdp3g_adjoint_create(pdp3g_ctx *ctx, int32_t window_steps,
+                                  int32_t checkpoint_interval, int32_t probe_r0,
+                                  int32_t probe_r1, int32_t probe_z0, int32_t probe_z1,
+                                  pdp3g_adjoint **out);
+pdp3g_status pdp3g_forward_window(pdp3g_adjoint *a, double *loss);
+pdp3g_status pdp3g_backward_window(pdp3g_adjoint *a);
+/* any output pointer may be NULL */
+pdp3g_status pdp3g_adjoint_species(pdp3g_adjoint *a, int32_t id, double *l_r, double *l_z,
+                                   double *l_ur, double *l_uphi, double *l_uz, double *l_w);
+/* comp in PDP3G_E_R .. PDP3G_H_Z */
+pdp3g_status pdp3g_adjoint_field(pdp3g_adjoint *a, int32_t comp, double *host_out);
+pdp3g_status pdp3g_adjoint_bunch_velocity(pdp3g_adjoint *a, int32_t id, double *l_v);
+/* The upstream radial gather weights jump at cell faces (node-centred
+   components) and cell middles (half-node components), so the loss of a
+   many-particle run moves with the particles' density at the jumps, which a
+   per-particle (pathwise) derivative does not see.  PDP3G_ADJ_MEAN_FIELD
+   (the default) adds each particle's expected share of those jump terms for
+   a particle density uniform inside each cell; PDP3G_ADJ_PATHWISE gives the
+   exact derivative of the particles' piecewise-smooth trajectories. */
+enum { PDP3G_ADJ_MEAN_FIELD = 0, PDP3G_ADJ_PATHWISE = 1 };
+pdp3g_status pdp3g_adjoint_set_mode(pdp3g_adjoint *a, int32_t mode);
+/* device time of the last forward and backward calls */
+pdp3g_status pdp3g_adjoint_timing(pdp3g_adjoint *a, double *forward_ms, double *backward_ms);
+int64_t pdp3g_adjoint_bytes(pdp3g_adjoint *a);
+void pdp3g_adjoint_destroy(pdp3g_adjoint *a);
+
 /* The CUDA stream (cudaStream_t) every launch of this context goes to, so a
    caller can order its own work or CUDA events against the step. */
 void *pdp3g_stream(pdp3g_ctx *ctx);

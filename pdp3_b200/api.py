@@ -112,6 +112,16 @@ EXPORTS = [
     ("pdp3g_ensemble_destroy", None, [_VP]),
     ("pdp3g_field_diagnostics_noalloc", _I32, [_VP] * 9 + [_I32, _I32, ctypes.c_double,
                                                           ctypes.c_double, _VP, _VP]),
+    ("pdp3g_adjoint_create", _I32, [_VP] + [_I32] * 6 + [ctypes.POINTER(_VP)]),
+    ("pdp3g_forward_window", _I32, [_VP, _D]),
+    ("pdp3g_backward_window", _I32, [_VP]),
+    ("pdp3g_adjoint_species", _I32, [_VP, _I32] + [_D] * 6),
+    ("pdp3g_adjoint_field", _I32, [_VP, _I32, _D]),
+    ("pdp3g_adjoint_bunch_velocity", _I32, [_VP, _I32, _D]),
+    ("pdp3g_adjoint_timing", _I32, [_VP, _D, _D]),
+    ("pdp3g_adjoint_set_mode", _I32, [_VP, _I32]),
+    ("pdp3g_adjoint_bytes", ctypes.c_int64, [_VP]),
+    ("pdp3g_adjoint_destroy", None, [_VP]),
 ]
 
 
@@ -333,6 +343,80 @@ class Ensemble:
     def close(self):
         if getattr(self, "h", None):
             self.L.pdp3g_ensemble_destroy(self.h)
+            self.h = None
+
+    def __del__(self):
+        try:
+            self.close()
+        except Exception:
+            pass
+
+
+class Adjoint:
+    """Forward/backward (vector-Jacobian) pair over a window of FP32 steps of
+    one Simulation (precision "fp32", relativistic Boris).  loss = sum over
+    the probe nodes [r0, r1) x [z0, z1) of E_z^2 times the node ring volume,
+    after the window.  backward() returns nothing; the gradients with respect
+    to the state at the start of the window are read with species(), field()
+    and bunch_velocity()."""
+
+    def __init__(self, sim, window_steps, checkpoint_interval, probe):
+        self.L = load()
+        self.sim = sim
+        r0, r1, z0, z1 = (int(x) for x in probe)
+        h = _VP()
+        st = self.L.pdp3g_adjoint_create(sim.h, int(window_steps), int(checkpoint_interval),
+                                         r0, r1, z0, z1, ctypes.byref(h))
+        sim._check(st, "adjoint_create")
+        self.h = h
+
+    def forward(self):
+        loss = ctypes.c_double()
+        self.sim._check(self.L.pdp3g_forward_window(self.h, ctypes.byref(loss)), "forward_window")
+        return loss.value
+
+    def backward(self):
+        self.sim._check(self.L.pdp3g_backward_window(self.h), "backward_window")
+
+    def species(self, sid):
+        """dL/d(initial state) of species sid: r, z (per metre), ur, uphi, uz
+        (u = gamma v / c) and w (weight)."""
+        n = self.sim.species_size(sid)
+        out = {k: np.empty(n) for k in ("r", "z", "ur", "uphi", "uz", "w")}
+        self.sim._check(self.L.pdp3g_adjoint_species(
+            self.h, sid, *[_p(out[k]) for k in ("r", "z", "ur", "uphi", "uz", "w")]),
+            "adjoint_species")
+        return out
+
+    def field(self, name):
+        out = np.empty(self.sim.nr * self.sim.nz)
+        self.sim._check(self.L.pdp3g_adjoint_field(self.h, COMP[name], _p(out)), "adjoint_field")
+        return out.reshape(self.sim.nr, self.sim.nz)
+
+    def bunch_velocity(self, sid):
+        v = ctypes.c_double()
+        self.sim._check(self.L.pdp3g_adjoint_bunch_velocity(self.h, sid, ctypes.byref(v)),
+                        "adjoint_bunch_velocity")
+        return v.value
+
+    def set_mode(self, mode):
+        """"mean_field" (default: adds the expected gather-jump terms) or
+        "pathwise" (the exact derivative of each particle's trajectory)."""
+        self.sim._check(self.L.pdp3g_adjoint_set_mode(
+            self.h, {"mean_field": 0, "pathwise": 1}[mode]), "adjoint_set_mode")
+
+    def timing(self):
+        f, b = ctypes.c_double(), ctypes.c_double()
+        self.sim._check(self.L.pdp3g_adjoint_timing(self.h, ctypes.byref(f), ctypes.byref(b)),
+                        "adjoint_timing")
+        return {"forward_ms": f.value, "backward_ms": b.value}
+
+    def device_bytes(self):
+        return self.L.pdp3g_adjoint_bytes(self.h)
+
+    def close(self):
+        if getattr(self, "h", None):
+            self.L.pdp3g_adjoint_destroy(self.h)
             self.h = None
 
     def __del__(self):

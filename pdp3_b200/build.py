@@ -32,8 +32,9 @@ UNITS = {
     "ensemble.cu": ["--prec-div=false", "--prec-sqrt=false"],
     "diag.cu": [],
     "noalloc.cu": [],
+    "adjoint.cu": ["--prec-div=false", "--prec-sqrt=false"],
 }
-HEADERS = ["pdp3g_internal.cuh", "particles_f32.cuh", "fields_body.cuh"]
+HEADERS = ["pdp3g_internal.cuh", "particles_f32.cuh", "fields_body.cuh", "adjoint_particle.cuh"]
 
 
 def nvcc():

@@ -534,37 +534,47 @@ pdp3g_status pdp3g_sort(pdp3g_ctx *ctx) {
 
 // ---- the step's phases (LoadInitParam::run, src/loadInitParam.cpp:481-527, 586)
 
+// Bunch::bunch_inject's schedule (src/bunch.cpp:87-124): the slots
+// [start, start + count) that the bunch injects at time t (count 0: none)
+static void inject_range(const pdp3g_ctx *ctx, const Species &sp, double t, long long &start,
+                         long long &count) {
+  start = 0;
+  count = 0;
+  const double dt = ctx->cfg.dt;
+  double begin = sp.duration * sp.bunch_number + sp.hole_duration * sp.bunch_number;
+  double end = begin + sp.duration;
+  int steps_amount = (int)std::ceil(sp.duration / dt);
+  unsigned int number = (unsigned int)(sp.fp32 ? sp.f32.n : sp.dev.n);
+  unsigned int particles_in_step = number / steps_amount;
+  int start_number = (t - begin) / dt * particles_in_step;
+  if (t >= begin && t < end && particles_in_step > 0) {
+    // indices start_number + i for i < particles_in_step, kept below number
+    start = (long long)(unsigned int)start_number;
+    count = particles_in_step;
+    if (start >= (long long)number) count = 0;
+    else if (start + count > (long long)number) count = (long long)number - start;
+  }
+}
+
 // Bunch::bunch_inject for every bunch (src/bunch.cpp:87-124)
 static void phase_inject(pdp3g_ctx *ctx) {
   cudaStream_t st = ctx->stream;
   for (auto &sp : ctx->species) {
     if (!sp.is_bunch) continue;
-    const double dt = ctx->cfg.dt;
-    double begin = sp.duration * sp.bunch_number + sp.hole_duration * sp.bunch_number;
-    double end = begin + sp.duration;
-    double dl = sp.velocity * dt;
-    int steps_amount = (int)std::ceil(sp.duration / dt);
-    unsigned int number = (unsigned int)(sp.fp32 ? sp.f32.n : sp.dev.n);
-    unsigned int particles_in_step = number / steps_amount;
-    int start_number = (ctx->t - begin) / dt * particles_in_step;
-    if (ctx->t >= begin && ctx->t < end && particles_in_step > 0) {
-      // indices start_number + i for i < particles_in_step, kept below number
-      long long start = (long long)(unsigned int)start_number;
-      long long count = particles_in_step;
-      if (start >= (long long)number) count = 0;
-      else if (start + count > (long long)number) count = (long long)number - start;
-      if (count > 0) {
-        if (sp.fp32) {
-          const double gv = sp.velocity / (LIGHT_SPEED * std::sqrt(1.0 - sp.velocity * sp.velocity /
-                                                                              LIGHT_SPEED_POW_2));
-          launch_bunch_inject_f32(sp.f32, start, count, dl, ctx->dz / 2.0, ctx->dz,
-                                  ctx->cfg.n_grid_z - 1, (float)gv, ctx->d_inv_pow11, st);
-        } else {
-          launch_bunch_inject(sp.dev, start, count, dl, ctx->dz / 2.0, sp.velocity,
-                              ctx->d_inv_pow11, st);
-        }
-        ctx->launches++;
+    long long start, count;
+    inject_range(ctx, sp, ctx->t, start, count);
+    if (count > 0) {
+      const double dl = sp.velocity * ctx->cfg.dt;
+      if (sp.fp32) {
+        const double gv = sp.velocity / (LIGHT_SPEED * std::sqrt(1.0 - sp.velocity * sp.velocity /
+                                                                            LIGHT_SPEED_POW_2));
+        launch_bunch_inject_f32(sp.f32, start, count, dl, ctx->dz / 2.0, ctx->dz,
+                                ctx->cfg.n_grid_z - 1, (float)gv, ctx->d_inv_pow11, st);
+      } else {
+        launch_bunch_inject(sp.dev, start, count, dl, ctx->dz / 2.0, sp.velocity,
+                            ctx->d_inv_pow11, st);
       }
+      ctx->launches++;
     }
   }
 }
@@ -1085,7 +1095,9 @@ pdp3g_status pdp3g_ensemble_create(pdp3g_ctx *const *runs, int32_t n_runs, pdp3g
 
 static pdp3g_status ens_launch(pdp3g_ensemble *e, int nsteps, bool allow_graph) {
   const int blocks = e->n_sm * e->blocks_per_sm;
-  e->dev.budget_cycles = e->budget_ms > 0 ? (long long)(e->budget_ms * e->clock_khz) : 0;
+  // 0 means no budget; any positive budget is at least one cycle
+  e->dev.budget_cycles =
+      e->budget_ms > 0 ? std::max<long long>(1, (long long)std::ceil(e->budget_ms * e->clock_khz)) : 0;
   e->last_used_graph = false;
   if (allow_graph && e->graph_ok) {
     if (e->exec && (e->graph_steps != nsteps || e->graph_blocks != blocks)) {
@@ -1099,7 +1111,23 @@ static pdp3g_status ens_launch(pdp3g_ensemble *e, int nsteps, bool allow_graph) 
       cudaError_t c2 = c1 == cudaSuccess ? ensemble_launch(e->dev, nsteps, blocks, e->stream) : c1;
       cudaGraph_t g = nullptr;
       cudaError_t c3 = c1 == cudaSuccess ? cudaStreamEndCapture(e->stream, &g) : c1;
-      cudaError_t c4 = (c2 == cudaSuccess && c3 == cudaSuccess)
+      // the captured node must keep the cooperative attribute: the kernel's
+      // grid-wide barriers need co-resident CTAs
+      bool coop = false;
+      if (c2 == cudaSuccess && c3 == cudaSuccess && g) {
+        size_t nn = 0;
+        if (cudaGraphGetNodes(g, nullptr, &nn) == cudaSuccess && nn == 1) {
+          cudaGraphNode_t node;
+          cudaGraphNodeType ty;
+          cudaLaunchAttributeValue v = {};
+          if (cudaGraphGetNodes(g, &node, &nn) == cudaSuccess &&
+              cudaGraphNodeGetType(node, &ty) == cudaSuccess && ty == cudaGraphNodeTypeKernel &&
+              cudaGraphKernelNodeGetAttribute(node, cudaLaunchAttributeCooperative, &v) ==
+                  cudaSuccess)
+            coop = v.cooperative != 0;
+        }
+      }
+      cudaError_t c4 = (c2 == cudaSuccess && c3 == cudaSuccess && coop)
                            ? cudaGraphInstantiate(&e->exec, g, 0)
                            : cudaErrorUnknown;
       if (c4 == cudaSuccess) {
@@ -1213,3 +1241,379 @@ pdp3g_status pdp3g_ensemble_info(pdp3g_ensemble *e, pdp3g_ensemble_stats *out) {
 const char *pdp3g_ensemble_last_error(pdp3g_ensemble *e) { return e ? e->last_error.c_str() : ""; }
 
 }  // extern "C"
+
+// ------------------------------------------------------------------ adjoint
+// Forward/backward (vector-Jacobian) pair over a window of FP32 steps.  The
+// forward stores the fields (E, H) and the particle state at the start of
+// every checkpoint interval and at the end; the backward walks the
+// intervals last to first, recomputes each interval's steps from its
+// checkpoint while storing every step's particle-phase input (particle
+// state after injection, E and the half-step H), then runs the reverse of
+// each step (adjoint.cu) from the last step of the interval to the first.
+
+namespace {
+
+struct AdjSnap {  // one species' FP32 particle state
+  int *cell = nullptr;
+  float *fr = nullptr, *fz = nullptr, *ur = nullptr, *uphi = nullptr, *uz = nullptr;
+  uint8_t *alive = nullptr;
+};
+
+}  // namespace
+
+struct pdp3g_adjoint {
+  pdp3g_ctx *ctx = nullptr;
+  int window = 0, interval = 0, r0 = 0, r1 = 0, z0 = 0, z1 = 0;
+  int nwin = 0;
+  std::vector<void *> allocs;
+  int64_t bytes = 0;
+  AdjGrids A{};
+  double *lgrids = nullptr;  // 12 grids: lE, lH, lHh, lJ
+  std::vector<AdjSpeciesDev> ls;
+  double *d_lv = nullptr;    // per species: adjoint of the bunch velocity
+  double *d_loss = nullptr;
+  double *ck_fields = nullptr;                 // (nwin + 1) x 6 grids (E, H)
+  std::vector<std::vector<AdjSnap>> ck_parts;  // [nwin + 1][species]
+  std::vector<double> ck_t;
+  std::vector<int64_t> ck_steps;
+  double *cap_fields = nullptr;                // interval x 6 grids (E, H half)
+  std::vector<std::vector<AdjSnap>> cap_parts; // [interval][species]
+  std::vector<double> cap_t;
+  bool have_forward = false;
+  int face_terms = 1;
+  double loss = 0;
+  float fwd_ms = 0, bwd_ms = 0;
+  cudaEvent_t ev0 = nullptr, ev1 = nullptr;
+};
+
+namespace {
+
+template <typename T>
+cudaError_t aalloc(pdp3g_adjoint *a, T **p, size_t count) {
+  cudaError_t e = cudaMalloc((void **)p, sizeof(T) * (count ? count : 1));
+  if (e == cudaSuccess) {
+    a->allocs.push_back((void *)*p);
+    a->bytes += (int64_t)(sizeof(T) * count);
+  }
+  return e;
+}
+
+cudaError_t snap_alloc(pdp3g_adjoint *a, const SpeciesF32 &f, AdjSnap &s) {
+  const size_t n = (size_t)f.n;
+  cudaError_t e;
+  if ((e = aalloc(a, &s.cell, n)) != cudaSuccess) return e;
+  if ((e = aalloc(a, &s.fr, n)) != cudaSuccess) return e;
+  if ((e = aalloc(a, &s.fz, n)) != cudaSuccess) return e;
+  if ((e = aalloc(a, &s.ur, n)) != cudaSuccess) return e;
+  if ((e = aalloc(a, &s.uphi, n)) != cudaSuccess) return e;
+  if ((e = aalloc(a, &s.uz, n)) != cudaSuccess) return e;
+  if (f.alive && (e = aalloc(a, &s.alive, n)) != cudaSuccess) return e;
+  return cudaSuccess;
+}
+
+// dir 0: species -> snapshot, 1: snapshot -> species
+cudaError_t snap_copy(const SpeciesF32 &f, const AdjSnap &s, int dir, cudaStream_t st) {
+  const size_t n = (size_t)f.n;
+  void *dev[7] = {f.cell, f.fr, f.fz, f.ur, f.uphi, f.uz, f.alive};
+  void *snp[7] = {s.cell, s.fr, s.fz, s.ur, s.uphi, s.uz, s.alive};
+  const size_t sz[7] = {4, 4, 4, 4, 4, 4, 1};
+  for (int j = 0; j < 7; j++) {
+    if (!dev[j] || !snp[j] || n == 0) continue;
+    cudaError_t e = dir == 0 ? cudaMemcpyAsync(snp[j], dev[j], n * sz[j], cudaMemcpyDeviceToDevice, st)
+                             : cudaMemcpyAsync(dev[j], snp[j], n * sz[j], cudaMemcpyDeviceToDevice, st);
+    if (e != cudaSuccess) return e;
+  }
+  return cudaSuccess;
+}
+
+pdp3g_status adj_save_checkpoint(pdp3g_adjoint *a, int idx) {
+  pdp3g_ctx *ctx = a->ctx;
+  const size_t ng = (size_t)ctx->cfg.n_grid_r * ctx->cfg.n_grid_z;
+  CK(cudaMemcpyAsync(a->ck_fields + (size_t)idx * 6 * ng, comp_ptr(ctx, PDP3G_E_R),
+                     sizeof(double) * 6 * ng, cudaMemcpyDeviceToDevice, ctx->stream));
+  for (size_t j = 0; j < ctx->species.size(); j++)
+    CK(snap_copy(ctx->species[j].f32, a->ck_parts[idx][j], 0, ctx->stream));
+  a->ck_t[idx] = ctx->t;
+  a->ck_steps[idx] = ctx->steps;
+  return PDP3G_OK;
+}
+
+pdp3g_status adj_restore_checkpoint(pdp3g_adjoint *a, int idx) {
+  pdp3g_ctx *ctx = a->ctx;
+  const size_t ng = (size_t)ctx->cfg.n_grid_r * ctx->cfg.n_grid_z;
+  CK(cudaMemcpyAsync(comp_ptr(ctx, PDP3G_E_R), a->ck_fields + (size_t)idx * 6 * ng,
+                     sizeof(double) * 6 * ng, cudaMemcpyDeviceToDevice, ctx->stream));
+  for (size_t j = 0; j < ctx->species.size(); j++)
+    CK(snap_copy(ctx->species[j].f32, a->ck_parts[idx][j], 1, ctx->stream));
+  ctx->t = a->ck_t[idx];
+  ctx->steps = a->ck_steps[idx];
+  return PDP3G_OK;
+}
+
+// one step of the window (LoadInitParam::run's sequence without re-sorting:
+// the adjoint keeps every particle in its slot); cap >= 0 stores the
+// particle-phase input of the step into capture slot cap
+pdp3g_status adj_forward_step(pdp3g_adjoint *a, int cap) {
+  pdp3g_ctx *ctx = a->ctx;
+  const size_t ng = (size_t)ctx->cfg.n_grid_r * ctx->cfg.n_grid_z;
+  if (cap >= 0) a->cap_t[cap] = ctx->t;
+  phase_inject(ctx);
+  if (cap >= 0)
+    for (size_t j = 0; j < ctx->species.size(); j++)
+      CK(snap_copy(ctx->species[j].f32, a->cap_parts[cap][j], 0, ctx->stream));
+  phase_calc_h(ctx);
+  if (cap >= 0) {
+    double *dst = a->cap_fields + (size_t)cap * 6 * ng;
+    CK(cudaMemcpyAsync(dst, comp_ptr(ctx, PDP3G_E_R), sizeof(double) * 3 * ng,
+                       cudaMemcpyDeviceToDevice, ctx->stream));
+    CK(cudaMemcpyAsync(dst + 3 * ng, comp_ptr(ctx, PDP3G_H_R_HALF), sizeof(double) * 3 * ng,
+                       cudaMemcpyDeviceToDevice, ctx->stream));
+  }
+  CK(phase_reset_j(ctx));
+  phase_particles(ctx);
+  phase_calc_e(ctx);
+  phase_advance(ctx);
+  return PDP3G_OK;
+}
+
+// reverse of the step stored in capture slot cap
+void adj_reverse_step(pdp3g_adjoint *a, int cap) {
+  pdp3g_ctx *ctx = a->ctx;
+  const size_t ng = (size_t)ctx->cfg.n_grid_r * ctx->cfg.n_grid_z;
+  cudaStream_t st = ctx->stream;
+  adj_launch_e(ctx->g, a->A, st);
+  const double *E3 = a->cap_fields + (size_t)cap * 6 * ng;
+  for (size_t j = 0; j < ctx->species.size(); j++) {
+    const Species &sp = ctx->species[j];
+    AdjSpeciesDev S = a->ls[j];
+    S.st = sp.f32;
+    const AdjSnap &sn = a->cap_parts[cap][j];
+    S.st.cell = sn.cell;
+    S.st.fr = sn.fr;
+    S.st.fz = sn.fz;
+    S.st.ur = sn.ur;
+    S.st.uphi = sn.uphi;
+    S.st.uz = sn.uz;
+    S.st.alive = sn.alive;
+    adj_launch_particles(ctx->g, E3, E3 + 3 * ng, S, a->A, a->face_terms, st);
+    if (sp.is_bunch) {
+      long long start, count;
+      inject_range(ctx, sp, a->cap_t[cap], start, count);
+      adj_launch_inject(S, start, count, ctx->cfg.dt, ctx->dz, sp.velocity, ctx->d_inv_pow11,
+                        a->d_lv + j, st);
+    }
+  }
+  adj_launch_h(ctx->g, a->A, st);
+}
+
+pdp3g_status adj_fail(pdp3g_adjoint *a, pdp3g_status st, const std::string &m) {
+  if (a && a->ctx) a->ctx->last_error = m;
+  return st;
+}
+
+}  // namespace
+
+void pdp3g_adjoint_destroy(pdp3g_adjoint *a) {
+  if (!a) return;
+  if (a->ctx) cudaSetDevice(a->ctx->device);
+  for (void *p : a->allocs) cudaFree(p);
+  if (a->ev0) cudaEventDestroy(a->ev0);
+  if (a->ev1) cudaEventDestroy(a->ev1);
+  delete a;
+}
+
+pdp3g_status pdp3g_adjoint_create(pdp3g_ctx *ctx, int32_t window_steps,
+                                  int32_t checkpoint_interval, int32_t probe_r0,
+                                  int32_t probe_r1, int32_t probe_z0, int32_t probe_z1,
+                                  pdp3g_adjoint **out) {
+  if (!ctx || !out || window_steps <= 0 || checkpoint_interval <= 0)
+    return fail(ctx, PDP3G_INVALID_ARG, "adjoint_create: bad arguments");
+  *out = nullptr;
+  const int nr = ctx->cfg.n_grid_r, nz = ctx->cfg.n_grid_z;
+  if (probe_r0 < 0 || probe_r1 > nr || probe_r0 >= probe_r1 || probe_z0 < 0 || probe_z1 > nz ||
+      probe_z0 >= probe_z1)
+    return fail(ctx, PDP3G_INVALID_ARG, "adjoint_create: probe outside the grid");
+  if (ctx->cfg.precision != PDP3G_FP32_CELL || ctx->cfg.pusher != PDP3G_PUSHER_BORIS)
+    return fail(ctx, PDP3G_NOT_SUPPORTED,
+                "adjoint: the FP32 cell-local form with the relativistic Boris pusher only");
+  CK(cudaSetDevice(ctx->device));
+  pdp3g_adjoint *a = new pdp3g_adjoint();
+  a->ctx = ctx;
+  a->window = window_steps;
+  a->interval = std::min(checkpoint_interval, window_steps);
+  a->nwin = (window_steps + a->interval - 1) / a->interval;
+  a->r0 = probe_r0;
+  a->r1 = probe_r1;
+  a->z0 = probe_z0;
+  a->z1 = probe_z1;
+  const size_t ng = (size_t)nr * nz;
+  const size_t nsp = ctx->species.size();
+  cudaError_t e = cudaSuccess;
+#define ACK(call)                                   \
+  do {                                              \
+    e = (call);                                     \
+    if (e != cudaSuccess) {                         \
+      pdp3g_adjoint_destroy(a);                     \
+      return cuda_fail(ctx, e, #call);              \
+    }                                               \
+  } while (0)
+  ACK(aalloc(a, &a->lgrids, 12 * ng));
+  double *L = a->lgrids;
+  a->A = AdjGrids{L, L + ng, L + 2 * ng, L + 3 * ng, L + 4 * ng, L + 5 * ng,
+                  L + 6 * ng, L + 7 * ng, L + 8 * ng, L + 9 * ng, L + 10 * ng, L + 11 * ng};
+  a->ls.resize(nsp);
+  for (size_t j = 0; j < nsp; j++) {
+    const size_t n = (size_t)ctx->species[j].f32.n;
+    AdjSpeciesDev &S = a->ls[j];
+    ACK(aalloc(a, &S.la, n));
+    ACK(aalloc(a, &S.lb, n));
+    ACK(aalloc(a, &S.lur, n));
+    ACK(aalloc(a, &S.luphi, n));
+    ACK(aalloc(a, &S.luz, n));
+    ACK(aalloc(a, &S.lw, n));
+  }
+  ACK(aalloc(a, &a->d_lv, nsp + 1));
+  ACK(aalloc(a, &a->d_loss, 1));
+  ACK(aalloc(a, &a->ck_fields, (size_t)(a->nwin + 1) * 6 * ng));
+  a->ck_parts.assign(a->nwin + 1, std::vector<AdjSnap>(nsp));
+  a->ck_t.assign(a->nwin + 1, 0.0);
+  a->ck_steps.assign(a->nwin + 1, 0);
+  for (int c = 0; c <= a->nwin; c++)
+    for (size_t j = 0; j < nsp; j++) ACK(snap_alloc(a, ctx->species[j].f32, a->ck_parts[c][j]));
+  ACK(aalloc(a, &a->cap_fields, (size_t)a->interval * 6 * ng));
+  a->cap_parts.assign(a->interval, std::vector<AdjSnap>(nsp));
+  a->cap_t.assign(a->interval, 0.0);
+  for (int c = 0; c < a->interval; c++)
+    for (size_t j = 0; j < nsp; j++) ACK(snap_alloc(a, ctx->species[j].f32, a->cap_parts[c][j]));
+  ACK(cudaEventCreate(&a->ev0));
+  ACK(cudaEventCreate(&a->ev1));
+#undef ACK
+  *out = a;
+  return PDP3G_OK;
+}
+
+pdp3g_status pdp3g_forward_window(pdp3g_adjoint *a, double *loss) {
+  if (!a) return PDP3G_INVALID_ARG;
+  pdp3g_ctx *ctx = a->ctx;
+  CK(cudaSetDevice(ctx->device));
+  cudaStream_t st = ctx->stream;
+  const size_t ng = (size_t)ctx->cfg.n_grid_r * ctx->cfg.n_grid_z;
+  CK(cudaEventRecord(a->ev0, st));
+  for (int s = 0; s < a->window; s++) {
+    if (s % a->interval == 0) {
+      pdp3g_status cs = adj_save_checkpoint(a, s / a->interval);
+      if (cs != PDP3G_OK) return cs;
+    }
+    pdp3g_status fs = adj_forward_step(a, -1);
+    if (fs != PDP3G_OK) return fs;
+  }
+  pdp3g_status cs = adj_save_checkpoint(a, a->nwin);
+  if (cs != PDP3G_OK) return cs;
+  CK(cudaMemsetAsync(a->d_loss, 0, sizeof(double), st));
+  CK(cudaMemsetAsync(a->A.lEz, 0, sizeof(double) * ng, st));
+  adj_launch_seed(ctx->g, a->A, a->r0, a->r1, a->z0, a->z1, a->d_loss, st);
+  CK(cudaEventRecord(a->ev1, st));
+  CK(cudaMemcpyAsync(&a->loss, a->d_loss, sizeof(double), cudaMemcpyDeviceToHost, st));
+  pdp3g_status ss = pdp3g_sync(ctx);
+  if (ss != PDP3G_OK) return ss;
+  CK(cudaEventElapsedTime(&a->fwd_ms, a->ev0, a->ev1));
+  a->have_forward = true;
+  if (loss) *loss = a->loss;
+  return PDP3G_OK;
+}
+
+pdp3g_status pdp3g_backward_window(pdp3g_adjoint *a) {
+  if (!a) return PDP3G_INVALID_ARG;
+  pdp3g_ctx *ctx = a->ctx;
+  if (!a->have_forward)
+    return adj_fail(a, PDP3G_INVALID_ARG, "backward_window: no forward_window to reverse");
+  CK(cudaSetDevice(ctx->device));
+  cudaStream_t st = ctx->stream;
+  const size_t ng = (size_t)ctx->cfg.n_grid_r * ctx->cfg.n_grid_z;
+  CK(cudaEventRecord(a->ev0, st));
+  CK(cudaMemsetAsync(a->lgrids, 0, sizeof(double) * 12 * ng, st));
+  for (size_t j = 0; j < a->ls.size(); j++) {
+    const size_t n = (size_t)ctx->species[j].f32.n;
+    AdjSpeciesDev &S = a->ls[j];
+    float *fl[5] = {S.la, S.lb, S.lur, S.luphi, S.luz};
+    for (float *p : fl) CK(cudaMemsetAsync(p, 0, sizeof(float) * n, st));
+    CK(cudaMemsetAsync(S.lw, 0, sizeof(double) * n, st));
+  }
+  CK(cudaMemsetAsync(a->d_lv, 0, sizeof(double) * (a->ls.size() + 1), st));
+  pdp3g_status rs = adj_restore_checkpoint(a, a->nwin);
+  if (rs != PDP3G_OK) return rs;
+  CK(cudaMemsetAsync(a->d_loss, 0, sizeof(double), st));
+  adj_launch_seed(ctx->g, a->A, a->r0, a->r1, a->z0, a->z1, a->d_loss, st);
+  for (int w = a->nwin - 1; w >= 0; w--) {
+    const int s0 = w * a->interval, s1 = std::min(a->window, s0 + a->interval);
+    rs = adj_restore_checkpoint(a, w);
+    if (rs != PDP3G_OK) return rs;
+    for (int s = s0; s < s1; s++) {
+      pdp3g_status fs = adj_forward_step(a, s - s0);
+      if (fs != PDP3G_OK) return fs;
+    }
+    for (int s = s1 - 1; s >= s0; s--) adj_reverse_step(a, s - s0);
+  }
+  rs = adj_restore_checkpoint(a, a->nwin);
+  if (rs != PDP3G_OK) return rs;
+  CK(cudaEventRecord(a->ev1, st));
+  CK(cudaGetLastError());
+  pdp3g_status ss = pdp3g_sync(ctx);
+  if (ss != PDP3G_OK) return ss;
+  CK(cudaEventElapsedTime(&a->bwd_ms, a->ev0, a->ev1));
+  return PDP3G_OK;
+}
+
+pdp3g_status pdp3g_adjoint_species(pdp3g_adjoint *a, int32_t id, double *l_r, double *l_z,
+                                   double *l_ur, double *l_uphi, double *l_uz, double *l_w) {
+  if (!a || id < 0 || id >= (int32_t)a->ls.size()) return PDP3G_INVALID_ARG;
+  pdp3g_ctx *ctx = a->ctx;
+  CK(cudaSetDevice(ctx->device));
+  const size_t n = (size_t)ctx->species[id].f32.n;
+  const AdjSpeciesDev &S = a->ls[id];
+  std::vector<float> buf(n);
+  const float *src[5] = {S.la, S.lb, S.lur, S.luphi, S.luz};
+  double *dst[5] = {l_r, l_z, l_ur, l_uphi, l_uz};
+  const double scale[5] = {1.0 / ctx->dr, 1.0 / ctx->dz, 1.0, 1.0, 1.0};
+  for (int j = 0; j < 5; j++) {
+    if (!dst[j] || n == 0) continue;
+    CK(cudaMemcpy(buf.data(), src[j], sizeof(float) * n, cudaMemcpyDeviceToHost));
+    for (size_t p = 0; p < n; p++) dst[j][p] = (double)buf[p] * scale[j];
+  }
+  if (l_w && n) CK(cudaMemcpy(l_w, S.lw, sizeof(double) * n, cudaMemcpyDeviceToHost));
+  return PDP3G_OK;
+}
+
+pdp3g_status pdp3g_adjoint_field(pdp3g_adjoint *a, int32_t comp, double *host_out) {
+  if (!a || !host_out || comp < PDP3G_E_R || comp > PDP3G_H_Z) return PDP3G_INVALID_ARG;
+  pdp3g_ctx *ctx = a->ctx;
+  CK(cudaSetDevice(ctx->device));
+  const size_t ng = (size_t)ctx->cfg.n_grid_r * ctx->cfg.n_grid_z;
+  CK(cudaMemcpy(host_out, a->lgrids + (size_t)comp * ng, sizeof(double) * ng,
+                cudaMemcpyDeviceToHost));
+  return PDP3G_OK;
+}
+
+pdp3g_status pdp3g_adjoint_bunch_velocity(pdp3g_adjoint *a, int32_t id, double *l_v) {
+  if (!a || !l_v || id < 0 || id >= (int32_t)a->ls.size()) return PDP3G_INVALID_ARG;
+
+  pdp3g_ctx *ctx = a->ctx;
+  CK(cudaSetDevice(ctx->device));
+  CK(cudaMemcpy(l_v, a->d_lv + id, sizeof(double), cudaMemcpyDeviceToHost));
+  return PDP3G_OK;
+}
+
+pdp3g_status pdp3g_adjoint_timing(pdp3g_adjoint *a, double *forward_ms, double *backward_ms) {
+  if (!a) return PDP3G_INVALID_ARG;
+  if (forward_ms) *forward_ms = a->fwd_ms;
+  if (backward_ms) *backward_ms = a->bwd_ms;
+  return PDP3G_OK;
+}
+
+int64_t pdp3g_adjoint_bytes(pdp3g_adjoint *a) { return a ? a->bytes : 0; }
+
+pdp3g_status pdp3g_adjoint_set_mode(pdp3g_adjoint *a, int32_t mode) {
+  if (!a || (mode != PDP3G_ADJ_MEAN_FIELD && mode != PDP3G_ADJ_PATHWISE)) return PDP3G_INVALID_ARG;
+  a->face_terms = mode == PDP3G_ADJ_MEAN_FIELD;
+  return PDP3G_OK;
+}

@@ -192,4 +192,29 @@ void launch_bunch_inject(const SpeciesDev &s, long long start, long long count, 
                          double half_dz, double velocity, const double *inv_pow11,
                          cudaStream_t st);
 
+// Adjoint (adjoint.cu): FP64 adjoint grids of one context and the adjoint
+// particle state of one FP32 species.
+struct AdjGrids {
+  double *lEr, *lEphi, *lEz;     // adjoint of E
+  double *lHr, *lHphi, *lHz;     // adjoint of H
+  double *lHhr, *lHhphi, *lHhz;  // adjoint of the half-step H of the current step
+  double *lJr, *lJphi, *lJz;     // adjoint of the current step's J
+};
+
+struct AdjSpeciesDev {
+  SpeciesF32 st;  // stored input state of the particle phase of the step
+  float *la, *lb, *lur, *luphi, *luz;  // adjoints of fr, fz, ur, uphi, uz
+  double *lw;                          // adjoint of w (accumulated over steps)
+};
+
+void adj_launch_e(const GridDev &g, const AdjGrids &A, cudaStream_t st);
+void adj_launch_h(const GridDev &g, const AdjGrids &A, cudaStream_t st);
+void adj_launch_particles(const GridDev &g, const double *E3, const double *Hh3,
+                          const AdjSpeciesDev &S, const AdjGrids &A, int face, cudaStream_t st);
+void adj_launch_inject(const AdjSpeciesDev &S, long long start, long long count, double dt,
+                       double dz, double velocity, const double *inv_pow11, double *lv,
+                       cudaStream_t st);
+void adj_launch_seed(const GridDev &g, const AdjGrids &A, int r0, int r1, int z0, int z1,
+                     double *loss, cudaStream_t st);
+
 }  // namespace pdp3g

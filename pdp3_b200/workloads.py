@@ -188,3 +188,171 @@ def small_config(seed=7, n_grid_r=17, n_grid_z=33, r_size=0.01, z_size=0.04, ppc
                       "reverse", seed)
     return Workload("small_%dx%d" % (n_grid_r - 1, n_grid_z - 1), r_size, z_size, n_grid_r,
                     n_grid_z, courant_dt(dr, dz), steps, pml, pusher, sp, bm)
+
+
+def ensemble_params(seed=1005, n_runs=64, cell=3.90625e-4):
+    """Run parameters of the batched-ensemble case: grids drawn uniformly from
+    r in {64, 128, 256} x z in {256, 512, 1024} cells (cell size fixed), 16-64
+    ppc, density log-uniform in [1e15, 1e17] m^-3, an electron bunch with
+    gamma uniform in [3, 10] per run.  Returns one dict per run; build each
+    Workload with ensemble_run_workload (so only one run's arrays are on the
+    host at a time)."""
+    rng = np.random.default_rng(seed)
+    runs = []
+    for r in range(n_runs):
+        nrc = int(rng.choice([64, 128, 256]))
+        nzc = int(rng.choice([256, 512, 1024]))
+        runs.append({"seed": seed * 1000 + r, "n_grid_r": nrc + 1, "n_grid_z": nzc + 1,
+                     "r_size": nrc * cell, "z_size": nzc * cell,
+                     "ppc": int(rng.integers(16, 65)),
+                     "density": float(10 ** rng.uniform(15, 17)),
+                     "gamma": float(rng.uniform(3, 10))})
+    return runs
+
+
+def ensemble_run_workload(p, steps=500):
+    """Workload of one ensemble run (see ensemble_params)."""
+    rng = np.random.default_rng(p["seed"])
+    nr, nz = p["n_grid_r"], p["n_grid_z"]
+    dr = p["r_size"] / (nr - 1)
+    dz = p["z_size"] / (nz - 1)
+    sp = thermal_plasma(rng, p["r_size"], p["z_size"], nr, nz, p["ppc"],
+                        lambda zc: np.full_like(zc, p["density"]), 1.0)
+    radius, length = 0.1 * p["r_size"], 0.05 * p["z_size"]
+    bunch_cells = (radius / dr) * (length / dz)
+    beam = BeamInit(-1.0, 1.0, int(round(64 * bunch_cells)), length, radius, 0.5 * p["density"],
+                    gamma_velocity(p["gamma"]), 1, 0.0, "reverse", p["seed"])
+    return Workload("ens_%dx%d_ppc%d" % (nr - 1, nz - 1, p["ppc"]), p["r_size"], p["z_size"],
+                    nr, nz, courant_dt(dr, dz), steps, absorbing_layer(nr, nz, 10), "boris", sp,
+                    beam)
+
+
+# ---------------------------------------------------------------- adjoint
+
+N_BUMPS = 16
+
+
+def bump_basis(z, z_size, n_bumps=N_BUMPS):
+    """phi_j(z), j < n_bumps: Gaussian bumps exp(-(z - z_j)^2 / (2 sigma^2))
+    centred at z_j = (j + 1/2) Z / n_bumps with sigma = Z / n_bumps, scaled by
+    1 / sqrt(2 pi) so that sum_j phi_j(z) ~ 1 away from the ends (the density
+    is then about the mean coefficient).  Returns an array (z.size, n_bumps)."""
+    z = np.asarray(z, dtype=np.float64)
+    centres = (np.arange(n_bumps) + 0.5) * z_size / n_bumps
+    sig = z_size / n_bumps
+    g = np.exp(-0.5 * ((z[:, None] - centres[None, :]) / sig) ** 2)
+    return g / math.sqrt(2.0 * math.pi)
+
+
+def random_reverse_np(idx, base):
+    """Radical inverse of idx in `base` (upstream random_reverse,
+    src/math/rand.cpp:40-53), vectorised."""
+    x = np.asarray(idx, dtype=np.int64).copy()
+    out = np.zeros(x.shape)
+    scale = 1.0 / base
+    while np.any(x >= 1):
+        out += (x % base) * scale
+        x //= base
+        scale /= base
+    return out
+
+
+def adjoint_theta(seed=1004):
+    """Parameters of the differentiable window: 16 bump coefficients drawn
+    from N(1e17, (1e16)^2) m^-3, bunch gamma 5, bunch radius 5 mm."""
+    rng = np.random.default_rng(seed)
+    return np.concatenate([rng.normal(1e17, 1e16, N_BUMPS), [5.0, 5e-3]])
+
+
+def adjoint_config(theta, seed=1004, n_grid_r=129, n_grid_z=1025, r_size=0.1, z_size=0.8,
+                   ppc=32, steps=500, beam_length=0.02, beam_density=5e16, nominal_radius=5e-3,
+                   bunch_ppc=64):
+    """Differentiable window: 128x1024 cells, 32 ppc per species, background
+    density sum_j c_j phi_j(z) (theta[:16] = c), electron bunch with
+    gamma = theta[16] and radius theta[17] injected at z = 0.  Every
+    particle's position and velocity is independent of theta; weights carry
+    the density and the bunch radius, and the bunch's macroparticle count is
+    fixed by the nominal radius, so theta only moves continuous quantities.
+    Returns (Workload, aux) with aux holding what adjoint_gradient needs."""
+    theta = np.asarray(theta, dtype=np.float64)
+    c, gamma, radius = theta[:N_BUMPS], float(theta[N_BUMPS]), float(theta[N_BUMPS + 1])
+    rng = np.random.default_rng(seed)
+    dr = r_size / (n_grid_r - 1)
+    dz = z_size / (n_grid_z - 1)
+    dens = lambda zc: bump_basis(zc, z_size) @ c
+    sp = thermal_plasma(rng, r_size, z_size, n_grid_r, n_grid_z, ppc, dens, 1.0)
+    # z-cell column of every plasma particle (cells of the particle domain)
+    kc = np.tile(np.repeat(np.arange(n_grid_z - 1, dtype=np.int32), ppc), n_grid_r - 1)
+    bunch_cells = (nominal_radius / dr) * (beam_length / dz)
+    beam = BeamInit(-1.0, 1.0, int(round(bunch_ppc * bunch_cells)), beam_length, radius,
+                    beam_density, gamma_velocity(gamma), 1, 0.0, "reverse", seed)
+    pml = absorbing_layer(n_grid_r, n_grid_z, 10)
+    wl = Workload("adjoint_%dx%d_ppc%d" % (n_grid_r - 1, n_grid_z - 1, ppc), r_size, z_size,
+                  n_grid_r, n_grid_z, courant_dt(dr, dz), steps, pml, "boris", sp, beam)
+    z_edges = np.concatenate(([dz / 2], dz * np.arange(1, n_grid_z - 1), [z_size - dz / 2]))
+    zc = 0.5 * (z_edges[:-1] + z_edges[1:])
+    aux = {"kc": kc, "zc": zc, "theta": theta.copy()}
+    return wl, aux
+
+
+def bunch_init_np(n, radius, duration, velocity, density, dr, dz):
+    """Radii and weights of Bunch::Bunch (src/bunch.cpp:6-80, TESTMODE
+    radial sequence) and their derivatives with respect to the radius."""
+    rnd = random_reverse_np(np.arange(n), 9)
+    r = (radius - dr) * rnd + dr / 2
+    dr_dR = rnd
+    b_len = duration * velocity
+    N_total = PI * radius ** 2 * b_len * density
+    dN_dR = 2.0 * PI * radius * b_len * density
+    far = r > dr
+    vol = np.where(far, 2 * PI * r * dr * dz, PI * r * r * dz)
+    dvol = np.where(far, 2 * PI * dr * dz, 2 * PI * r * dz) * dr_dR
+    v_avg = vol.sum() / n
+    dv_avg = dvol.sum() / n
+    half = r > dr / 2
+    num = np.where(half, 2 * PI * r * dr * dz, PI * (r * r + r * dr + dr * dr / 4) * dz)
+    dnum = np.where(half, 2 * PI * dr * dz, PI * (2 * r + dr) * dz) * dr_dR
+    norm = num / v_avg
+    dnorm = (dnum * v_avg - num * dv_avg) / (v_avg * v_avg)
+    w = N_total / n * norm
+    dw_dR = dN_dR / n * norm + N_total / n * dnorm
+    return r, w, dr_dR, dw_dR
+
+
+def adjoint_gradient(wl, aux, plasma_adj, bunch_adj, bunch_dl_dv):
+    """dL/dtheta from the adjoints of the window's initial state.
+    plasma_adj: per plasma species dict with "w" (dL/dw per particle);
+    bunch_adj: dict with "r" (dL/dr) and "w"; bunch_dl_dv: dL/dv_beam."""
+    theta = aux["theta"]
+    c = theta[:N_BUMPS]
+    phi = bump_basis(aux["zc"], wl.z_size)           # (columns, bumps)
+    n_col = phi @ c
+    g = np.zeros(theta.size)
+    for a, s in zip(plasma_adj, wl.species):
+        # w_p = n(zc) vol/ppc  ->  dw_p/dc_j = w_p phi_j(zc) / n(zc)
+        col = np.bincount(aux["kc"], weights=a["w"] * s.w, minlength=phi.shape[0])
+        g[:N_BUMPS] += (col / n_col) @ phi
+    b = wl.beam
+    gamma = theta[N_BUMPS]
+    v = gamma_velocity(gamma)
+    dv_dgamma = LIGHT_SPEED / (gamma ** 3 * math.sqrt(1.0 - 1.0 / (gamma * gamma)))
+    g[N_BUMPS] = bunch_dl_dv * dv_dgamma
+    _, _, dr_dR, dw_dR = bunch_init_np(b.number_macro, b.radius, b.bunch_length / v, v,
+                                       b.density, wl.dr, wl.dz)
+    g[N_BUMPS + 1] = float(np.dot(bunch_adj["r"], dr_dR) + np.dot(bunch_adj["w"], dw_dR))
+    return g
+
+
+def probe_loss(ez, dr, dz, probe):
+    """sum over probe nodes of E_z^2 times the node ring volume (the loss of
+    the adjoint window)."""
+    r0, r1, z0, z1 = probe
+    i = np.arange(r0, r1, dtype=np.float64)
+    vol = np.where(i == 0, PI * dz * dr * dr / 4.0, 2.0 * PI * dz * dr * dr * i)
+    return float(np.sum(ez[r0:r1, z0:z1] ** 2 * vol[:, None]))
+
+
+# probe nodes (r0, r1, z0, z1): 16 x 64 cells on the axis over z in
+# [0.094, 0.144] m, which holds the bunch's tail and the start of its wake
+# after the 500-step window (the head is then 173 cells from the entrance)
+ADJOINT_PROBE = (0, 16, 120, 184)
