@@ -113,15 +113,21 @@ def make_workload(name, seed, ppc=None):
         return W.wake_config(seed=seed, steps=1000, ppc=ppc or 64)
     if name == "thermal":
         return W.thermal_config(seed=seed, steps=200, ppc=ppc or 32)
+    if name == "large":
+        return W.large_config(ppc=ppc or 64)
     raise ValueError(name)
+
+
+def plasma_species_count(wl):
+    return len(wl.species) + (2 if wl.device_plasma is not None else 0)
 
 
 def species_bytes(sim, wl, precision):
     """Algorithmic bytes of one pass of the particle phase."""
     b = BYTES_PER_PARTICLE[precision]
     total = 0
-    for s in wl.species:
-        total += s.n * b
+    for sid in range(plasma_species_count(wl)):
+        total += sim.species_size(sid) * b
     if wl.beam is not None:
         n_b = wl.beam.number_macro * wl.beam.number_bunches
         total += n_b * 2  # alive flag read (every slot) and written
@@ -129,9 +135,9 @@ def species_bytes(sim, wl, precision):
 
 
 def alive_count(sim, wl):
-    n = sum(s.n for s in wl.species)
-    for sid in range(len(wl.species), len(wl.species) +
-                     (wl.beam.number_bunches if wl.beam is not None else 0)):
+    n_pl = plasma_species_count(wl)
+    n = sum(sim.species_size(sid) for sid in range(n_pl))
+    for sid in range(n_pl, n_pl + (wl.beam.number_bunches if wl.beam is not None else 0)):
         n += int(sim.species(sid)["alive"].sum())
     return n
 
@@ -147,7 +153,20 @@ def cpu_sample_run(wl, steps, warmup, fraction, threads):
     from oracle import refsim
     rng = np.random.default_rng(12345)
     sub = []
-    for s in wl.species:
+    species = wl.species
+    if wl.device_plasma is not None:
+        # plasma generated on the GPU: the sample is the same grid and density
+        # profile at round(ppc * fraction) particles per cell, built on the host
+        from pdp3_b200 import workloads as W
+        dp = wl.device_plasma
+        k_ppc = max(1, int(round(dp.ppc * fraction)))
+        fraction = k_ppc / dp.ppc
+        dens = ((lambda zc: dp.n_max * np.minimum(zc / dp.z_ramp, 1.0)) if dp.z_ramp > 0
+                else (lambda zc: np.full_like(zc, dp.n_max)))
+        species = W.thermal_plasma(np.random.default_rng(dp.seed), dp.r_size, dp.z_size,
+                                   dp.n_grid_r, dp.n_grid_z, k_ppc, dens, dp.t_ev, dp.ion_mass_me)
+        sub = [(s, np.arange(s.n)) for s in species]
+    for s in ([] if sub else species):
         k = max(1, int(s.n * fraction))
         idx = np.sort(rng.choice(s.n, size=k, replace=False))
         sub.append((s, idx))
@@ -230,7 +249,12 @@ def main():
     ap.add_argument("--impl", default="ours", choices=["ours", "reference"])
     ap.add_argument("--precision", default="fp32", choices=["fp64", "fp32"],
                     help="the form reported as value (the other is measured beside it)")
-    ap.add_argument("--workload", default="wake", choices=["wake", "thermal", "ensemble"])
+    ap.add_argument("--workload", default="wake",
+                    choices=["wake", "thermal", "large", "ensemble", "adjoint"])
+    ap.add_argument("--adjoint-fd-params", default="near",
+                    help="parameters checked by finite differences in --workload adjoint: "
+                         "'near' (the 4 density bumps nearest the probe, gamma, radius), "
+                         "'all', or 'none'")
     ap.add_argument("--ensemble-runs", type=int, default=64)
     ap.add_argument("--ppc", type=int, default=None,
                     help="macroparticles per cell (profiling runs on a smaller case)")
@@ -248,6 +272,8 @@ def main():
         return run_reference(args, rank, world)
     if args.workload == "ensemble":
         return run_ensemble(args, rank, world, local_rank)
+    if args.workload == "adjoint":
+        return run_adjoint(args, rank, world, local_rank)
 
     import torch
     dist = None
@@ -346,8 +372,13 @@ def main():
     # end to end through the public API from pinned host buffers: every step
     # uploads the particle state, steps, and reads the state and E_z back.
     e2e = None
-    if args.e2e_steps > 0:
+    if args.e2e_steps > 0 and wl.device_plasma is None:
         e2e = run_e2e(sim, wl, torch, stream, args.e2e_steps)
+    elif wl.device_plasma is not None:
+        e2e = {"value": None, "unit": UNIT, "h2d_bytes_per_step": None,
+               "d2h_bytes_per_step": None,
+               "note": "not measured: the full-state round trip of this case (~30 GB per "
+                       "step in FP64 host arrays) exceeds the host memory budget"}
 
     cpu = None
     if rank == 0 and world == 1 and not args.no_cpu_baseline:
@@ -380,7 +411,7 @@ def main():
             "roofline": {"bound": "hbm", "achieved": achieved, "peak": peaks.get("hbm_gbs"),
                          "unit": "GB/s", "frac": achieved / peaks.get("hbm_gbs"),
                          "traffic": traffic,
-                         "kernel": "k_push_deposit_%s (all species)" % head_prec[-2:],
+                         "kernel": "k_push_deposit_f%s (all species)" % head_prec[-2:],
                          "peak_source": peak_src,
                          "algorithmic_bytes_per_launch": bytes_particle_phase},
             "e2e": e2e,
@@ -461,6 +492,109 @@ def run_ensemble(args, rank, world, local_rank):
     return 0
 
 
+def fitted_fd_slope(api, W, fam, theta, j, steps, probe, hmax=0.02, npts=4):
+    """dL/dtheta_j of the FP64 form from a cubic fitted to the loss at 2*npts
+    relative steps in [-hmax, hmax] (the loss of a many-particle run is a
+    staircase of small jumps, so a single central difference is noisy).
+    Returns (slope, standard error)."""
+    xs = np.concatenate([-np.arange(npts, 0, -1), np.arange(1, npts + 1)]) * (hmax / npts)
+    ls = []
+    for x in xs:
+        t = theta.copy()
+        t[j] = theta[j] * (1 + x)
+        wl, _ = fam.workload(t)
+        sim = api.from_workload(wl, precision="fp64")
+        sim.step(steps)
+        sim.sync()
+        ls.append(W.probe_loss(sim.field("E_z"), wl.dr, wl.dz, probe))
+        sim.close()
+    X = np.vstack([np.ones_like(xs), xs, xs ** 2, xs ** 3]).T
+    coef = np.linalg.lstsq(X, np.array(ls), rcond=None)[0]
+    resid = np.array(ls) - X @ coef
+    s2 = float(resid @ resid) / max(len(xs) - 4, 1)
+    se = math.sqrt(s2 * np.linalg.inv(X.T @ X)[1, 1])
+    return coef[1] / theta[j], se / abs(theta[j])
+
+
+def run_adjoint(args, rank, world, local_rank):
+    """Differentiable window (128x1024 cells, 32 ppc per species, gamma=5
+    bunch, 500 steps, checkpoints every 50): device time of the forward and
+    backward window, and the gradient against FP64 finite differences.
+    value = forward-window particle-steps/s."""
+    import torch
+    from pdp3_b200 import api
+    from pdp3_b200 import workloads as W
+    torch.cuda.set_device(local_rank)
+    steps, interval, probe = 500, 50, W.ADJOINT_PROBE
+    theta = W.adjoint_theta()
+    fam = W.AdjointFamily(theta)
+    wl, aux = fam.workload(theta)
+    sim = api.from_workload(wl, precision="fp32", device=local_rank)
+    adj = api.Adjoint(sim, steps, interval, probe)
+    adj.forward()        # warm-up pair (500 + 1000 steps)
+    adj.backward()
+    clocks = ClockSampler(local_rank)
+    clocks.start()
+    time.sleep(0.3)
+    loss = adj.forward()
+    adj.backward()
+    clk = clocks.stop()
+    t = adj.timing()
+
+    def grad():
+        return W.adjoint_gradient(wl, aux, [adj.species(0), adj.species(1)], adj.species(2),
+                                  adj.bunch_velocity(2))
+    g_mf = grad()
+    adj.set_mode("pathwise")
+    adj.backward()
+    g_pw = grad()
+    n_alive_end = sum(sim.species_size(s) for s in (0, 1)) + int(sim.species(2)["alive"].sum())
+    adj_bytes = adj.device_bytes()
+    adj.close()
+    sim.close()
+    if args.adjoint_fd_params == "none":
+        params = []
+    elif args.adjoint_fd_params == "all":
+        params = list(range(theta.size))
+    else:
+        zc = (np.arange(W.N_BUMPS) + 0.5) * wl.z_size / W.N_BUMPS
+        zp = 0.5 * (probe[2] + probe[3]) * wl.dz
+        params = sorted(np.argsort(np.abs(zc - zp))[:4].tolist()) + [W.N_BUMPS, W.N_BUMPS + 1]
+    fd = {}
+    for j in params:
+        slope, se = fitted_fd_slope(api, W, fam, theta, j, steps, probe)
+        fd[j] = {"fd": slope, "fd_se": se, "mean_field": g_mf[j], "pathwise": g_pw[j],
+                 "rel_err_mean_field": (g_mf[j] - slope) / slope,
+                 "rel_err_pathwise": (g_pw[j] - slope) / slope}
+    dens = [j for j in params if j < W.N_BUMPS]
+    summary = {}
+    if dens:
+        f = np.array([fd[j]["fd"] for j in dens])
+        for mode in ("mean_field", "pathwise"):
+            a = np.array([fd[j][mode] for j in dens])
+            summary["density_block_rel_err_" + mode] = float(np.linalg.norm(a - f) /
+                                                             np.linalg.norm(f))
+    value = wl.n_particles * steps / (t["forward_ms"] / 1000.0)
+    if rank == 0:
+        print(json.dumps({
+            "metric": METRIC, "value": value * world, "unit": UNIT, "n_gpus": world,
+            "steps": steps, "warmup": steps, "ms_per_step": t["forward_ms"] / steps,
+            "higher_is_better": True, "scaling": "weak", "vs_baseline": None,
+            "dtype": "f32+f64acc", "data": "synthetic (seeded)",
+            "config": {"workload": wl.name, "window_steps": steps,
+                       "checkpoint_interval": interval, "probe_nodes": list(probe),
+                       "particles": wl.n_particles, "alive_at_end": n_alive_end,
+                       "parallelism": "replicas x%d" % world},
+            "adjoint": {"loss": loss, "forward_ms": t["forward_ms"],
+                        "backward_ms": t["backward_ms"],
+                        "backward_over_forward": t["backward_ms"] / t["forward_ms"],
+                        "device_bytes": adj_bytes,
+                        "fd": "FP64 form, cubic fit over 8 relative steps in [-2%, 2%]",
+                        "params": {str(j): v for j, v in fd.items()}, "summary": summary},
+            "clocks": clk}), flush=True)
+    return 0
+
+
 def load_traffic(workload, precision, wl):
     """DRAM bytes (read + write) of one pass of the particle phase, from the
     committed ncu summary of the same kernel on the 8-ppc case of this
@@ -472,7 +606,9 @@ def load_traffic(workload, precision, wl):
             for line in f:
                 if line.startswith("dram_bytes_per_particle:"):
                     per = float(line.split(":")[1])
-                    return per * sum(s.n for s in wl.species)
+                    n_plasma = wl.n_particles - (wl.beam.number_macro * wl.beam.number_bunches
+                                                 if wl.beam is not None else 0)
+                    return per * n_plasma
     except OSError:
         pass
     return None

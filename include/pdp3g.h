@@ -112,6 +112,14 @@ pdp3g_status pdp3g_add_species(pdp3g_ctx *ctx, double charge_e, double mass_me, 
                                const double *r, const double *z, const double *vr,
                                const double *vphi, const double *vz, const double *w,
                                const uint8_t *alive, int32_t *id);
+/* The same with the six FP64 arrays in device memory of the context's
+   device (e.g. generated there), all particles alive; the arrays are read
+   before the call returns.  No upstream counterpart (the upstream fills its
+   host arrays in place). */
+pdp3g_status pdp3g_add_species_device(pdp3g_ctx *ctx, double charge_e, double mass_me,
+                                      int64_t n, const double *r, const double *z,
+                                      const double *vr, const double *vphi, const double *vz,
+                                      const double *w, int32_t *id);
 
 /* Bunch(name, charge, mass, n, geom, duration, radius, density, velocity,
    bunch_number, hole_duration), src/bunch.cpp:6-80 (TESTMODE radial

@@ -72,6 +72,8 @@ EXPORTS = [
     ("pdp3g_destroy", None, [_VP]),
     ("pdp3g_add_species", _I32, [_VP, ctypes.c_double, ctypes.c_double, ctypes.c_int64] +
      [_D] * 6 + [_U8, ctypes.POINTER(_I32)]),
+    ("pdp3g_add_species_device", _I32, [_VP, ctypes.c_double, ctypes.c_double, ctypes.c_int64] +
+     [_VP] * 6 + [ctypes.POINTER(_I32)]),
     ("pdp3g_add_bunch", _I32, [_VP, ctypes.c_double, ctypes.c_double, ctypes.c_int64,
                                ctypes.c_double, ctypes.c_double, ctypes.c_double,
                                ctypes.c_double, _I32, ctypes.c_double, ctypes.POINTER(_I32)]),
@@ -184,6 +186,19 @@ class Simulation:
                                              ctypes.byref(sid)), "add_species")
         return sid.value
 
+    def add_species_device(self, charge_e, mass_me, r, z, vr, vphi, vz, w):
+        """Adds a species from six FP64 device arrays (torch tensors on this
+        simulation's device, contiguous, equal length)."""
+        arrs = [r, z, vr, vphi, vz, w]
+        n = int(arrs[0].numel())
+        for a in arrs:
+            assert a.is_cuda and a.is_contiguous() and a.numel() == n and str(a.dtype) == "torch.float64"
+        sid = _I32()
+        self._check(self.L.pdp3g_add_species_device(self.h, float(charge_e), float(mass_me), n,
+                                                    *[a.data_ptr() for a in arrs],
+                                                    ctypes.byref(sid)), "add_species_device")
+        return sid.value
+
     def add_bunch(self, charge_e, mass_me, n, duration, radius, density, velocity,
                   bunch_number=0, hole_duration=0.0):
         sid = _I32()
@@ -283,13 +298,18 @@ class Simulation:
             pass
 
 
-def from_workload(wl, precision="fp64", device=0, pusher=None, sort_interval=0):
-    """Builds a Simulation holding a pdp3_b200.workloads.Workload."""
+def from_workload(wl, precision="fp64", device=0, pusher=None, sort_interval=None):
+    """Builds a Simulation holding a pdp3_b200.workloads.Workload (sort
+    interval: the workload's unless given)."""
+    if sort_interval is None:
+        sort_interval = getattr(wl, "sort_interval", 0)
     sim = Simulation(wl.r_size, wl.z_size, wl.n_grid_r, wl.n_grid_z, wl.dt, pml=wl.pml,
                      pusher=pusher or wl.pusher, precision=precision, device=device,
                      sort_interval=sort_interval)
     for s in wl.species:
         sim.add_species(s.charge_e, s.mass_me, s.r, s.z, s.vr, s.vphi, s.vz, s.w)
+    if getattr(wl, "device_plasma", None) is not None:
+        wl.device_plasma.add_to(sim, device)
     if wl.beam is not None:
         b = wl.beam
         for nb in range(b.number_bunches):

@@ -12,6 +12,9 @@
 //   4  H update   H' = H + a(E), Hh = H + a(E)/2    (src/hField.cpp:93-157)
 //        lE += a^T(lH' + lHh/2),  lH = lH' + lHh
 // Stencil transposes scatter with FP64 atomics.
+#include <algorithm>
+#include <climits>
+
 #include "adjoint_particle.cuh"
 #include "pdp3g_internal.cuh"
 
@@ -137,10 +140,43 @@ __device__ __forceinline__ void ladd(const GridDev &g, double *f, int i, int k, 
   atomicAdd(f + (size_t)i * g.nz + k, (double)v);
 }
 
-// step 2: particles.  Es = E of step s, Hh = H half-time of step s.
-__global__ void __launch_bounds__(128) k_adj_particles(GridDev g, const double *E3,
-                                                      const double *Hh3, AdjSpeciesDev S,
-                                                      AdjGrids A, int face) {
+constexpr int ADJ_THREADS = 128;
+constexpr int ADJ_TILE = 1024;  // nodes per component in the shared accumulator
+
+struct AdjShared {
+  float acc[6][ADJ_TILE];  // adjoints of E_r, E_phi, E_z, Hh_r, Hh_phi, Hh_z
+  int red[4][ADJ_THREADS / 32];
+  int box[4];
+};
+
+struct AdjTile {
+  float (*acc)[ADJ_TILE];
+  int r0, z0, nrb, nzb;
+  bool on;
+};
+
+// adds v to component comp at node (i, k): the CTA's shared tile when the
+// node is inside it, else the FP64 grid
+__device__ __forceinline__ void tadd(const GridDev &g, const AdjTile &t, double *grid, int comp,
+                                     int i, int k, float v) {
+  if (v == 0.0f) return;
+  const int li = i - t.r0, lk = k - t.z0;
+  if (t.on && (unsigned)li < (unsigned)t.nrb && (unsigned)lk < (unsigned)t.nzb) {
+    atomicAdd(&t.acc[comp][li * t.nzb + lk], v);
+    return;
+  }
+  ladd(g, grid, i, k, v);
+}
+
+// step 2: particles.  E3 = E of step s, Hh3 = H half-time of step s (three
+// consecutive grids each).  One CTA takes chunks of ADJ_THREADS consecutive
+// particles; the field-node adjoints of a chunk are summed in FP32 in shared
+// memory over the bounding box of its cells (particles sorted by cell keep
+// it small) and added to the FP64 grids once per node.
+__global__ void __launch_bounds__(ADJ_THREADS, 3) k_adj_particles(GridDev g, const double *E3,
+                                                              const double *Hh3, AdjSpeciesDev S,
+                                                              AdjGrids A, int face) {
+  __shared__ AdjShared sm;
   const int ncz = g.nz - 1;
   const size_t ng = (size_t)g.nr * g.nz;
   adj::Consts<float> C;
@@ -155,72 +191,140 @@ __global__ void __launch_bounds__(128) k_adj_particles(GridDev g, const double *
   C.nz = g.nz;
   C.bunch = S.st.kind == KIND_BUNCH;
   C.face = face;
-  for (long long p = blockIdx.x * (long long)blockDim.x + threadIdx.x; p < S.st.n;
-       p += (long long)gridDim.x * blockDim.x) {
-    if (S.st.alive != nullptr && !S.st.alive[p]) continue;
-    adj::Tape<float> tp;
-    const int c = S.st.cell[p];
-    if (c < 0 || c >= (g.nr - 1) * ncz) continue;  // flagged by the forward step
-    tp.i = c / ncz;
-    tp.k = c - tp.i * ncz;
-    tp.a = S.st.fr[p];
-    tp.b = S.st.fz[p];
-    tp.u[0] = S.st.ur[p];
-    tp.u[1] = S.st.uphi[p];
-    tp.u[2] = S.st.uz[p];
-    tp.w = S.st.w[p];
-    adj::gather_weights(tp);
-    const double *fE[3] = {E3, E3 + ng, E3 + 2 * ng}, *fH[3] = {Hh3, Hh3 + ng, Hh3 + 2 * ng};
-    int ri[2][3], zi[2][3];
-    for (int fld = 0; fld < 2; fld++)
+  for (int idx = threadIdx.x; idx < 6 * ADJ_TILE; idx += ADJ_THREADS) (&sm.acc[0][0])[idx] = 0.0f;
+  __syncthreads();
+  const long long nchunks = (S.st.n + ADJ_THREADS - 1) / ADJ_THREADS;
+  for (long long chunk = blockIdx.x; chunk < nchunks; chunk += gridDim.x) {
+    const long long p = chunk * ADJ_THREADS + threadIdx.x;
+    bool live = p < S.st.n && (S.st.alive == nullptr || S.st.alive[p]);
+    const int c = live ? S.st.cell[p] : 0;
+    if (c < 0 || c >= (g.nr - 1) * ncz) live = false;  // flagged by the forward step
+    const int ci = c / ncz, ck = c - (c / ncz) * ncz;
+    // bounding box of the chunk's cells
+    int v4[4] = {live ? ci : INT_MAX, live ? -ci : INT_MAX, live ? ck : INT_MAX,
+                 live ? -ck : INT_MAX};
+#pragma unroll
+    for (int j = 0; j < 4; j++)
+#pragma unroll
+      for (int o = 16; o > 0; o >>= 1) v4[j] = min(v4[j], __shfl_xor_sync(0xffffffffu, v4[j], o));
+    if ((threadIdx.x & 31) == 0)
+#pragma unroll
+      for (int j = 0; j < 4; j++) sm.red[j][threadIdx.x >> 5] = v4[j];
+    __syncthreads();
+    if (threadIdx.x < 4) {
+      int m = INT_MAX;
+      for (int w = 0; w < ADJ_THREADS / 32; w++) m = min(m, sm.red[threadIdx.x][w]);
+      sm.box[threadIdx.x] = m;
+    }
+    __syncthreads();
+    AdjTile t;
+    t.acc = sm.acc;
+    t.r0 = sm.box[0] - 1;
+    t.z0 = sm.box[2] - 1;
+    t.nrb = -sm.box[1] - sm.box[0] + 4;
+    t.nzb = -sm.box[3] - sm.box[2] + 4;
+    t.on = sm.box[0] != INT_MAX && t.nrb * t.nzb <= ADJ_TILE;
+    if (live) {
+      adj::Tape<float> tp;
+      tp.i = ci;
+      tp.k = ck;
+      tp.a = S.st.fr[p];
+      tp.b = S.st.fz[p];
+      tp.u[0] = S.st.ur[p];
+      tp.u[1] = S.st.uphi[p];
+      tp.u[2] = S.st.uz[p];
+      tp.w = S.st.w[p];
+      adj::gather_weights(tp);
+      // node rows/columns of the two weightings (clamped as the forward gather)
+      const int ir_h = min(tp.ir_h, g.nr - 2), ir_n = min(tp.i, g.nr - 2);
+      const int kz_h = min(tp.kz_h, g.nz - 2), kz_n = min(tp.k, g.nz - 2);
+#pragma unroll
       for (int cc = 0; cc < 3; cc++) {
-        int ir = adj::comp_rhalf(fld, cc) ? tp.ir_h : tp.i;
-        int kz = adj::comp_zhalf(fld, cc) ? tp.kz_h : tp.k;
-        ir = min(ir, g.nr - 2);
-        kz = min(kz, g.nz - 2);
-        ri[fld][cc] = ir;
-        zi[fld][cc] = kz;
-        const double *f = fld == 0 ? fE[cc] : fH[cc];
-        float *dst = fld == 0 ? tp.fe[cc] : tp.fh[cc];
-        dst[0] = node_val(g, f, ir, kz);
-        dst[1] = node_val(g, f, ir + 1, kz);
-        dst[2] = node_val(g, f, ir, kz + 1);
-        dst[3] = node_val(g, f, ir + 1, kz + 1);
+        {
+          const int ir = adj::comp_rhalf(0, cc) ? ir_h : ir_n;
+          const int kz = adj::comp_zhalf(0, cc) ? kz_h : kz_n;
+          const double *f = E3 + cc * ng;
+          tp.fe[cc][0] = node_val(g, f, ir, kz);
+          tp.fe[cc][1] = node_val(g, f, ir + 1, kz);
+          tp.fe[cc][2] = node_val(g, f, ir, kz + 1);
+          tp.fe[cc][3] = node_val(g, f, ir + 1, kz + 1);
+        }
+        {
+          const int ir = adj::comp_rhalf(1, cc) ? ir_h : ir_n;
+          const int kz = adj::comp_zhalf(1, cc) ? kz_h : kz_n;
+          const double *f = Hh3 + cc * ng;
+          tp.fh[cc][0] = node_val(g, f, ir, kz);
+          tp.fh[cc][1] = node_val(g, f, ir + 1, kz);
+          tp.fh[cc][2] = node_val(g, f, ir, kz + 1);
+          tp.fh[cc][3] = node_val(g, f, ir + 1, kz + 1);
+        }
       }
-    adj::forward(C, tp);
-    float l_jphi[4] = {lget(g, A.lJphi, tp.i1, tp.k1), lget(g, A.lJphi, tp.i1 + 1, tp.k1),
-                       lget(g, A.lJphi, tp.i1, tp.k1 + 1), lget(g, A.lJphi, tp.i1 + 1, tp.k1 + 1)};
-    float l_piece[3][4] = {{0, 0, 0, 0}, {0, 0, 0, 0}, {0, 0, 0, 0}};
-    if (tp.path_ok)
-      for (int q = 0; q <= tp.np; q++) {
-        const int ci = tp.pc_i[q], ck = tp.pc_k[q];
-        l_piece[q][0] = lget(g, A.lJz, ci, ck);
-        l_piece[q][1] = lget(g, A.lJz, ci + 1, ck);
-        l_piece[q][2] = lget(g, A.lJr, ci, ck);
-        l_piece[q][3] = lget(g, A.lJr, ci, ck + 1);
+      adj::forward(C, tp);
+      float l_jphi[4] = {lget(g, A.lJphi, tp.i1, tp.k1), lget(g, A.lJphi, tp.i1 + 1, tp.k1),
+                         lget(g, A.lJphi, tp.i1, tp.k1 + 1),
+                         lget(g, A.lJphi, tp.i1 + 1, tp.k1 + 1)};
+      float l_piece[3][4] = {{0, 0, 0, 0}, {0, 0, 0, 0}, {0, 0, 0, 0}};
+      if (tp.path_ok) {
+#pragma unroll
+        for (int q = 0; q < 3; q++) {
+          if (q > tp.np) continue;
+          const int qi = tp.pci(q), qk = tp.pck(q);
+          l_piece[q][0] = lget(g, A.lJz, qi, qk);
+          l_piece[q][1] = lget(g, A.lJz, qi + 1, qk);
+          l_piece[q][2] = lget(g, A.lJr, qi, qk);
+          l_piece[q][3] = lget(g, A.lJr, qi, qk + 1);
+        }
       }
-    const float l_uout[3] = {S.lur[p], S.luphi[p], S.luz[p]};
-    float l_a, l_b, l_u[3], l_w, l_fe[3][4], l_fh[3][4];
-    adj::reverse(C, tp, S.la[p], S.lb[p], l_uout, l_jphi, l_piece, l_a, l_b, l_u, l_w, l_fe,
-                 l_fh);
-    S.la[p] = l_a;
-    S.lb[p] = l_b;
-    S.lur[p] = l_u[0];
-    S.luphi[p] = l_u[1];
-    S.luz[p] = l_u[2];
-    S.lw[p] += (double)l_w;
-    double *lEs[3] = {A.lEr, A.lEphi, A.lEz}, *lHs[3] = {A.lHhr, A.lHhphi, A.lHhz};
-    for (int cc = 0; cc < 3; cc++) {
-      for (int fld = 0; fld < 2; fld++) {
-        const int ir = ri[fld][cc], kz = zi[fld][cc];
-        double *dst = fld == 0 ? lEs[cc] : lHs[cc];
-        const float *lv = fld == 0 ? l_fe[cc] : l_fh[cc];
-        ladd(g, dst, ir, kz, lv[0]);
-        ladd(g, dst, ir + 1, kz, lv[1]);
-        ladd(g, dst, ir, kz + 1, lv[2]);
-        ladd(g, dst, ir + 1, kz + 1, lv[3]);
+      const float l_uout[3] = {S.lur[p], S.luphi[p], S.luz[p]};
+      float l_a, l_b, l_u[3], l_w, l_fe[3][4], l_fh[3][4];
+      adj::reverse(C, tp, S.la[p], S.lb[p], l_uout, l_jphi, l_piece, l_a, l_b, l_u, l_w, l_fe,
+                   l_fh);
+      S.la[p] = l_a;
+      S.lb[p] = l_b;
+      S.lur[p] = l_u[0];
+      S.luphi[p] = l_u[1];
+      S.luz[p] = l_u[2];
+      S.lw[p] += (double)l_w;
+#pragma unroll
+      for (int cc = 0; cc < 3; cc++) {
+        {
+          const int ir = adj::comp_rhalf(0, cc) ? ir_h : ir_n;
+          const int kz = adj::comp_zhalf(0, cc) ? kz_h : kz_n;
+          double *grid = cc == 0 ? A.lEr : (cc == 1 ? A.lEphi : A.lEz);
+          tadd(g, t, grid, cc, ir, kz, l_fe[cc][0]);
+          tadd(g, t, grid, cc, ir + 1, kz, l_fe[cc][1]);
+          tadd(g, t, grid, cc, ir, kz + 1, l_fe[cc][2]);
+          tadd(g, t, grid, cc, ir + 1, kz + 1, l_fe[cc][3]);
+        }
+        {
+          const int ir = adj::comp_rhalf(1, cc) ? ir_h : ir_n;
+          const int kz = adj::comp_zhalf(1, cc) ? kz_h : kz_n;
+          double *grid = cc == 0 ? A.lHhr : (cc == 1 ? A.lHhphi : A.lHhz);
+          tadd(g, t, grid, 3 + cc, ir, kz, l_fh[cc][0]);
+          tadd(g, t, grid, 3 + cc, ir + 1, kz, l_fh[cc][1]);
+          tadd(g, t, grid, 3 + cc, ir, kz + 1, l_fh[cc][2]);
+          tadd(g, t, grid, 3 + cc, ir + 1, kz + 1, l_fh[cc][3]);
+        }
       }
     }
+    __syncthreads();
+    if (t.on) {
+      const int nb = t.nrb * t.nzb;
+      for (int idx = threadIdx.x; idx < nb; idx += ADJ_THREADS) {
+        const int li = idx / t.nzb, lk = idx - li * t.nzb;
+#pragma unroll
+        for (int comp = 0; comp < 6; comp++) {
+          const float v = sm.acc[comp][idx];
+          if (v != 0.0f) {
+            sm.acc[comp][idx] = 0.0f;
+            double *grid = comp == 0 ? A.lEr : comp == 1 ? A.lEphi : comp == 2 ? A.lEz
+                         : comp == 3 ? A.lHhr : comp == 4 ? A.lHhphi : A.lHhz;
+            ladd(g, grid, t.r0 + li, t.z0 + lk, v);
+          }
+        }
+      }
+    }
+    __syncthreads();
   }
 }
 
@@ -292,7 +396,17 @@ void adj_launch_h(const GridDev &g, const AdjGrids &A, cudaStream_t st) {
 void adj_launch_particles(const GridDev &g, const double *E3, const double *Hh3,
                           const AdjSpeciesDev &S, const AdjGrids &A, int face, cudaStream_t st) {
   if (S.st.n <= 0) return;
-  k_adj_particles<<<blocks_for(S.st.n, 128), 128, 0, st>>>(g, E3, Hh3, S, A, face);
+  const long long nchunks = (S.st.n + ADJ_THREADS - 1) / ADJ_THREADS;
+  int bpsm = 0;
+  if (cudaOccupancyMaxActiveBlocksPerMultiprocessor(&bpsm, k_adj_particles, ADJ_THREADS, 0) !=
+          cudaSuccess || bpsm < 1)
+    bpsm = 1;
+  int dev = 0, nsm = 148;
+  cudaGetDevice(&dev);
+  cudaDeviceGetAttribute(&nsm, cudaDevAttrMultiProcessorCount, dev);
+  const long long blocks = std::min<long long>(nchunks, (long long)bpsm * nsm);
+  k_adj_particles<<<(int)std::max<long long>(blocks, 1), ADJ_THREADS, 0, st>>>(g, E3, Hh3, S, A,
+                                                                               face);
 }
 
 void adj_launch_inject(const AdjSpeciesDev &S, long long start, long long count, double dt,

@@ -55,14 +55,31 @@ struct Tape {
   bool alive_now;
   int in, kn;
   T an, bn, st, ct, uout[3];
-  // r-z path: points Q[0..np+1] relative to the start cell, pieces p in cells
-  int np, kindp[2], pc_i[3], pc_k[3];
-  T ts[2], qa[4], qb[4];
+  // r-z path: points Q0..Q(np+1) relative to the start cell (qa, qb),
+  // piece p in cell (pci_p, pck_p), crossing p at parameter ts_p through an
+  // r face (kind 0) or a z face (kind 1).  Scalars, not arrays, so that the
+  // compiler keeps the whole tape in registers.
+  int np, kind0, kind1, pci0, pci1, pci2, pck0, pck1, pck2;
+  T ts0, ts1, qa0, qa1, qa2, qa3, qb0, qb1, qb2, qb3;
   bool path_ok;
+  PDP3_HD T qa(int p) const { return p == 0 ? qa0 : (p == 1 ? qa1 : (p == 2 ? qa2 : qa3)); }
+  PDP3_HD T qb(int p) const { return p == 0 ? qb0 : (p == 1 ? qb1 : (p == 2 ? qb2 : qb3)); }
+  PDP3_HD int pci(int p) const { return p == 0 ? pci0 : (p == 1 ? pci1 : pci2); }
+  PDP3_HD int pck(int p) const { return p == 0 ? pck0 : (p == 1 ? pck1 : pck2); }
+  PDP3_HD T ts(int p) const { return p == 0 ? ts0 : ts1; }
+  PDP3_HD int kind(int p) const { return p == 0 ? kind0 : kind1; }
 };
 
 template <typename T>
 PDP3_HD T tmin(T x, T y) { return x < y ? x : y; }
+
+// element p of a 3- or 4-entry tape array by selects (no run-time indexing)
+template <typename T>
+PDP3_HD T sel3(int p, T a0, T a1, T a2) { return p == 0 ? a0 : (p == 1 ? a1 : a2); }
+template <typename T>
+PDP3_HD T sel4(int p, T a0, T a1, T a2, T a3) {
+  return p == 0 ? a0 : (p == 1 ? a1 : (p == 2 ? a2 : a3));
+}
 
 // ---------------------------------------------------------------- pieces
 
@@ -234,10 +251,11 @@ PDP3_HD int comp_zhalf(int field, int c) {
 }
 
 template <typename T>
-PDP3_HD T interp(const Tape<T> &tp, const T f[4], bool rh, bool zh) {
-  const T *wr = rh ? tp.wrh : tp.wrn;
-  const T *wz = zh ? tp.wzh : tp.wzn;
-  return wz[0] * (f[0] * wr[0] + f[1] * wr[1]) + wz[1] * (f[2] * wr[0] + f[3] * wr[1]);
+PDP3_HD T interp(const Tape<T> &tp, T f0, T f1, T f2, T f3, bool rh, bool zh) {
+  // value selects (no pointer into the tape), so the tape can stay in registers
+  const T wr0 = rh ? tp.wrh[0] : tp.wrn[0], wr1 = rh ? tp.wrh[1] : tp.wrn[1];
+  const T wz0 = zh ? tp.wzh[0] : tp.wzn[0], wz1 = zh ? tp.wzh[1] : tp.wzn[1];
+  return wz0 * (f0 * wr0 + f1 * wr1) + wz1 * (f2 * wr0 + f3 * wr1);
 }
 
 // ----------------------------------------------------------------- forward
@@ -255,13 +273,18 @@ PDP3_HD void renorm_t(int &i, T &f) {
 template <typename T>
 PDP3_HD void forward(const Consts<T> &C, Tape<T> &tp) {
   gather_weights(tp);
+#pragma unroll
   for (int c = 0; c < 3; c++) {
-    tp.e[c] = interp(tp, tp.fe[c], comp_rhalf(0, c), comp_zhalf(0, c));
-    tp.h[c] = interp(tp, tp.fh[c], comp_rhalf(1, c), comp_zhalf(1, c));
+    tp.e[c] = interp(tp, tp.fe[c][0], tp.fe[c][1], tp.fe[c][2], tp.fe[c][3], comp_rhalf(0, c),
+                     comp_zhalf(0, c));
+    tp.h[c] = interp(tp, tp.fh[c][0], tp.fh[c][1], tp.fh[c][2], tp.fh[c][3], comp_rhalf(1, c),
+                     comp_zhalf(1, c));
   }
   // Boris, relativistic
+#pragma unroll
   for (int c = 0; c < 3; c++) tp.um[c] = tp.u[c] + C.ke * tp.e[c];
   tp.gi = T(1) / sqrt(T(1) + tp.um[0] * tp.um[0] + tp.um[1] * tp.um[1] + tp.um[2] * tp.um[2]);
+#pragma unroll
   for (int c = 0; c < 3; c++) tp.tb[c] = C.kb * tp.h[c] * tp.gi;
   tp.c2 = T(2) / (T(1) + tp.tb[0] * tp.tb[0] + tp.tb[1] * tp.tb[1] + tp.tb[2] * tp.tb[2]);
   tp.wv[0] = tp.um[0] + (tp.um[1] * tp.tb[2] - tp.um[2] * tp.tb[1]);
@@ -270,8 +293,10 @@ PDP3_HD void forward(const Consts<T> &C, Tape<T> &tp) {
   tp.v2[0] = tp.wv[1] * tp.tb[2] - tp.wv[2] * tp.tb[1];
   tp.v2[1] = tp.wv[2] * tp.tb[0] - tp.wv[0] * tp.tb[2];
   tp.v2[2] = tp.wv[0] * tp.tb[1] - tp.wv[1] * tp.tb[0];
+#pragma unroll
   for (int c = 0; c < 3; c++) tp.up[c] = tp.um[c] + tp.c2 * tp.v2[c] + C.ke * tp.e[c];
   tp.inv_g = T(1) / sqrt(T(1) + tp.up[0] * tp.up[0] + tp.up[1] * tp.up[1] + tp.up[2] * tp.up[2]);
+#pragma unroll
   for (int c = 0; c < 3; c++) tp.vel[c] = tp.up[c] * tp.inv_g;
   // first half move, rz rotation
   tp.dr_h = tp.vel[0] * C.cr;
@@ -349,43 +374,44 @@ PDP3_HD void forward(const Consts<T> &C, Tape<T> &tp) {
   T tr = 2, tz = 2;
   if (di != 0) tr = ((di > 0 ? T(1) : T(0)) - tp.a) / (A - tp.a);
   if (dk != 0) tz = ((dk > 0 ? T(1) : T(0)) - tp.b) / (B - tp.b);
+  tp.ts0 = tp.ts1 = T(2);
+  tp.kind0 = tp.kind1 = 0;
   if (tr <= T(1) && tz <= T(1)) {
-    if (tr <= tz) { tp.ts[0] = tr; tp.kindp[0] = 0; tp.ts[1] = tz; tp.kindp[1] = 1; }
-    else { tp.ts[0] = tz; tp.kindp[0] = 1; tp.ts[1] = tr; tp.kindp[1] = 0; }
+    if (tr <= tz) { tp.ts0 = tr; tp.kind0 = 0; tp.ts1 = tz; tp.kind1 = 1; }
+    else { tp.ts0 = tz; tp.kind0 = 1; tp.ts1 = tr; tp.kind1 = 0; }
     tp.np = 2;
   } else if (tr <= T(1)) {
-    tp.ts[0] = tr; tp.kindp[0] = 0; tp.np = 1;
+    tp.ts0 = tr; tp.kind0 = 0; tp.np = 1;
   } else if (tz <= T(1)) {
-    tp.ts[0] = tz; tp.kindp[0] = 1; tp.np = 1;
+    tp.ts0 = tz; tp.kind0 = 1; tp.np = 1;
   }
-  tp.qa[0] = tp.a;
-  tp.qb[0] = tp.b;
-  int ci = tp.i, ck = tp.k;
-  for (int p = 0; p < tp.np; p++) {
-    if (tp.kindp[p] == 0) {
-      tp.qa[p + 1] = di > 0 ? T(1) : T(0);
-      tp.qb[p + 1] = tp.b + tp.ts[p] * (B - tp.b);
-    } else {
-      tp.qa[p + 1] = tp.a + tp.ts[p] * (A - tp.a);
-      tp.qb[p + 1] = dk > 0 ? T(1) : T(0);
-    }
-  }
-  tp.qa[tp.np + 1] = A;
-  tp.qb[tp.np + 1] = B;
-  for (int p = 0; p <= tp.np; p++) {
-    tp.pc_i[p] = ci;
-    tp.pc_k[p] = ck;
-    if (p < tp.np) {
-      if (tp.kindp[p] == 0) ci += di; else ck += dk;
-    }
-  }
+  // crossing point p: the crossed coordinate sits on the face
+  const T fa = di > 0 ? T(1) : T(0), fb = dk > 0 ? T(1) : T(0);
+  const T ca0 = tp.kind0 == 0 ? fa : tp.a + tp.ts0 * (A - tp.a);
+  const T cb0 = tp.kind0 == 0 ? tp.b + tp.ts0 * (B - tp.b) : fb;
+  const T ca1 = tp.kind1 == 0 ? fa : tp.a + tp.ts1 * (A - tp.a);
+  const T cb1 = tp.kind1 == 0 ? tp.b + tp.ts1 * (B - tp.b) : fb;
+  tp.qa0 = tp.a;
+  tp.qb0 = tp.b;
+  tp.qa1 = tp.np >= 1 ? ca0 : A;
+  tp.qb1 = tp.np >= 1 ? cb0 : B;
+  tp.qa2 = tp.np >= 2 ? ca1 : A;
+  tp.qb2 = tp.np >= 2 ? cb1 : B;
+  tp.qa3 = A;
+  tp.qb3 = B;
+  tp.pci0 = tp.i;
+  tp.pck0 = tp.k;
+  tp.pci1 = tp.pci0 + (tp.np >= 1 && tp.kind0 == 0 ? di : 0);
+  tp.pck1 = tp.pck0 + (tp.np >= 1 && tp.kind0 == 1 ? dk : 0);
+  tp.pci2 = tp.pci1 + (tp.np >= 2 && tp.kind1 == 0 ? di : 0);
+  tp.pck2 = tp.pck1 + (tp.np >= 2 && tp.kind1 == 1 ? dk : 0);
 }
 
 // Deposit values of the particle's pieces (for checks): jz/jr per piece
 template <typename T>
 PDP3_HD void piece_outputs(const Consts<T> &C, const Tape<T> &tp, int p, T out[4]) {
-  const T oi = T(tp.pc_i[p] - tp.i), ok = T(tp.pc_k[p] - tp.k);
-  piece_fwd(tp.pc_i[p], tp.qa[p] - oi, tp.qb[p] - ok, tp.qa[p + 1] - oi, tp.qb[p + 1] - ok,
+  const T oi = T(tp.pci(p) - tp.i), ok = T(tp.pck(p) - tp.k);
+  piece_fwd(tp.pci(p), tp.qa(p) - oi, tp.qb(p) - ok, tp.qa(p + 1) - oi, tp.qb(p + 1) - ok,
             C.kz * tp.w, C.kr * tp.w, out);
 }
 
@@ -404,9 +430,9 @@ PDP3_HD void piece_outputs(const Consts<T> &C, const Tape<T> &tp, int p, T out[4
 //     f_i (2i + 1) / (2 (i + 1)(i + 2)).
 // f_j is the node row's value interpolated in z with the particle's weights.
 template <typename T>
-PDP3_HD T radial_jump(const Tape<T> &tp, const T f[4], const T wz[2], bool rh) {
+PDP3_HD T radial_jump(const Tape<T> &tp, T f0, T f1, T f2, T f3, T wz0, T wz1, bool rh) {
   const int i = tp.i;
-  const T lo = wz[0] * f[0] + wz[1] * f[2], hi = wz[0] * f[1] + wz[1] * f[3];
+  const T lo = wz0 * f0 + wz1 * f2, hi = wz0 * f1 + wz1 * f3;
   if (!rh) {
     // nodes i, i+1: top face jump uses f_{i+1}, bottom face (i >= 1) f_i
     const T top = hi / T(i + 2);
@@ -416,6 +442,25 @@ PDP3_HD T radial_jump(const Tape<T> &tp, const T f[4], const T wz[2], bool rh) {
   if (i < 1) return T(0);
   const T fi = tp.ir_h == i ? lo : hi;  // node i is the inner node when ir = i
   return fi * T(2 * i + 1) / (T(2) * T(i + 1) * T(i + 2));
+}
+
+// adjoint of one gathered component: lv = adjoint of the gathered value;
+// writes the adjoints of its four node values and adds the position terms
+template <typename T>
+PDP3_HD void gather_rev(const Consts<T> &C, const Tape<T> &tp, const T f[4], bool rh, bool zh,
+                        T lv, T lf[4], T &l_a, T &l_b) {
+  const T wr0 = rh ? tp.wrh[0] : tp.wrn[0], wr1 = rh ? tp.wrh[1] : tp.wrn[1];
+  const T dwr0 = rh ? tp.dwrh[0] : tp.dwrn[0], dwr1 = rh ? tp.dwrh[1] : tp.dwrn[1];
+  const T wz0 = zh ? tp.wzh[0] : tp.wzn[0], wz1 = zh ? tp.wzh[1] : tp.wzn[1];
+  const T f0 = f[0], f1 = f[1], f2 = f[2], f3 = f[3];
+  lf[0] = lv * wz0 * wr0;
+  lf[1] = lv * wz0 * wr1;
+  lf[2] = lv * wz1 * wr0;
+  lf[3] = lv * wz1 * wr1;
+  l_a += lv * (wz0 * (f0 * dwr0 + f1 * dwr1) + wz1 * (f2 * dwr0 + f3 * dwr1));
+  // d wz0 / db = -1, d wz1 / db = +1 for both the node and the half-node weights
+  l_b += lv * (-(f0 * wr0 + f1 * wr1) + (f2 * wr0 + f3 * wr1));
+  if (C.face) l_a += lv * radial_jump(tp, f0, f1, f2, f3, wz0, wz1, rh);
 }
 
 // ----------------------------------------------------------------- reverse
@@ -449,28 +494,44 @@ PDP3_HD void reverse(const Consts<T> &C, const Tape<T> &tp, T l_an, T l_bn, cons
     l_dy += l_st / tp.r2;
     // ---- r-z path adjoint
     if (tp.path_ok) {
-      T l_qa[4] = {0, 0, 0, 0}, l_qb[4] = {0, 0, 0, 0};
+      // adjoints of the path points Q0..Q3, kept in scalars: the piece loop is
+      // not unrolled (one copy of piece_rev) and reads the tape through
+      // selects, so nothing is indexed at run time
+      T lqa0 = 0, lqa1 = 0, lqa2 = 0, lqa3 = 0, lqb0 = 0, lqb1 = 0, lqb2 = 0, lqb3 = 0;
+#pragma unroll 1
       for (int p = 0; p <= tp.np; p++) {
-        const T oi = T(tp.pc_i[p] - tp.i), ok = T(tp.pc_k[p] - tp.k);
+        const int pci = tp.pci(p), pck = tp.pck(p);
+        const T oi = T(pci - tp.i), ok = T(pck - tp.k);
+        const T qa0 = tp.qa(p), qb0 = tp.qb(p), qa1 = tp.qa(p + 1), qb1 = tp.qb(p + 1);
+        const T lo[4] = {sel3(p, l_piece[0][0], l_piece[1][0], l_piece[2][0]),
+                         sel3(p, l_piece[0][1], l_piece[1][1], l_piece[2][1]),
+                         sel3(p, l_piece[0][2], l_piece[1][2], l_piece[2][2]),
+                         sel3(p, l_piece[0][3], l_piece[1][3], l_piece[2][3])};
         T la0 = 0, lc0 = 0, la1 = 0, lc1 = 0, lkz = 0, lkr = 0;
-        piece_rev(tp.pc_i[p], tp.qa[p] - oi, tp.qb[p] - ok, tp.qa[p + 1] - oi, tp.qb[p + 1] - ok,
-                  C.kz * tp.w, C.kr * tp.w, l_piece[p], la0, lc0, la1, lc1, lkz, lkr);
-        l_qa[p] += la0;
-        l_qb[p] += lc0;
-        l_qa[p + 1] += la1;
-        l_qb[p + 1] += lc1;
+        piece_rev(pci, qa0 - oi, qb0 - ok, qa1 - oi, qb1 - ok, C.kz * tp.w, C.kr * tp.w, lo,
+                  la0, lc0, la1, lc1, lkz, lkr);
+        // Q_p gets (la0, lc0), Q_{p+1} gets (la1, lc1)
+        lqa0 += p == 0 ? la0 : T(0);
+        lqa1 += p == 1 ? la0 : (p == 0 ? la1 : T(0));
+        lqa2 += p == 2 ? la0 : (p == 1 ? la1 : T(0));
+        lqa3 += p == 2 ? la1 : T(0);
+        lqb0 += p == 0 ? lc0 : T(0);
+        lqb1 += p == 1 ? lc0 : (p == 0 ? lc1 : T(0));
+        lqb2 += p == 2 ? lc0 : (p == 1 ? lc1 : T(0));
+        lqb3 += p == 2 ? lc1 : T(0);
         l_w += lkz * C.kz + lkr * C.kr;
       }
       // crossing points depend on P0 = (a, b) and P1 = (A, B)
       const int di = tp.in - tp.i, dk = tp.kn - tp.k;
       const T Ar = T(di) + tp.an, Br = T(dk) + tp.bn;  // = A, B relative to the start cell
+#pragma unroll 1
       for (int p = 1; p <= tp.np; p++) {
-        const T t = tp.ts[p - 1];
-        if (tp.kindp[p - 1] == 0) {
+        const T t = tp.ts(p - 1);
+        if (tp.kind(p - 1) == 0) {
           // qb = b + t (B - b), t = (fr - a)/(A - a)
           const T fr = di > 0 ? T(1) : T(0), den = Ar - tp.a;
           const T dt_da = (-(den) + (fr - tp.a)) / (den * den), dt_dA = -(fr - tp.a) / (den * den);
-          const T l = l_qb[p];
+          const T l = p == 1 ? lqb1 : lqb2;
           l_b += l * (1 - t);
           l_B += l * t;
           l_a += l * (Br - tp.b) * dt_da;
@@ -478,17 +539,17 @@ PDP3_HD void reverse(const Consts<T> &C, const Tape<T> &tp, T l_an, T l_bn, cons
         } else {
           const T fz = dk > 0 ? T(1) : T(0), den = Br - tp.b;
           const T dt_db = (-(den) + (fz - tp.b)) / (den * den), dt_dB = -(fz - tp.b) / (den * den);
-          const T l = l_qa[p];
+          const T l = p == 1 ? lqa1 : lqa2;
           l_a += l * (1 - t);
           l_A += l * t;
           l_b += l * (Ar - tp.a) * dt_db;
           l_B += l * (Ar - tp.a) * dt_dB;
         }
       }
-      l_a += l_qa[0];
-      l_b += l_qb[0];
-      l_A += l_qa[tp.np + 1];
-      l_B += l_qb[tp.np + 1];
+      l_a += lqa0;
+      l_b += lqb0;
+      l_A += tp.np == 0 ? lqa1 : (tp.np == 1 ? lqa2 : lqa3);
+      l_B += tp.np == 0 ? lqb1 : (tp.np == 1 ? lqb2 : lqb3);
     }
   } else {
     l_up[0] += tp.ur_sign * l_uout[0];
@@ -582,24 +643,10 @@ PDP3_HD void reverse(const Consts<T> &C, const Tape<T> &tp, T l_an, T l_bn, cons
     l_e[c] += C.ke * l_um[c];
   }
   // ---- gather reverse: field-node adjoints and position dependence
-  for (int fld = 0; fld < 2; fld++) {
-    for (int c = 0; c < 3; c++) {
-      const bool rh = comp_rhalf(fld, c), zh = comp_zhalf(fld, c);
-      const T *wr = rh ? tp.wrh : tp.wrn;
-      const T *dwr = rh ? tp.dwrh : tp.dwrn;
-      const T *wz = zh ? tp.wzh : tp.wzn;
-      const T dwz0 = -1, dwz1 = 1;
-      const T *f = fld == 0 ? tp.fe[c] : tp.fh[c];
-      const T lv = fld == 0 ? l_e[c] : l_h[c];
-      T *lf = fld == 0 ? l_fe[c] : l_fh[c];
-      lf[0] = lv * wz[0] * wr[0];
-      lf[1] = lv * wz[0] * wr[1];
-      lf[2] = lv * wz[1] * wr[0];
-      lf[3] = lv * wz[1] * wr[1];
-      l_a += lv * (wz[0] * (f[0] * dwr[0] + f[1] * dwr[1]) + wz[1] * (f[2] * dwr[0] + f[3] * dwr[1]));
-      l_b += lv * (dwz0 * (f[0] * wr[0] + f[1] * wr[1]) + dwz1 * (f[2] * wr[0] + f[3] * wr[1]));
-      if (C.face) l_a += lv * radial_jump(tp, f, wz, rh);
-    }
+#pragma unroll
+  for (int c = 0; c < 3; c++) {
+    gather_rev(C, tp, tp.fe[c], comp_rhalf(0, c), comp_zhalf(0, c), l_e[c], l_fe[c], l_a, l_b);
+    gather_rev(C, tp, tp.fh[c], comp_rhalf(1, c), comp_zhalf(1, c), l_h[c], l_fh[c], l_a, l_b);
   }
 }
 

@@ -29,7 +29,7 @@ struct Species {
 };
 
 struct StepEvents {
-  cudaEvent_t ev[6];
+  cudaEvent_t ev[7];
 };
 
 }  // namespace
@@ -163,14 +163,16 @@ pdp3g_status harvest_timing(pdp3g_ctx *ctx) {
   if (ctx->events_used == 0) return PDP3G_OK;
   CK(cudaStreamSynchronize(ctx->stream));
   for (size_t s = 0; s < ctx->events_used; s++) {
-    float ms[5];
-    for (int j = 0; j < 5; j++)
+    float ms[6];
+    for (int j = 0; j < 6; j++)
       CK(cudaEventElapsedTime(&ms[j], ctx->step_events[s].ev[j], ctx->step_events[s].ev[j + 1]));
-    // ev0..1 injection, 1..2 H update, 2..3 J clear, 3..4 particles, 4..5 E update
+    // ev0..1 injection, 1..2 H update, 2..3 J clear, 3..4 re-sort, 4..5 particles,
+    // 5..6 E update
     ctx->acc.ms_other += ms[0] + ms[2];
-    ctx->acc.ms_fields += ms[1] + ms[4];
-    ctx->acc.ms_particles += ms[3];
-    ctx->acc.ms_step_total += ms[0] + ms[1] + ms[2] + ms[3] + ms[4];
+    ctx->acc.ms_fields += ms[1] + ms[5];
+    ctx->acc.ms_sort += ms[3];
+    ctx->acc.ms_particles += ms[4];
+    ctx->acc.ms_step_total += ms[0] + ms[1] + ms[2] + ms[3] + ms[4] + ms[5];
   }
   ctx->events_used = 0;
   return PDP3G_OK;
@@ -443,6 +445,66 @@ pdp3g_status pdp3g_add_species(pdp3g_ctx *ctx, double charge_e, double mass_me, 
   return PDP3G_OK;
 }
 
+pdp3g_status pdp3g_add_species_device(pdp3g_ctx *ctx, double charge_e, double mass_me,
+                                      int64_t n, const double *r, const double *z,
+                                      const double *vr, const double *vphi, const double *vz,
+                                      const double *w, int32_t *id) {
+  if (!ctx || n <= 0 || !r || !z || !vr || !vphi || !vz || !w)
+    return fail(ctx, PDP3G_INVALID_ARG, "add_species_device: null array");
+  if (n > (int64_t)1 << 40) return fail(ctx, PDP3G_INVALID_ARG, "add_species_device: n too large");
+  CK(cudaSetDevice(ctx->device));
+  const double *src[6] = {r, z, vr, vphi, vz, w};
+  for (const double *p : src) {
+    cudaPointerAttributes at{};
+    if (cudaPointerGetAttributes(&at, p) != cudaSuccess || at.type != cudaMemoryTypeDevice ||
+        at.device != ctx->device) {
+      cudaGetLastError();
+      return fail(ctx, PDP3G_INVALID_ARG,
+                  "add_species_device: arrays must be device memory of the context's device");
+    }
+  }
+  Species sp;
+  sp.charge_si = charge_e * EL_CHARGE;  // src/particles.cpp:30-32
+  sp.mass_si = mass_me * EL_MASS;
+  cudaStream_t st = ctx->stream;
+  const size_t b = sizeof(double) * (size_t)n;
+  if (ctx->cfg.precision == PDP3G_FP32_CELL) {
+    sp.fp32 = true;
+    SpeciesF32 &f = sp.f32;
+    f.n = n;
+    f.kind = KIND_PLASMA;
+    f32_constants(ctx, sp);
+    CK(dalloc(ctx, &f.cell, (size_t)n));
+    CK(dalloc(ctx, &f.fr, (size_t)n));
+    CK(dalloc(ctx, &f.fz, (size_t)n));
+    CK(dalloc(ctx, &f.ur, (size_t)n));
+    CK(dalloc(ctx, &f.uphi, (size_t)n));
+    CK(dalloc(ctx, &f.uz, (size_t)n));
+    float *wf = nullptr;
+    CK(dalloc(ctx, &wf, (size_t)n));
+    f.w = wf;
+    pdp3g_status rs = stage_reserve(ctx, (size_t)n);
+    if (rs != PDP3G_OK) return rs;
+    for (int j = 0; j < 6; j++)
+      CK(cudaMemcpyAsync(ctx->d_stage + (size_t)j * n, src[j], b, cudaMemcpyDeviceToDevice, st));
+    pdp3g_status cs = convert_staged_f32(ctx, sp, true);
+    if (cs != PDP3G_OK) return cs;
+  } else {
+    sp.dev.charge = sp.charge_si;
+    sp.dev.mass = sp.mass_si;
+    sp.dev.kind = KIND_PLASMA;
+    pdp3g_status as = alloc_species(ctx, sp, n, false);
+    if (as != PDP3G_OK) return as;
+    double *dst[6] = {sp.dev.r, sp.dev.z, sp.dev.vr, sp.dev.vphi, sp.dev.vz, (double *)sp.dev.w};
+    for (int j = 0; j < 6; j++)
+      CK(cudaMemcpyAsync(dst[j], src[j], b, cudaMemcpyDeviceToDevice, st));
+    CK(cudaStreamSynchronize(st));
+  }
+  ctx->species.push_back(sp);
+  if (id) *id = (int32_t)ctx->species.size() - 1;
+  return PDP3G_OK;
+}
+
 pdp3g_status pdp3g_add_bunch(pdp3g_ctx *ctx, double charge_e, double mass_me, int64_t n,
                              double duration, double radius, double density, double velocity,
                              int32_t bunch_number, double hole_duration, int32_t *id) {
@@ -628,15 +690,16 @@ pdp3g_status pdp3g_step(pdp3g_ctx *ctx, int32_t nsteps) {
     phase_calc_h(ctx);
     if (ev) cudaEventRecord(ev->ev[2], st);
     CK(phase_reset_j(ctx));
+    if (ev) cudaEventRecord(ev->ev[3], st);
     if (ctx->cfg.sort_interval > 0 && ctx->steps % ctx->cfg.sort_interval == 0) {
       pdp3g_status ss = sort_all(ctx);
       if (ss != PDP3G_OK) return ss;
     }
-    if (ev) cudaEventRecord(ev->ev[3], st);
-    phase_particles(ctx);
     if (ev) cudaEventRecord(ev->ev[4], st);
-    phase_calc_e(ctx);
+    phase_particles(ctx);
     if (ev) cudaEventRecord(ev->ev[5], st);
+    phase_calc_e(ctx);
+    if (ev) cudaEventRecord(ev->ev[6], st);
     phase_advance(ctx);
     if (ctx->timing && ctx->events_used >= 4096) {
       pdp3g_status hs = harvest_timing(ctx);

@@ -73,6 +73,10 @@ class Workload:
     pusher: str = "boris"
     species: List[SpeciesInit] = field(default_factory=list)
     beam: Optional[BeamInit] = None
+    sort_interval: int = 0
+    # plasma generated on the GPU instead of `species` (cases too large for
+    # host arrays): a DevicePlasma
+    device_plasma: Optional["DevicePlasma"] = None
 
     @property
     def dr(self):
@@ -85,6 +89,8 @@ class Workload:
     @property
     def n_particles(self):
         n = sum(s.n for s in self.species)
+        if self.device_plasma is not None:
+            n += 2 * self.device_plasma.n
         if self.beam is not None:
             n += self.beam.number_macro * self.beam.number_bunches
         return n
@@ -295,6 +301,30 @@ def adjoint_config(theta, seed=1004, n_grid_r=129, n_grid_z=1025, r_size=0.1, z_
     return wl, aux
 
 
+class AdjointFamily:
+    """adjoint_config for many theta at one seed: the theta-independent
+    arrays (positions, velocities, cell volumes) are built once and each
+    workload() only rescales the plasma weights and replaces the bunch."""
+
+    def __init__(self, theta0, **kw):
+        self.kw = kw
+        self.wl0, self.aux0 = adjoint_config(theta0, **kw)
+        c0 = np.asarray(theta0, dtype=np.float64)[:N_BUMPS]
+        self.n0_col = bump_basis(self.aux0["zc"], self.wl0.z_size) @ c0
+
+    def workload(self, theta):
+        import dataclasses
+        theta = np.asarray(theta, dtype=np.float64)
+        n_col = bump_basis(self.aux0["zc"], self.wl0.z_size) @ theta[:N_BUMPS]
+        scale = (n_col / self.n0_col)[self.aux0["kc"]]
+        species = [dataclasses.replace(s, w=s.w * scale) for s in self.wl0.species]
+        beam = dataclasses.replace(self.wl0.beam, radius=float(theta[N_BUMPS + 1]),
+                                   velocity=gamma_velocity(float(theta[N_BUMPS])))
+        wl = dataclasses.replace(self.wl0, species=species, beam=beam)
+        aux = dict(self.aux0, theta=theta.copy())
+        return wl, aux
+
+
 def bunch_init_np(n, radius, duration, velocity, density, dr, dz):
     """Radii and weights of Bunch::Bunch (src/bunch.cpp:6-80, TESTMODE
     radial sequence) and their derivatives with respect to the radius."""
@@ -356,3 +386,103 @@ def probe_loss(ez, dr, dz, probe):
 # [0.094, 0.144] m, which holds the bunch's tail and the start of its wake
 # after the 500-step window (the head is then 173 cells from the entrance)
 ADJOINT_PROBE = (0, 16, 120, 184)
+
+
+# ------------------------------------------------------- device-side plasma
+
+
+@dataclass
+class DevicePlasma:
+    """Electrons and protons generated on the GPU with torch (seeded CUDA
+    generator), with the same conventions as thermal_plasma: `ppc` particles
+    per domain cell, r with pdf ~ r and z uniform inside the cell, weight
+    n(z_cell) * (cell volume) / ppc, ions on the electron positions, 1 eV
+    Maxwellian electrons, cold ions.  The density is n_max * min(z / z_ramp, 1)
+    (z_ramp = 0: uniform n_max)."""
+    seed: int
+    r_size: float
+    z_size: float
+    n_grid_r: int
+    n_grid_z: int
+    ppc: int
+    n_max: float
+    z_ramp: float = 0.0
+    t_ev: float = 1.0
+    ion_mass_me: float = 1836.0
+
+    @property
+    def n(self):
+        return (self.n_grid_r - 1) * (self.n_grid_z - 1) * self.ppc
+
+    def add_to(self, sim, device):
+        """Generates the two species on `device` and adds them to sim."""
+        import torch
+        dev = torch.device("cuda", device)
+        gen = torch.Generator(device=dev)
+        gen.manual_seed(self.seed)
+        nr, nz, ppc = self.n_grid_r, self.n_grid_z, self.ppc
+        dr = self.r_size / (nr - 1)
+        dz = self.z_size / (nz - 1)
+        nrc, nzc = nr - 1, nz - 1
+        n = nrc * nzc * ppc
+        idx = torch.arange(n, device=dev, dtype=torch.int64)
+        ic = idx // (nzc * ppc)
+        kc = (idx // ppc) % nzc
+        del idx
+        # cell edges of the particle domain [dr/2, R - dr/2] x [dz/2, Z - dz/2]
+        lo_r = torch.where(ic == 0, torch.full_like(ic, 0, dtype=torch.float64) + dr / 2,
+                           ic.to(torch.float64) * dr)
+        hi_r = torch.where(ic == nrc - 1, torch.full_like(lo_r, self.r_size - dr / 2),
+                           (ic + 1).to(torch.float64) * dr)
+        del ic
+        u = torch.rand(n, generator=gen, device=dev, dtype=torch.float64)
+        r = torch.sqrt(lo_r * lo_r + u * (hi_r * hi_r - lo_r * lo_r))
+        vol = math.pi * (hi_r * hi_r - lo_r * lo_r)
+        del lo_r, hi_r
+        lo_z = torch.where(kc == 0, torch.full_like(u, dz / 2), kc.to(torch.float64) * dz)
+        hi_z = torch.where(kc == nzc - 1, torch.full_like(u, self.z_size - dz / 2),
+                           (kc + 1).to(torch.float64) * dz)
+        del kc
+        torch.rand(n, generator=gen, device=dev, dtype=torch.float64, out=u)
+        z = lo_z + u * (hi_z - lo_z)
+        vol *= hi_z - lo_z
+        zc = 0.5 * (lo_z + hi_z)
+        del lo_z, hi_z
+        if self.z_ramp > 0:
+            dens = self.n_max * torch.clamp(zc / self.z_ramp, max=1.0)
+        else:
+            dens = torch.full_like(zc, self.n_max)
+        w = dens * vol / ppc
+        del dens, vol, zc
+        sig = math.sqrt(self.t_ev * EL_CHARGE / EL_MASS)
+        v = [torch.randn(n, generator=gen, device=dev, dtype=torch.float64) * sig
+             for _ in range(3)]
+        sim.add_species_device(-1.0, 1.0, r, z, v[0], v[1], v[2], w)
+        del v
+        zero = torch.zeros(n, device=dev, dtype=torch.float64)
+        sim.add_species_device(1.0, self.ion_mass_me, r, z, zero, zero, zero, w)
+        del r, z, w, zero, u
+        torch.cuda.synchronize(dev)
+        torch.cuda.empty_cache()
+
+
+def large_config(seed=1003, n_grid_r=513, n_grid_z=4097, r_size=0.1, z_size=0.8, ppc=64,
+                 density=1e17, ramp_fraction=0.2, steps=2000, beam_gamma=10.0,
+                 beam_radius=5e-3, beam_length=0.02, beam_density=5e16, pusher="vay",
+                 sort_interval=20):
+    """Large FP32 case: 512x4096 cells, electrons and protons at 64 ppc
+    (268,435,456 particles, generated on the GPU), density ramped linearly
+    from 0 to 1e17 m^-3 over the first 20% of z, gamma = 10 electron bunch
+    (r 5 mm, length 2 cm, 5e16 m^-3) with the Vay pusher, particles re-sorted
+    by cell every 20 steps."""
+    dr = r_size / (n_grid_r - 1)
+    dz = z_size / (n_grid_z - 1)
+    plasma = DevicePlasma(seed, r_size, z_size, n_grid_r, n_grid_z, ppc, density,
+                          ramp_fraction * z_size)
+    bunch_cells = (beam_radius / dr) * (beam_length / dz)
+    beam = BeamInit(-1.0, 1.0, int(round(64 * bunch_cells)), beam_length, beam_radius,
+                    beam_density, gamma_velocity(beam_gamma), 1, 0.0, "reverse", seed)
+    return Workload("large_%dx%d_ppc%d" % (n_grid_r - 1, n_grid_z - 1, ppc), r_size, z_size,
+                    n_grid_r, n_grid_z, courant_dt(dr, dz), steps,
+                    absorbing_layer(n_grid_r, n_grid_z, 10), pusher, [], beam, sort_interval,
+                    plasma)

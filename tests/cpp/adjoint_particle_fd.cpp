@@ -66,7 +66,7 @@ static T objective(const Consts<T> &C, const In &in, const LamOut &L, Tape<T> *k
 static bool same_branch(const Tape<T> &x, const Tape<T> &y) {
   return x.in == y.in && x.kn == y.kn && x.i1 == y.i1 && x.k1 == y.k1 && x.np == y.np &&
          x.ir_h == y.ir_h && x.kz_h == y.kz_h && x.sr == y.sr && x.sz == y.sz &&
-         x.alive_now == y.alive_now && (x.np == 0 || x.kindp[0] == y.kindp[0]);
+         x.alive_now == y.alive_now && (x.np == 0 || x.kind0 == y.kind0);
 }
 
 static int pathwise() {
@@ -161,7 +161,7 @@ static T gather_at(T x, const T *F0, const T *F1, T b, bool rh, bool zh, T *dG, 
   const T *wr = rh ? tp.wrh : tp.wrn, *dwr = rh ? tp.dwrh : tp.dwrn;
   const T *wz = zh ? tp.wzh : tp.wzn;
   if (dG) *dG = wz[0] * (f[0] * dwr[0] + f[1] * dwr[1]) + wz[1] * (f[2] * dwr[0] + f[3] * dwr[1]);
-  if (jump) *jump = radial_jump(tp, f, wz, rh);
+  if (jump) *jump = radial_jump(tp, f[0], f[1], f[2], f[3], wz[0], wz[1], rh);
   return wz[0] * (f[0] * wr[0] + f[1] * wr[1]) + wz[1] * (f[2] * wr[0] + f[3] * wr[1]);
 }
 

@@ -1,0 +1,130 @@
+"""The adjoint window (pdp3g_forward_window / pdp3g_backward_window) on B200.
+
+* Fields only (no particles): the window is linear in the initial E and H and
+  the loss quadratic, so the adjoint of every initial field component must
+  equal central differences to rounding (1e-9 of the largest entry).
+* Small differentiable window (32x256 cells, 8 ppc per species, gamma=5
+  bunch, 100 steps, checkpoints every 20): the gradient with respect to the
+  density coefficients, the bunch gamma and the bunch radius against FP64
+  central differences (a cubic fitted to the loss at eight steps of up to
+  1% of each parameter); pathwise mode, whose derivative is the one such
+  small steps measure at this size.
+* Forward + backward leaves the state the forward ended in, and the adjoint
+  rejects what it does not support.
+"""
+import numpy as np
+import pytest
+
+from pdp3_b200 import api
+from pdp3_b200 import workloads as W
+
+pytestmark = pytest.mark.gpu
+
+SMALL = dict(n_grid_r=33, n_grid_z=257, r_size=0.025, z_size=0.2, ppc=8)
+PROBE = (0, 8, 10, 42)
+
+
+def test_field_adjoint_is_exact():
+    wl = W.small_config(beam=False)
+    sim = api.Simulation(wl.r_size, wl.z_size, wl.n_grid_r, wl.n_grid_z, wl.dt, pml=wl.pml,
+                         precision="fp32")
+    rng = np.random.default_rng(3)
+    comps = ("E_r", "E_phi", "E_z", "H_r", "H_phi", "H_z")
+    init = {c: rng.normal(0, 1e3 if c[0] == "E" else 1.0, (wl.n_grid_r, wl.n_grid_z))
+            for c in comps}
+
+    def load(pert=None):
+        for c, a in init.items():
+            b = a.copy()
+            if pert is not None and pert[0] == c:
+                b[pert[1], pert[2]] += pert[3]
+            sim.set_field(c, b)
+
+    probe = (0, 4, 10, 20)
+    load()
+    adj = api.Adjoint(sim, 30, 7, probe)
+    adj.forward()
+    adj.backward()
+    grads = {c: adj.field(c) for c in comps}
+    adj.close()
+    for c in ("E_r", "E_phi", "E_z", "H_phi"):
+        scale = np.abs(grads[c]).max()
+        assert scale > 0, c
+        h = 1.0 if c[0] == "E" else 1e-3
+        for (i, k) in [(1, 12), (2, 15), (0, 14), (3, 11), (5, 20)]:
+            vals = []
+            for sgn in (1, -1):
+                load((c, i, k, sgn * h))
+                a2 = api.Adjoint(sim, 30, 7, probe)
+                vals.append(a2.forward())
+                a2.close()
+            fd = (vals[0] - vals[1]) / (2 * h)
+            assert abs(fd - grads[c][i, k]) <= 1e-9 * scale, (c, i, k, fd, grads[c][i, k])
+    sim.close()
+
+
+def fitted_slope(fam, th, j, steps, hmax=0.01, npts=4):
+    xs = np.concatenate([-np.arange(npts, 0, -1), np.arange(1, npts + 1)]) * (hmax / npts)
+    ls = []
+    for x in xs:
+        t = th.copy()
+        t[j] = th[j] * (1 + x)
+        wl, _ = fam.workload(t)
+        sim = api.from_workload(wl, precision="fp64")
+        sim.step(steps)
+        sim.sync()
+        ls.append(W.probe_loss(sim.field("E_z"), wl.dr, wl.dz, PROBE))
+        sim.close()
+    X = np.vstack([np.ones_like(xs), xs, xs ** 2, xs ** 3]).T
+    coef = np.linalg.lstsq(X, np.array(ls), rcond=None)[0]
+    return coef[1] / th[j]
+
+
+def test_gradient_matches_fp64_finite_differences():
+    th = W.adjoint_theta()
+    fam = W.AdjointFamily(th, **SMALL)
+    wl, aux = fam.workload(th)
+    sim = api.from_workload(wl, precision="fp32")
+    adj = api.Adjoint(sim, 100, 20, PROBE)
+    adj.set_mode("pathwise")
+    adj.forward()
+    adj.backward()
+    g = W.adjoint_gradient(wl, aux, [adj.species(0), adj.species(1)], adj.species(2),
+                           adj.bunch_velocity(2))
+    t = adj.timing()
+    assert t["backward_ms"] <= 4.0 * t["forward_ms"], t
+    adj.close()
+    sim.close()
+    dens = [0, 1, 2]
+    fd = {j: fitted_slope(fam, th, j, 100) for j in dens + [16]}
+    gd, fdd = np.array([g[j] for j in dens]), np.array([fd[j] for j in dens])
+    assert np.linalg.norm(gd - fdd) <= 1e-3 * np.linalg.norm(fdd), (gd, fdd)
+    assert abs(g[16] - fd[16]) <= 1e-3 * abs(fd[16]), (g[16], fd[16])
+
+
+def test_backward_restores_forward_end_state_and_rejects_misuse():
+    th = W.adjoint_theta()
+    wl, _ = W.AdjointFamily(th, **SMALL).workload(th)
+    sim = api.from_workload(wl, precision="fp32")
+    adj = api.Adjoint(sim, 40, 15, PROBE)
+    with pytest.raises(api.Pdp3gError):
+        adj.backward()  # nothing to reverse yet
+    adj.forward()
+    after = {c: sim.field(c) for c in ("E_z", "H_phi")}
+    sp = sim.species(0)
+    t_end = sim.time
+    adj.backward()
+    for c, a in after.items():
+        assert np.array_equal(sim.field(c), a), c
+    sp2 = sim.species(0)
+    for k in ("r", "z", "vr", "vz"):
+        assert np.array_equal(sp2[k], sp[k]), k
+    assert sim.time == t_end
+    with pytest.raises(api.Pdp3gError):
+        api.Adjoint(sim, 10, 5, (0, 8, 10, 10_000))  # probe outside the grid
+    adj.close()
+    sim.close()
+    s64 = api.from_workload(wl, precision="fp64")
+    with pytest.raises(api.Pdp3gError):
+        api.Adjoint(s64, 10, 5, PROBE)  # the FP64 form has no adjoint
+    s64.close()
