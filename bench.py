@@ -251,6 +251,11 @@ def main():
                     help="the form reported as value (the other is measured beside it)")
     ap.add_argument("--workload", default="wake",
                     choices=["wake", "thermal", "large", "ensemble", "adjoint"])
+    ap.add_argument("--adjoint-scale", type=int, default=1,
+                    help="--workload adjoint: divide the grid's cells in r and z by this "
+                         "(1: the 128x1024 case)")
+    ap.add_argument("--adjoint-steps", type=int, default=500)
+    ap.add_argument("--adjoint-interval", type=int, default=50)
     ap.add_argument("--adjoint-fd-params", default="near",
                     help="parameters checked by finite differences in --workload adjoint: "
                          "'near' (the 4 density bumps nearest the probe, gamma, radius), "
@@ -525,14 +530,27 @@ def run_adjoint(args, rank, world, local_rank):
     from pdp3_b200 import api
     from pdp3_b200 import workloads as W
     torch.cuda.set_device(local_rank)
-    steps, interval, probe = 500, 50, W.ADJOINT_PROBE
+    steps, interval = args.adjoint_steps, args.adjoint_interval
+    sc = max(1, args.adjoint_scale)
+    kw = {}
+    probe = W.ADJOINT_PROBE
+    if sc > 1:
+        kw = dict(n_grid_r=128 // sc + 1, n_grid_z=1024 // sc + 1, r_size=0.1 / sc,
+                  z_size=0.8 / sc)
+        probe = (0, max(2, 16 // sc), 120 // sc, 184 // sc)
     theta = W.adjoint_theta()
-    fam = W.AdjointFamily(theta)
+    fam = W.AdjointFamily(theta, **kw)
     wl, aux = fam.workload(theta)
+    # warm-up: one window on a separate context (a second forward on the
+    # same context would start from the first window's end state)
     sim = api.from_workload(wl, precision="fp32", device=local_rank)
     adj = api.Adjoint(sim, steps, interval, probe)
-    adj.forward()        # warm-up pair (500 + 1000 steps)
+    adj.forward()
     adj.backward()
+    adj.close()
+    sim.close()
+    sim = api.from_workload(wl, precision="fp32", device=local_rank)
+    adj = api.Adjoint(sim, steps, interval, probe)
     clocks = ClockSampler(local_rank)
     clocks.start()
     time.sleep(0.3)
@@ -541,13 +559,13 @@ def run_adjoint(args, rank, world, local_rank):
     clk = clocks.stop()
     t = adj.timing()
 
-    def grad():
+    def grad(mean_field):
         return W.adjoint_gradient(wl, aux, [adj.species(0), adj.species(1)], adj.species(2),
-                                  adj.bunch_velocity(2))
-    g_mf = grad()
+                                  adj.bunch_velocity(2), mean_field=mean_field)
+    g_mf = grad(True)
     adj.set_mode("pathwise")
     adj.backward()
-    g_pw = grad()
+    g_pw = grad(False)
     n_alive_end = sum(sim.species_size(s) for s in (0, 1)) + int(sim.species(2)["alive"].sum())
     adj_bytes = adj.device_bytes()
     adj.close()

@@ -239,6 +239,10 @@ pdp3g_status pdp3g_ensemble_run(pdp3g_ensemble *e, int32_t nsteps);
 pdp3g_status pdp3g_ensemble_autotune(pdp3g_ensemble *e, int32_t steps_per_trial,
                                      int32_t *blocks_per_sm);
 pdp3g_status pdp3g_ensemble_set_budget(pdp3g_ensemble *e, double max_ms);  /* 0: none */
+/* re-sort every run's plasma species by cell every `steps` steps (between
+   persistent launches); default: the smallest positive sort_interval of the
+   runs' configs; 0: never */
+pdp3g_status pdp3g_ensemble_set_sort_interval(pdp3g_ensemble *e, int32_t steps);
 pdp3g_status pdp3g_ensemble_cancel(pdp3g_ensemble *e, int32_t cancel);     /* any thread */
 pdp3g_status pdp3g_ensemble_info(pdp3g_ensemble *e, pdp3g_ensemble_stats *out);
 const char *pdp3g_ensemble_last_error(pdp3g_ensemble *e);
@@ -250,9 +254,11 @@ void pdp3g_ensemble_destroy(pdp3g_ensemble *e);
    Loss: sum over the probe nodes i in [probe_r0, probe_r1), k in
    [probe_z0, probe_z1) of E_z(i, k)^2 V_i after the window, with V_i the
    node's ring volume 2 pi i dr^2 dz (pi dr^2 dz / 4 on the axis).
-   pdp3g_forward_window steps the context window_steps steps (no re-sorting,
-   so every particle keeps its slot), storing E, H and the particle state
-   every checkpoint_interval steps and at the end, and returns the loss.
+   pdp3g_forward_window steps the context window_steps steps from its
+   current state (no re-sorting, so every particle keeps its slot), storing
+   E, H and the particle state every checkpoint_interval steps and at the
+   end, and returns the loss; a second call starts a new window from where
+   the first ended and replaces its checkpoints.
    pdp3g_backward_window recomputes each interval from its checkpoint
    (storing every step's particle-phase input) and runs the hand-written
    reverse of each step, last to first; it leaves the context in the state

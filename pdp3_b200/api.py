@@ -108,6 +108,7 @@ EXPORTS = [
     ("pdp3g_ensemble_run", _I32, [_VP, _I32]),
     ("pdp3g_ensemble_autotune", _I32, [_VP, _I32, ctypes.POINTER(_I32)]),
     ("pdp3g_ensemble_set_budget", _I32, [_VP, ctypes.c_double]),
+    ("pdp3g_ensemble_set_sort_interval", _I32, [_VP, _I32]),
     ("pdp3g_ensemble_cancel", _I32, [_VP, _I32]),
     ("pdp3g_ensemble_info", _I32, [_VP, ctypes.POINTER(EnsembleInfo)]),
     ("pdp3g_ensemble_last_error", ctypes.c_char_p, [_VP]),
@@ -351,6 +352,10 @@ class Ensemble:
 
     def set_budget(self, max_ms):
         self._check(self.L.pdp3g_ensemble_set_budget(self.h, float(max_ms)), "set_budget")
+
+    def set_sort_interval(self, steps):
+        self._check(self.L.pdp3g_ensemble_set_sort_interval(self.h, int(steps)),
+                    "set_sort_interval")
 
     def cancel(self, on=True):
         self._check(self.L.pdp3g_ensemble_cancel(self.h, 1 if on else 0), "cancel")

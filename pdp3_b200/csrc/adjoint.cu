@@ -3,7 +3,7 @@
 // Reverse of one step s, given the adjoints of the state after it
 // (lE, lH: FP64 grids; la, lb, lu: FP32 per particle):
 //   1  E update   E' = ke E - kh (J + curl H')   (src/eField.cpp:85-170)
-//        lJ = -kh lE',  lH' += curl^T(-kh lE'),  then lE = ke lE'
+//        lJ = -kh lE',  lH' += curl^T(-kh lE'),  lE = ke lE'
 //   2  particles  (adjoint_particle.cuh reverse on each particle's tape,
 //        recomputed from the stored post-injection state of step s)
 //        la/lb/lu updated in place, lw += ..., lE += gather^T, lHh += gather^T
@@ -23,8 +23,10 @@ namespace pdp3g {
 #define AIDX(i, k) ((size_t)(i) * (size_t)nz + (size_t)(k))
 
 
-// step 1a: lJ and the curl^T part into lH (reads lE)
-__global__ void k_adj_e1(GridDev g, AdjGrids A) {
+// step 1: E update transposed, node (i, k) of the E update's range:
+// lJ = -kh lE', lH += curl^T(-kh lE'), lE = ke lE' (the scatter goes to lH
+// only, so each thread can scale its own lE in place)
+__global__ void k_adj_e(GridDev g, AdjGrids A) {
   const int nr = g.nr, nz = g.nz;
   const double dr = g.dr, dz = g.dz, dt = g.dt;
   const long long total = (long long)(nr - 1) * (nz - 1);
@@ -34,87 +36,63 @@ __global__ void k_adj_e1(GridDev g, AdjGrids A) {
     const double epsx2 = 2 * 1.0 * EPSILON0;
     const double sigma_t = g.sigma[AIDX(i, k)] * dt;
     const double kh = 2 * dt / (epsx2 + sigma_t);
+    const double ke = (epsx2 - sigma_t) / (epsx2 + sigma_t);
     if (k >= 1) {  // E_r
       const double gr = -kh * A.lEr[AIDX(i, k)];
-      A.lJr[AIDX(i, k)] = gr;
+      A.lJr[AIDX(i, k)] = (float)gr;
       atomicAdd(&A.lHphi[AIDX(i, k)], gr / dz);
       atomicAdd(&A.lHphi[AIDX(i, k - 1)], -gr / dz);
+      A.lEr[AIDX(i, k)] *= ke;
     }
-    if (i == 0) {  // E_z on axis
-      const double gz = -kh * A.lEz[AIDX(i, k)];
-      A.lJz[AIDX(i, k)] = gz;
+    const double gz = -kh * A.lEz[AIDX(i, k)];
+    A.lJz[AIDX(i, k)] = (float)gz;
+    A.lEz[AIDX(i, k)] *= ke;
+    if (i == 0) {  // on-axis E_z: 4/dr H_phi
       atomicAdd(&A.lHphi[AIDX(i, k)], -4.0 * gz / dr);
     } else {
-      const double gz = -kh * A.lEz[AIDX(i, k)];
-      A.lJz[AIDX(i, k)] = gz;
       atomicAdd(&A.lHphi[AIDX(i, k)], gz * (-1.0 / dr - 1.0 / (2.0 * dr * i)));
       atomicAdd(&A.lHphi[AIDX(i - 1, k)], gz * (1.0 / dr - 1.0 / (2.0 * dr * i)));
       if (k >= 1) {  // E_phi
         const double gp = -kh * A.lEphi[AIDX(i, k)];
-        A.lJphi[AIDX(i, k)] = gp;
+        A.lJphi[AIDX(i, k)] = (float)gp;
         atomicAdd(&A.lHr[AIDX(i, k)], -gp / dz);
         atomicAdd(&A.lHr[AIDX(i, k - 1)], gp / dz);
         atomicAdd(&A.lHz[AIDX(i, k)], gp / dr);
         atomicAdd(&A.lHz[AIDX(i - 1, k)], -gp / dr);
+        A.lEphi[AIDX(i, k)] *= ke;
       }
     }
   }
 }
 
-// step 1b: lE = ke lE on the updated nodes
-__global__ void k_adj_e2(GridDev g, AdjGrids A) {
-  const int nr = g.nr, nz = g.nz;
-  const double dt = g.dt;
-  const long long total = (long long)(nr - 1) * (nz - 1);
-  for (long long t = blockIdx.x * (long long)blockDim.x + threadIdx.x; t < total;
-       t += (long long)gridDim.x * blockDim.x) {
-    const int i = (int)(t / (nz - 1)), k = (int)(t - (long long)i * (nz - 1));
-    const double epsx2 = 2 * 1.0 * EPSILON0;
-    const double sigma_t = g.sigma[AIDX(i, k)] * dt;
-    const double ke = (epsx2 - sigma_t) / (epsx2 + sigma_t);
-    if (k >= 1) A.lEr[AIDX(i, k)] *= ke;
-    A.lEz[AIDX(i, k)] *= ke;
-    if (i >= 1 && k >= 1) A.lEphi[AIDX(i, k)] *= ke;
-  }
-}
-
-// step 4a: lE += a^T (lH + lHh/2)
-__global__ void k_adj_h1(GridDev g, AdjGrids A) {
+// step 4: H update transposed, every node: where the H update ran,
+// lE += a^T(lH + lHh/2) and lH += lHh; everywhere lHh = 0 (the half-step
+// values the update did not write never change, so their adjoints are
+// dropped).  The scatter goes to lE only.
+__global__ void k_adj_h(GridDev g, AdjGrids A) {
   const int nr = g.nr, nz = g.nz;
   const double dr = g.dr, dz = g.dz, dt = g.dt;
-  const long long total = (long long)nr * (nz - 1);
-  for (long long t = blockIdx.x * (long long)blockDim.x + threadIdx.x; t < total;
-       t += (long long)gridDim.x * blockDim.x) {
-    const int i = (int)(t / (nz - 1)), k = (int)(t - (long long)i * (nz - 1));
-    const double la = A.lHr[AIDX(i, k)] + 0.5 * A.lHhr[AIDX(i, k)];
-    const double ca = dt / (dz * MAGN_CONST);
-    atomicAdd(&A.lEphi[AIDX(i, k + 1)], la * ca);
-    atomicAdd(&A.lEphi[AIDX(i, k)], -la * ca);
-    if (i < nr - 1) {
-      const double lb = A.lHphi[AIDX(i, k)] + 0.5 * A.lHhphi[AIDX(i, k)];
-      atomicAdd(&A.lEz[AIDX(i + 1, k)], lb * dt / (dr * MAGN_CONST));
-      atomicAdd(&A.lEz[AIDX(i, k)], -lb * dt / (dr * MAGN_CONST));
-      atomicAdd(&A.lEr[AIDX(i, k + 1)], -lb * dt / (dz * MAGN_CONST));
-      atomicAdd(&A.lEr[AIDX(i, k)], lb * dt / (dz * MAGN_CONST));
-      // H_z -= c, Hh_z = H_z - c/2
-      const double lc = -(A.lHz[AIDX(i, k)] + 0.5 * A.lHhz[AIDX(i, k)]);
-      const double p = 1.0 / (2.0 * dr * (i + 0.5));
-      atomicAdd(&A.lEphi[AIDX(i + 1, k)], lc * dt * (p + 1.0 / dr) / MAGN_CONST);
-      atomicAdd(&A.lEphi[AIDX(i, k)], lc * dt * (p - 1.0 / dr) / MAGN_CONST);
-    }
-  }
-}
-
-// step 4b: lH += lHh on the updated nodes, lHh = 0
-__global__ void k_adj_h2(GridDev g, AdjGrids A) {
-  const int nr = g.nr, nz = g.nz;
   const long long total = (long long)nr * nz;
   for (long long t = blockIdx.x * (long long)blockDim.x + threadIdx.x; t < total;
        t += (long long)gridDim.x * blockDim.x) {
     const int i = (int)(t / nz), k = (int)(t - (long long)i * nz);
     if (k <= nz - 2) {
+      const double la = A.lHr[t] + 0.5 * A.lHhr[t];
+      const double ca = dt / (dz * MAGN_CONST);
+      atomicAdd(&A.lEphi[AIDX(i, k + 1)], la * ca);
+      atomicAdd(&A.lEphi[AIDX(i, k)], -la * ca);
       A.lHr[t] += A.lHhr[t];
-      if (i <= nr - 2) {
+      if (i < nr - 1) {
+        const double lb = A.lHphi[t] + 0.5 * A.lHhphi[t];
+        atomicAdd(&A.lEz[AIDX(i + 1, k)], lb * dt / (dr * MAGN_CONST));
+        atomicAdd(&A.lEz[AIDX(i, k)], -lb * dt / (dr * MAGN_CONST));
+        atomicAdd(&A.lEr[AIDX(i, k + 1)], -lb * dt / (dz * MAGN_CONST));
+        atomicAdd(&A.lEr[AIDX(i, k)], lb * dt / (dz * MAGN_CONST));
+        // H_z -= c, Hh_z = H_z - c/2
+        const double lc = -(A.lHz[t] + 0.5 * A.lHhz[t]);
+        const double p = 1.0 / (2.0 * dr * (i + 0.5));
+        atomicAdd(&A.lEphi[AIDX(i + 1, k)], lc * dt * (p + 1.0 / dr) / MAGN_CONST);
+        atomicAdd(&A.lEphi[AIDX(i, k)], lc * dt * (p - 1.0 / dr) / MAGN_CONST);
         A.lHphi[t] += A.lHhphi[t];
         A.lHz[t] += A.lHhz[t];
       }
@@ -125,14 +103,22 @@ __global__ void k_adj_h2(GridDev g, AdjGrids A) {
   }
 }
 
-
-__device__ __forceinline__ float node_val(const GridDev &g, const double *f, int i, int k) {
-  return (float)f[(size_t)i * g.nz + k];
+__device__ __forceinline__ float node_val(const GridDev &g, const float *f, int i, int k) {
+  return __ldg(f + (size_t)i * g.nz + k);
 }
 
-__device__ __forceinline__ float lget(const GridDev &g, const double *f, int i, int k) {
+// adjoint of J at (i, k), 0 outside the grid
+__device__ __forceinline__ float lget(const GridDev &g, const float *f, int i, int k) {
   if ((unsigned)i >= (unsigned)g.nr || (unsigned)k >= (unsigned)g.nz) return 0.0f;
-  return (float)f[(size_t)i * g.nz + k];
+  return __ldg(f + (size_t)i * g.nz + k);
+}
+
+__global__ void k_capture_fields(const double *e3, const double *hh3, float *dst, size_t ng) {
+  for (size_t t = blockIdx.x * (size_t)blockDim.x + threadIdx.x; t < 3 * ng;
+       t += (size_t)gridDim.x * blockDim.x) {
+    dst[t] = (float)e3[t];
+    dst[3 * ng + t] = (float)hh3[t];
+  }
 }
 
 __device__ __forceinline__ void ladd(const GridDev &g, double *f, int i, int k, float v) {
@@ -140,7 +126,15 @@ __device__ __forceinline__ void ladd(const GridDev &g, double *f, int i, int k, 
   atomicAdd(f + (size_t)i * g.nz + k, (double)v);
 }
 
-constexpr int ADJ_THREADS = 128;
+#ifndef ADJ_THREADS_PER_CTA
+#define ADJ_THREADS_PER_CTA 128
+#endif
+#ifndef ADJ_MIN_BLOCKS
+#define ADJ_MIN_BLOCKS 6  // CTAs per SM the register budget is sized for
+#endif
+// the particle reverse is latency-bound (gathers and adjoint reads behind
+// long dependency chains): more resident warps beat fewer register spills
+constexpr int ADJ_THREADS = ADJ_THREADS_PER_CTA;
 constexpr int ADJ_TILE = 1024;  // nodes per component in the shared accumulator
 
 struct AdjShared {
@@ -173,9 +167,8 @@ __device__ __forceinline__ void tadd(const GridDev &g, const AdjTile &t, double 
 // particles; the field-node adjoints of a chunk are summed in FP32 in shared
 // memory over the bounding box of its cells (particles sorted by cell keep
 // it small) and added to the FP64 grids once per node.
-__global__ void __launch_bounds__(ADJ_THREADS, 3) k_adj_particles(GridDev g, const double *E3,
-                                                              const double *Hh3, AdjSpeciesDev S,
-                                                              AdjGrids A, int face) {
+__global__ void __launch_bounds__(ADJ_THREADS, ADJ_MIN_BLOCKS) k_adj_particles(
+    GridDev g, const float *E3, const float *Hh3, AdjSpeciesDev S, AdjGrids A, int face) {
   __shared__ AdjShared sm;
   const int ncz = g.nz - 1;
   const size_t ng = (size_t)g.nr * g.nz;
@@ -243,7 +236,7 @@ __global__ void __launch_bounds__(ADJ_THREADS, 3) k_adj_particles(GridDev g, con
         {
           const int ir = adj::comp_rhalf(0, cc) ? ir_h : ir_n;
           const int kz = adj::comp_zhalf(0, cc) ? kz_h : kz_n;
-          const double *f = E3 + cc * ng;
+          const float *f = E3 + cc * ng;
           tp.fe[cc][0] = node_val(g, f, ir, kz);
           tp.fe[cc][1] = node_val(g, f, ir + 1, kz);
           tp.fe[cc][2] = node_val(g, f, ir, kz + 1);
@@ -252,7 +245,7 @@ __global__ void __launch_bounds__(ADJ_THREADS, 3) k_adj_particles(GridDev g, con
         {
           const int ir = adj::comp_rhalf(1, cc) ? ir_h : ir_n;
           const int kz = adj::comp_zhalf(1, cc) ? kz_h : kz_n;
-          const double *f = Hh3 + cc * ng;
+          const float *f = Hh3 + cc * ng;
           tp.fh[cc][0] = node_val(g, f, ir, kz);
           tp.fh[cc][1] = node_val(g, f, ir + 1, kz);
           tp.fh[cc][2] = node_val(g, f, ir, kz + 1);
@@ -383,17 +376,19 @@ static int blocks_for(long long n, int threads) {
 }
 
 void adj_launch_e(const GridDev &g, const AdjGrids &A, cudaStream_t st) {
-  const long long n = (long long)(g.nr - 1) * (g.nz - 1);
-  k_adj_e1<<<blocks_for(n, 256), 256, 0, st>>>(g, A);
-  k_adj_e2<<<blocks_for(n, 256), 256, 0, st>>>(g, A);
+  k_adj_e<<<blocks_for((long long)(g.nr - 1) * (g.nz - 1), 256), 256, 0, st>>>(g, A);
 }
 
 void adj_launch_h(const GridDev &g, const AdjGrids &A, cudaStream_t st) {
-  k_adj_h1<<<blocks_for((long long)g.nr * (g.nz - 1), 256), 256, 0, st>>>(g, A);
-  k_adj_h2<<<blocks_for((long long)g.nr * g.nz, 256), 256, 0, st>>>(g, A);
+  k_adj_h<<<blocks_for((long long)g.nr * g.nz, 256), 256, 0, st>>>(g, A);
 }
 
-void adj_launch_particles(const GridDev &g, const double *E3, const double *Hh3,
+void adj_launch_capture_fields(const double *e3, const double *hh3, float *dst, size_t ng,
+                               cudaStream_t st) {
+  k_capture_fields<<<blocks_for((long long)(3 * ng), 256), 256, 0, st>>>(e3, hh3, dst, ng);
+}
+
+void adj_launch_particles(const GridDev &g, const float *E3, const float *Hh3,
                           const AdjSpeciesDev &S, const AdjGrids &A, int face, cudaStream_t st) {
   if (S.st.n <= 0) return;
   const long long nchunks = (S.st.n + ADJ_THREADS - 1) / ADJ_THREADS;

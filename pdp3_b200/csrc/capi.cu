@@ -1023,6 +1023,7 @@ struct pdp3g_ensemble {
   EnsRun *d_runs = nullptr;
   EnsSpecies *d_species = nullptr;
   int *d_status = nullptr;
+  long long *d_budget = nullptr;
   int *h_cancel = nullptr;  // host-mapped
   int *d_cancel = nullptr;
   EnsembleDev dev{};
@@ -1030,10 +1031,13 @@ struct pdp3g_ensemble {
   int blocks_per_sm = 0;
   int max_blocks_per_sm = 0;
   double budget_ms = 0;
+  long long budget_host = 0;  // cycles, source of the copy to d_budget
   long long clock_khz = 0;
   cudaGraph_t graph = nullptr;
   cudaGraphExec_t exec = nullptr;
-  int graph_steps = -1, graph_blocks = -1;
+  int graph_blocks = -1;
+  int sort_interval = 0;        // re-sort every run by cell every this many steps
+  int64_t steps_total = 0;      // steps advanced by this ensemble (sort schedule)
   bool graph_ok = true;
   bool last_used_graph = false;
   double last_ms = 0;
@@ -1064,6 +1068,7 @@ void pdp3g_ensemble_destroy(pdp3g_ensemble *e) {
   cudaFree(e->d_runs);
   cudaFree(e->d_species);
   cudaFree(e->d_status);
+  cudaFree(e->d_budget);
   if (e->h_cancel) cudaFreeHost(e->h_cancel);
   if (e->stream) cudaStreamDestroy(e->stream);
   delete e;
@@ -1129,6 +1134,7 @@ pdp3g_status pdp3g_ensemble_create(pdp3g_ctx *const *runs, int32_t n_runs, pdp3g
       cudaMalloc(&e->d_species, sizeof(EnsSpecies) * std::max<size_t>(hs.size(), 1)) !=
           cudaSuccess ||
       cudaMalloc(&e->d_status, sizeof(int) * 4) != cudaSuccess ||
+      cudaMalloc(&e->d_budget, sizeof(long long)) != cudaSuccess ||
       cudaHostAlloc(&e->h_cancel, sizeof(int), cudaHostAllocMapped) != cudaSuccess ||
       cudaHostGetDevicePointer((void **)&e->d_cancel, e->h_cancel, 0) != cudaSuccess)
     return bail(PDP3G_CUDA_ERROR, "ensemble allocation");
@@ -1148,7 +1154,12 @@ pdp3g_status pdp3g_ensemble_create(pdp3g_ctx *const *runs, int32_t n_runs, pdp3g
   d.inv_pow11 = runs[0]->d_inv_pow11;
   d.cancel = e->d_cancel;
   d.status = e->d_status;
-  d.budget_cycles = 0;
+  d.budget_cycles = e->d_budget;
+  cudaMemset(e->d_budget, 0, sizeof(long long));
+  for (auto *c : e->runs)
+    if (c->cfg.sort_interval > 0 &&
+        (e->sort_interval == 0 || c->cfg.sort_interval < e->sort_interval))
+      e->sort_interval = c->cfg.sort_interval;
   e->max_blocks_per_sm = ensemble_max_blocks_per_sm();
   if (e->max_blocks_per_sm <= 0) return bail(PDP3G_CUDA_ERROR, "ensemble kernel does not fit");
   e->blocks_per_sm = e->max_blocks_per_sm;
@@ -1156,14 +1167,17 @@ pdp3g_status pdp3g_ensemble_create(pdp3g_ctx *const *runs, int32_t n_runs, pdp3g
   return PDP3G_OK;
 }
 
-static pdp3g_status ens_launch(pdp3g_ensemble *e, int nsteps, bool allow_graph) {
+static pdp3g_status ens_launch(pdp3g_ensemble *e, bool allow_graph) {
   const int blocks = e->n_sm * e->blocks_per_sm;
-  // 0 means no budget; any positive budget is at least one cycle
-  e->dev.budget_cycles =
+  // 0 means no budget; any positive budget is at least one cycle.  Written
+  // to device memory on the launch stream, so a replayed graph reads it.
+  e->budget_host =
       e->budget_ms > 0 ? std::max<long long>(1, (long long)std::ceil(e->budget_ms * e->clock_khz)) : 0;
+  EK(cudaMemcpyAsync(e->d_budget, &e->budget_host, sizeof(long long), cudaMemcpyHostToDevice,
+                     e->stream));
   e->last_used_graph = false;
   if (allow_graph && e->graph_ok) {
-    if (e->exec && (e->graph_steps != nsteps || e->graph_blocks != blocks)) {
+    if (e->exec && e->graph_blocks != blocks) {
       cudaGraphExecDestroy(e->exec);
       cudaGraphDestroy(e->graph);
       e->exec = nullptr;
@@ -1171,7 +1185,7 @@ static pdp3g_status ens_launch(pdp3g_ensemble *e, int nsteps, bool allow_graph) 
     }
     if (!e->exec) {
       cudaError_t c1 = cudaStreamBeginCapture(e->stream, cudaStreamCaptureModeThreadLocal);
-      cudaError_t c2 = c1 == cudaSuccess ? ensemble_launch(e->dev, nsteps, blocks, e->stream) : c1;
+      cudaError_t c2 = c1 == cudaSuccess ? ensemble_launch(e->dev, blocks, e->stream) : c1;
       cudaGraph_t g = nullptr;
       cudaError_t c3 = c1 == cudaSuccess ? cudaStreamEndCapture(e->stream, &g) : c1;
       // the captured node must keep the cooperative attribute: the kernel's
@@ -1195,7 +1209,6 @@ static pdp3g_status ens_launch(pdp3g_ensemble *e, int nsteps, bool allow_graph) 
                            : cudaErrorUnknown;
       if (c4 == cudaSuccess) {
         e->graph = g;
-        e->graph_steps = nsteps;
         e->graph_blocks = blocks;
       } else {
         if (g) cudaGraphDestroy(g);
@@ -1210,24 +1223,23 @@ static pdp3g_status ens_launch(pdp3g_ensemble *e, int nsteps, bool allow_graph) 
       return PDP3G_OK;
     }
   }
-  EK(ensemble_launch(e->dev, nsteps, blocks, e->stream));
+  EK(ensemble_launch(e->dev, blocks, e->stream));
   return PDP3G_OK;
 }
 
-static pdp3g_status ens_run(pdp3g_ensemble *e, int nsteps, bool allow_graph, float *ms_out) {
-  EK(cudaSetDevice(e->device));
-  for (size_t r = 0; r < e->runs.size(); r++) {
-    EK(cudaStreamSynchronize(e->runs[r]->stream));
-    e->h_runs[r].t = e->runs[r]->t;
-  }
+// one persistent launch of nsteps steps; *done receives the steps done
+static pdp3g_status ens_segment(pdp3g_ensemble *e, int nsteps, bool allow_graph, float *ms_out,
+                                int *done, int *stop) {
+  for (size_t r = 0; r < e->runs.size(); r++) e->h_runs[r].t = e->runs[r]->t;
   EK(cudaMemcpyAsync(e->d_runs, e->h_runs.data(), sizeof(EnsRun) * e->h_runs.size(),
                      cudaMemcpyHostToDevice, e->stream));
-  EK(cudaMemsetAsync(e->d_status, 0, sizeof(int) * 4, e->stream));
+  const int init[4] = {0, 0, nsteps, 0};
+  EK(cudaMemcpyAsync(e->d_status, init, sizeof(init), cudaMemcpyHostToDevice, e->stream));
   cudaEvent_t a, b;
   cudaEventCreate(&a);
   cudaEventCreate(&b);
   cudaEventRecord(a, e->stream);
-  pdp3g_status st = ens_launch(e, nsteps, allow_graph);
+  pdp3g_status st = ens_launch(e, allow_graph);
   cudaEventRecord(b, e->stream);
   cudaError_t sync = cudaStreamSynchronize(e->stream);
   float ms = 0;
@@ -1238,16 +1250,81 @@ static pdp3g_status ens_run(pdp3g_ensemble *e, int nsteps, bool allow_graph, flo
   if (sync != cudaSuccess) return ens_fail(e, PDP3G_CUDA_ERROR, cudaGetErrorString(sync));
   int status[4] = {0, 0, 0, 0};
   EK(cudaMemcpy(status, e->d_status, sizeof(status), cudaMemcpyDeviceToHost));
-  const int done = status[0];
   for (auto *c : e->runs) {
-    for (int i = 0; i < done; i++) c->t = c->t + c->cfg.dt;
-    c->steps += done;
+    for (int i = 0; i < status[0]; i++) c->t = c->t + c->cfg.dt;
+    c->steps += status[0];
   }
-  e->last_ms = ms;
-  e->last_steps_done = done;
-  if (ms_out) *ms_out = ms;
-  if (status[1] == 1) return ens_fail(e, PDP3G_TIMEOUT, "ensemble cancelled");
-  if (status[1] == 2) return ens_fail(e, PDP3G_TIMEOUT, "ensemble time budget exhausted");
+  e->steps_total += status[0];
+  *ms_out = ms;
+  *done = status[0];
+  *stop = status[1];
+  return PDP3G_OK;
+}
+
+// re-sort every run's plasma species by cell (pdp3g_sort), device-timed
+static pdp3g_status ens_sort(pdp3g_ensemble *e, float *ms_out) {
+  cudaEvent_t a, b;
+  cudaEventCreate(&a);
+  cudaEventCreate(&b);
+  cudaEventRecord(a, e->stream);
+  for (auto *c : e->runs) {
+    EK(cudaStreamWaitEvent(c->stream, a, 0));
+    pdp3g_status st = sort_all(c);
+    if (st != PDP3G_OK) return ens_fail(e, st, "ensemble re-sort: " + c->last_error);
+    cudaEvent_t done;
+    cudaEventCreateWithFlags(&done, cudaEventDisableTiming);
+    cudaEventRecord(done, c->stream);
+    EK(cudaStreamWaitEvent(e->stream, done, 0));
+    cudaEventDestroy(done);
+  }
+  cudaEventRecord(b, e->stream);
+  EK(cudaStreamSynchronize(e->stream));
+  float ms = 0;
+  cudaEventElapsedTime(&ms, a, b);
+  cudaEventDestroy(a);
+  cudaEventDestroy(b);
+  *ms_out = ms;
+  return PDP3G_OK;
+}
+
+static pdp3g_status ens_run(pdp3g_ensemble *e, int nsteps, bool allow_graph, float *ms_out) {
+  EK(cudaSetDevice(e->device));
+  for (auto *c : e->runs) EK(cudaStreamSynchronize(c->stream));
+  float total = 0;
+  int done_total = 0, stop = 0;
+  while (done_total < nsteps && stop == 0) {
+    int seg = nsteps - done_total;
+    if (e->sort_interval > 0) {
+      if (e->steps_total % e->sort_interval == 0) {
+        float ms = 0;
+        pdp3g_status st = ens_sort(e, &ms);
+        if (st != PDP3G_OK) return st;
+        total += ms;
+      }
+      seg = std::min<int>(seg, e->sort_interval - (int)(e->steps_total % e->sort_interval));
+    }
+    // the budget covers the whole call: each segment gets what is left
+    const double saved_budget = e->budget_ms;
+    if (saved_budget > 0) {
+      if (total >= saved_budget) {
+        stop = 2;
+        break;
+      }
+      e->budget_ms = saved_budget - total;
+    }
+    float ms = 0;
+    int done = 0;
+    pdp3g_status st = ens_segment(e, seg, allow_graph, &ms, &done, &stop);
+    e->budget_ms = saved_budget;
+    if (st != PDP3G_OK) return st;
+    total += ms;
+    done_total += done;
+  }
+  e->last_ms = total;
+  e->last_steps_done = done_total;
+  if (ms_out) *ms_out = total;
+  if (stop == 1) return ens_fail(e, PDP3G_TIMEOUT, "ensemble cancelled");
+  if (stop == 2) return ens_fail(e, PDP3G_TIMEOUT, "ensemble time budget exhausted");
   return PDP3G_OK;
 }
 
@@ -1274,6 +1351,12 @@ pdp3g_status pdp3g_ensemble_autotune(pdp3g_ensemble *e, int32_t steps_per_trial,
   }
   e->blocks_per_sm = best_b;
   if (blocks_per_sm) *blocks_per_sm = best_b;
+  return PDP3G_OK;
+}
+
+pdp3g_status pdp3g_ensemble_set_sort_interval(pdp3g_ensemble *e, int32_t steps) {
+  if (!e || steps < 0) return PDP3G_INVALID_ARG;
+  e->sort_interval = steps;
   return PDP3G_OK;
 }
 
@@ -1331,7 +1414,8 @@ struct pdp3g_adjoint {
   std::vector<void *> allocs;
   int64_t bytes = 0;
   AdjGrids A{};
-  double *lgrids = nullptr;  // 12 grids: lE, lH, lHh, lJ
+  double *lgrids = nullptr;  // 9 grids: lE, lH, lHh
+  float *lj = nullptr;       // 3 grids: lJ
   std::vector<AdjSpeciesDev> ls;
   double *d_lv = nullptr;    // per species: adjoint of the bunch velocity
   double *d_loss = nullptr;
@@ -1339,7 +1423,7 @@ struct pdp3g_adjoint {
   std::vector<std::vector<AdjSnap>> ck_parts;  // [nwin + 1][species]
   std::vector<double> ck_t;
   std::vector<int64_t> ck_steps;
-  double *cap_fields = nullptr;                // interval x 6 grids (E, H half)
+  float *cap_fields = nullptr;                 // interval x 6 grids (E, H half), FP32
   std::vector<std::vector<AdjSnap>> cap_parts; // [interval][species]
   std::vector<double> cap_t;
   bool have_forward = false;
@@ -1426,11 +1510,8 @@ pdp3g_status adj_forward_step(pdp3g_adjoint *a, int cap) {
       CK(snap_copy(ctx->species[j].f32, a->cap_parts[cap][j], 0, ctx->stream));
   phase_calc_h(ctx);
   if (cap >= 0) {
-    double *dst = a->cap_fields + (size_t)cap * 6 * ng;
-    CK(cudaMemcpyAsync(dst, comp_ptr(ctx, PDP3G_E_R), sizeof(double) * 3 * ng,
-                       cudaMemcpyDeviceToDevice, ctx->stream));
-    CK(cudaMemcpyAsync(dst + 3 * ng, comp_ptr(ctx, PDP3G_H_R_HALF), sizeof(double) * 3 * ng,
-                       cudaMemcpyDeviceToDevice, ctx->stream));
+    adj_launch_capture_fields(comp_ptr(ctx, PDP3G_E_R), comp_ptr(ctx, PDP3G_H_R_HALF),
+                              a->cap_fields + (size_t)cap * 6 * ng, ng, ctx->stream);
   }
   CK(phase_reset_j(ctx));
   phase_particles(ctx);
@@ -1445,7 +1526,7 @@ void adj_reverse_step(pdp3g_adjoint *a, int cap) {
   const size_t ng = (size_t)ctx->cfg.n_grid_r * ctx->cfg.n_grid_z;
   cudaStream_t st = ctx->stream;
   adj_launch_e(ctx->g, a->A, st);
-  const double *E3 = a->cap_fields + (size_t)cap * 6 * ng;
+  const float *E3 = a->cap_fields + (size_t)cap * 6 * ng;
   for (size_t j = 0; j < ctx->species.size(); j++) {
     const Species &sp = ctx->species[j];
     AdjSpeciesDev S = a->ls[j];
@@ -1520,10 +1601,12 @@ pdp3g_status pdp3g_adjoint_create(pdp3g_ctx *ctx, int32_t window_steps,
       return cuda_fail(ctx, e, #call);              \
     }                                               \
   } while (0)
-  ACK(aalloc(a, &a->lgrids, 12 * ng));
+  ACK(aalloc(a, &a->lgrids, 9 * ng));
+  ACK(aalloc(a, &a->lj, 3 * ng));
   double *L = a->lgrids;
+  float *J = a->lj;
   a->A = AdjGrids{L, L + ng, L + 2 * ng, L + 3 * ng, L + 4 * ng, L + 5 * ng,
-                  L + 6 * ng, L + 7 * ng, L + 8 * ng, L + 9 * ng, L + 10 * ng, L + 11 * ng};
+                  L + 6 * ng, L + 7 * ng, L + 8 * ng, J, J + ng, J + 2 * ng};
   a->ls.resize(nsp);
   for (size_t j = 0; j < nsp; j++) {
     const size_t n = (size_t)ctx->species[j].f32.n;
@@ -1594,7 +1677,8 @@ pdp3g_status pdp3g_backward_window(pdp3g_adjoint *a) {
   cudaStream_t st = ctx->stream;
   const size_t ng = (size_t)ctx->cfg.n_grid_r * ctx->cfg.n_grid_z;
   CK(cudaEventRecord(a->ev0, st));
-  CK(cudaMemsetAsync(a->lgrids, 0, sizeof(double) * 12 * ng, st));
+  CK(cudaMemsetAsync(a->lgrids, 0, sizeof(double) * 9 * ng, st));
+  CK(cudaMemsetAsync(a->lj, 0, sizeof(float) * 3 * ng, st));
   for (size_t j = 0; j < a->ls.size(); j++) {
     const size_t n = (size_t)ctx->species[j].f32.n;
     AdjSpeciesDev &S = a->ls[j];

@@ -63,7 +63,11 @@ __device__ void ens_inject(const EnsembleDev &E, const EnsSpecies &sp) {
   }
 }
 
-__global__ void __launch_bounds__(F32_THREADS, 4) k_ensemble(EnsembleDev E, int nsteps) {
+// The step count is read from E.status[2] (written before each launch), so
+// one captured graph serves every segment length.
+__global__ void __launch_bounds__(F32_THREADS, 4) k_ensemble(EnsembleDev E) {
+  const int nsteps = *(volatile int *)&E.status[2];
+  const long long budget = *(volatile const long long *)E.budget_cycles;
   cg::grid_group grid = cg::this_grid();
   __shared__ F32Shared sm;
   __shared__ struct {
@@ -80,7 +84,7 @@ __global__ void __launch_bounds__(F32_THREADS, 4) k_ensemble(EnsembleDev E, int 
     if (gtid == 0) {
       int stop = 0;
       if (*E.cancel) stop = 1;
-      else if (E.budget_cycles > 0 && clock64() - t_start > E.budget_cycles) stop = 2;
+      else if (budget > 0 && clock64() - t_start > budget) stop = 2;
       E.status[1] = stop;
       __threadfence();
     }
@@ -151,9 +155,9 @@ int ensemble_max_blocks_per_sm() {
   return nb;
 }
 
-// One cooperative launch of nsteps steps (graph capture of this call is done
-// by the caller).
-cudaError_t ensemble_launch(const EnsembleDev &E, int nsteps, int blocks, cudaStream_t st) {
+// One cooperative launch of E.status[2] steps (graph capture of this call is
+// done by the caller).
+cudaError_t ensemble_launch(const EnsembleDev &E, int blocks, cudaStream_t st) {
   cudaLaunchConfig_t cfg = {};
   cfg.gridDim = dim3(blocks);
   cfg.blockDim = dim3(F32_THREADS);
@@ -164,7 +168,7 @@ cudaError_t ensemble_launch(const EnsembleDev &E, int nsteps, int blocks, cudaSt
   attr[0].val.cooperative = 1;
   cfg.attrs = attr;
   cfg.numAttrs = 1;
-  return cudaLaunchKernelEx(&cfg, k_ensemble, E, nsteps);
+  return cudaLaunchKernelEx(&cfg, k_ensemble, E);
 }
 
 }  // namespace pdp3g

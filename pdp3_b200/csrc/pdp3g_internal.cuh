@@ -142,12 +142,13 @@ struct EnsembleDev {
   long long total_h, total_e, total_j, total_chunks;
   const double *inv_pow11;
   volatile int *cancel;  // host-mapped
-  int *status;           // [0] steps done, [1] stop (0 run, 1 cancelled, 2 budget)
-  long long budget_cycles;
+  int *status;           // [0] steps done, [1] stop (0 run, 1 cancelled, 2 budget),
+                         // [2] steps to run (set before each launch)
+  const long long *budget_cycles;  // device: 0 = none (read at launch, so graphs see updates)
 };
 
 int ensemble_max_blocks_per_sm();
-cudaError_t ensemble_launch(const EnsembleDev &E, int nsteps, int blocks, cudaStream_t st);
+cudaError_t ensemble_launch(const EnsembleDev &E, int blocks, cudaStream_t st);
 
 // byte offsets of the radix sort's scratch (sort.cu)
 struct SortLayout {
@@ -198,7 +199,8 @@ struct AdjGrids {
   double *lEr, *lEphi, *lEz;     // adjoint of E
   double *lHr, *lHphi, *lHz;     // adjoint of H
   double *lHhr, *lHhphi, *lHhz;  // adjoint of the half-step H of the current step
-  double *lJr, *lJphi, *lJz;     // adjoint of the current step's J
+  float *lJr, *lJphi, *lJz;      // adjoint of the current step's J (read by the FP32
+                                 // particle reverse only, so stored in FP32)
 };
 
 struct AdjSpeciesDev {
@@ -209,8 +211,12 @@ struct AdjSpeciesDev {
 
 void adj_launch_e(const GridDev &g, const AdjGrids &A, cudaStream_t st);
 void adj_launch_h(const GridDev &g, const AdjGrids &A, cudaStream_t st);
-void adj_launch_particles(const GridDev &g, const double *E3, const double *Hh3,
+void adj_launch_particles(const GridDev &g, const float *E3, const float *Hh3,
                           const AdjSpeciesDev &S, const AdjGrids &A, int face, cudaStream_t st);
+// FP32 copy of the particle phase's field inputs: E (3 grids from e3) and the
+// half-step H (3 grids from hh3) into dst (6 grids)
+void adj_launch_capture_fields(const double *e3, const double *hh3, float *dst, size_t ng,
+                               cudaStream_t st);
 void adj_launch_inject(const AdjSpeciesDev &S, long long start, long long count, double dt,
                        double dz, double velocity, const double *inv_pow11, double *lv,
                        cudaStream_t st);

@@ -349,10 +349,27 @@ def bunch_init_np(n, radius, duration, velocity, density, dr, dz):
     return r, w, dr_dR, dw_dR
 
 
-def adjoint_gradient(wl, aux, plasma_adj, bunch_adj, bunch_dl_dv):
+def bunch_weight_jump_dR(n, radius, duration, velocity, density, dr, dz):
+    """Expected-jump part of dw_i/dR for Bunch::Bunch's weights.  The volume
+    sum v_total switches from pi r^2 dz to 2 pi r dr dz at r = dr, a jump of
+    pi dr^2 dz; the radii (R - dr) U_i + dr/2 (U_i the radical-inverse
+    sequence, uniform in [0, 1)) cross r = dr at the rate n (dr/2)/(R - dr)^2
+    per unit R, so the mean of v_total over the sequence moves by that rate
+    times the jump, which every weight feels through v_avg."""
+    r, w, _, _ = bunch_init_np(n, radius, duration, velocity, density, dr, dz)
+    far = r > dr
+    vol = np.where(far, 2 * PI * r * dr * dz, PI * r * r * dz)
+    v_avg = vol.sum() / n
+    dv_avg_jump = PI * dr * dr * dz * (dr / 2) / (radius - dr) ** 2
+    return -w * dv_avg_jump / v_avg
+
+
+def adjoint_gradient(wl, aux, plasma_adj, bunch_adj, bunch_dl_dv, mean_field=False):
     """dL/dtheta from the adjoints of the window's initial state.
     plasma_adj: per plasma species dict with "w" (dL/dw per particle);
-    bunch_adj: dict with "r" (dL/dr) and "w"; bunch_dl_dv: dL/dv_beam."""
+    bunch_adj: dict with "r" (dL/dr) and "w"; bunch_dl_dv: dL/dv_beam.
+    mean_field adds the expected jump term of the bunch weights' volume
+    branch (bunch_weight_jump_dR), to go with the adjoint's mean-field mode."""
     theta = aux["theta"]
     c = theta[:N_BUMPS]
     phi = bump_basis(aux["zc"], wl.z_size)           # (columns, bumps)
@@ -369,6 +386,9 @@ def adjoint_gradient(wl, aux, plasma_adj, bunch_adj, bunch_dl_dv):
     g[N_BUMPS] = bunch_dl_dv * dv_dgamma
     _, _, dr_dR, dw_dR = bunch_init_np(b.number_macro, b.radius, b.bunch_length / v, v,
                                        b.density, wl.dr, wl.dz)
+    if mean_field:
+        dw_dR = dw_dR + bunch_weight_jump_dR(b.number_macro, b.radius, b.bunch_length / v, v,
+                                             b.density, wl.dr, wl.dz)
     g[N_BUMPS + 1] = float(np.dot(bunch_adj["r"], dr_dR) + np.dot(bunch_adj["w"], dw_dR))
     return g
 

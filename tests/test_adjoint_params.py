@@ -71,3 +71,20 @@ def test_gradient_chain_rule():
         tm[j] -= h
         fd = (functional(tp) - functional(tm)) / (2 * h)
         assert abs(fd - g[j]) <= 1e-6 * max(abs(fd), abs(g[j])), (j, fd, g[j])
+
+
+def test_bunch_weight_jump_term():
+    """Bunch::Bunch's volume sum switches branch at r = dr; over an R step
+    that moves many radii across it, the mean weight's difference quotient
+    equals the pathwise derivative plus bunch_weight_jump_dR (and not the
+    pathwise derivative alone)."""
+    n, R, dr, dz, v = 10486, 5e-3, 7.8125e-4, 7.8125e-4, 2.9394e8
+    dur = 0.02 / v
+    _, _, _, dw = W.bunch_init_np(n, R, dur, v, 5e16, dr, dz)
+    jump = W.bunch_weight_jump_dR(n, R, dur, v, 5e16, dr, dz)
+    h = 1e-4
+    wp = W.bunch_init_np(n, R + h, dur, v, 5e16, dr, dz)[1]
+    wm = W.bunch_init_np(n, R - h, dur, v, 5e16, dr, dz)[1]
+    fd = np.mean((wp - wm) / (2 * h))
+    assert abs(fd / np.mean(dw + jump) - 1) <= 1e-4
+    assert abs(fd / np.mean(dw) - 1) >= 5e-3

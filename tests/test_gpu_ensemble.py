@@ -92,3 +92,26 @@ def test_ensemble_rejects_fp64_runs():
     sim = api.from_workload(wl, precision="fp64")
     with pytest.raises(api.Pdp3gError):
         api.Ensemble([sim])
+
+
+def test_ensemble_resorts_like_runs_stepped_alone():
+    """Runs configured to re-sort every 4 steps: the ensemble sorts them
+    between persistent launches (steps 0, 4, 8) as pdp3g_step does."""
+    wls = small_runs(3)
+    alone = [api.from_workload(wl, precision="fp32", sort_interval=4) for wl in wls]
+    batch = [api.from_workload(wl, precision="fp32", sort_interval=4) for wl in wls]
+    for s in alone:
+        s.step(10)
+        s.sync()
+    ens = api.Ensemble(batch)
+    ens.run(6)
+    ens.run(4)  # crosses the step-8 re-sort inside the call
+    assert ens.info()["last_steps_done"] == 4
+    for a, b in zip(alone, batch):
+        b.sync()
+        for c in ("E_z", "J_r", "J_phi"):
+            assert rel_inf(b.field(c), a.field(c)) <= 1e-4, c
+        sa, sb = a.species(0), b.species(0)
+        # same particles in the same slots after the same sorts
+        assert np.abs(sa["r"] - sb["r"]).max() <= 1e-6 * wls[0].r_size
+    ens.close()
