@@ -127,10 +127,10 @@ __device__ __forceinline__ void ladd(const GridDev &g, double *f, int i, int k, 
 }
 
 #ifndef ADJ_THREADS_PER_CTA
-#define ADJ_THREADS_PER_CTA 128
+#define ADJ_THREADS_PER_CTA 256
 #endif
 #ifndef ADJ_MIN_BLOCKS
-#define ADJ_MIN_BLOCKS 6  // CTAs per SM the register budget is sized for
+#define ADJ_MIN_BLOCKS 4  // CTAs per SM the register budget is sized for (64 registers)
 #endif
 // the particle reverse is latency-bound (gathers and adjoint reads behind
 // long dependency chains): more resident warps beat fewer register spills

@@ -618,24 +618,35 @@ static void inject_range(const pdp3g_ctx *ctx, const Species &sp, double t, long
   }
 }
 
+// Bunch::bunch_inject of one FP32 bunch into the arrays of `view` (the
+// species' own arrays, or a stored state of it)
+static void inject_f32(pdp3g_ctx *ctx, const Species &sp, const SpeciesF32 &view) {
+  long long start, count;
+  inject_range(ctx, sp, ctx->t, start, count);
+  if (count <= 0) return;
+  const double dl = sp.velocity * ctx->cfg.dt;
+  const double gv =
+      sp.velocity / (LIGHT_SPEED * std::sqrt(1.0 - sp.velocity * sp.velocity / LIGHT_SPEED_POW_2));
+  launch_bunch_inject_f32(view, start, count, dl, ctx->dz / 2.0, ctx->dz, ctx->cfg.n_grid_z - 1,
+                          (float)gv, ctx->d_inv_pow11, ctx->stream);
+  ctx->launches++;
+}
+
 // Bunch::bunch_inject for every bunch (src/bunch.cpp:87-124)
 static void phase_inject(pdp3g_ctx *ctx) {
   cudaStream_t st = ctx->stream;
   for (auto &sp : ctx->species) {
     if (!sp.is_bunch) continue;
+    if (sp.fp32) {
+      inject_f32(ctx, sp, sp.f32);
+      continue;
+    }
     long long start, count;
     inject_range(ctx, sp, ctx->t, start, count);
     if (count > 0) {
       const double dl = sp.velocity * ctx->cfg.dt;
-      if (sp.fp32) {
-        const double gv = sp.velocity / (LIGHT_SPEED * std::sqrt(1.0 - sp.velocity * sp.velocity /
-                                                                            LIGHT_SPEED_POW_2));
-        launch_bunch_inject_f32(sp.f32, start, count, dl, ctx->dz / 2.0, ctx->dz,
-                                ctx->cfg.n_grid_z - 1, (float)gv, ctx->d_inv_pow11, st);
-      } else {
-        launch_bunch_inject(sp.dev, start, count, dl, ctx->dz / 2.0, sp.velocity,
-                            ctx->d_inv_pow11, st);
-      }
+      launch_bunch_inject(sp.dev, start, count, dl, ctx->dz / 2.0, sp.velocity,
+                          ctx->d_inv_pow11, st);
       ctx->launches++;
     }
   }
@@ -1424,7 +1435,8 @@ struct pdp3g_adjoint {
   std::vector<double> ck_t;
   std::vector<int64_t> ck_steps;
   float *cap_fields = nullptr;                 // interval x 6 grids (E, H half), FP32
-  std::vector<std::vector<AdjSnap>> cap_parts; // [interval][species]
+  std::vector<std::vector<AdjSnap>> cap_parts; // [interval + 1][species]: states of the
+                                               // recomputed interval, slot j = step j's input
   std::vector<double> cap_t;
   bool have_forward = false;
   int face_terms = 1;
@@ -1500,21 +1512,51 @@ pdp3g_status adj_restore_checkpoint(pdp3g_adjoint *a, int idx) {
 // one step of the window (LoadInitParam::run's sequence without re-sorting:
 // the adjoint keeps every particle in its slot); cap >= 0 stores the
 // particle-phase input of the step into capture slot cap
+// species j's arrays replaced by state slot `slot` of the window
+SpeciesF32 slot_view(const pdp3g_adjoint *a, size_t j, int slot) {
+  SpeciesF32 v = a->ctx->species[j].f32;
+  const AdjSnap &sn = a->cap_parts[slot][j];
+  v.cell = sn.cell;
+  v.fr = sn.fr;
+  v.fz = sn.fz;
+  v.ur = sn.ur;
+  v.uphi = sn.uphi;
+  v.uz = sn.uz;
+  v.alive = sn.alive;
+  return v;
+}
+
+// one step of the window (LoadInitParam::run's sequence without re-sorting:
+// the adjoint keeps every particle in its slot).  cap < 0: the context's own
+// state, in place.  cap >= 0 (the backward's recompute): the particles of
+// state slot cap are injected into, pushed and written to slot cap + 1, so
+// slot cap keeps the particle phase's input for the reverse, with no copy.
 pdp3g_status adj_forward_step(pdp3g_adjoint *a, int cap) {
   pdp3g_ctx *ctx = a->ctx;
   const size_t ng = (size_t)ctx->cfg.n_grid_r * ctx->cfg.n_grid_z;
-  if (cap >= 0) a->cap_t[cap] = ctx->t;
-  phase_inject(ctx);
-  if (cap >= 0)
-    for (size_t j = 0; j < ctx->species.size(); j++)
-      CK(snap_copy(ctx->species[j].f32, a->cap_parts[cap][j], 0, ctx->stream));
-  phase_calc_h(ctx);
-  if (cap >= 0) {
-    adj_launch_capture_fields(comp_ptr(ctx, PDP3G_E_R), comp_ptr(ctx, PDP3G_H_R_HALF),
-                              a->cap_fields + (size_t)cap * 6 * ng, ng, ctx->stream);
+  if (cap < 0) {
+    phase_inject(ctx);
+    phase_calc_h(ctx);
+    CK(phase_reset_j(ctx));
+    phase_particles(ctx);
+    phase_calc_e(ctx);
+    phase_advance(ctx);
+    return PDP3G_OK;
   }
+  a->cap_t[cap] = ctx->t;
+  for (size_t j = 0; j < ctx->species.size(); j++)
+    if (ctx->species[j].is_bunch) inject_f32(ctx, ctx->species[j], slot_view(a, j, cap));
+  phase_calc_h(ctx);
+  adj_launch_capture_fields(comp_ptr(ctx, PDP3G_E_R), comp_ptr(ctx, PDP3G_H_R_HALF),
+                            a->cap_fields + (size_t)cap * 6 * ng, ng, ctx->stream);
   CK(phase_reset_j(ctx));
-  phase_particles(ctx);
+  for (size_t j = 0; j < ctx->species.size(); j++) {
+    const SpeciesF32 in = slot_view(a, j, cap), nx = slot_view(a, j, cap + 1);
+    launch_push_deposit_f32_to(ctx->g, in, in_place(nx), ctx->cfg.pusher, ctx->n_sm,
+                               ctx->f32_blocks_per_sm, ctx->stream);
+    ctx->launches++;
+    ctx->particle_launches++;
+  }
   phase_calc_e(ctx);
   phase_advance(ctx);
   return PDP3G_OK;
@@ -1531,14 +1573,7 @@ void adj_reverse_step(pdp3g_adjoint *a, int cap) {
     const Species &sp = ctx->species[j];
     AdjSpeciesDev S = a->ls[j];
     S.st = sp.f32;
-    const AdjSnap &sn = a->cap_parts[cap][j];
-    S.st.cell = sn.cell;
-    S.st.fr = sn.fr;
-    S.st.fz = sn.fz;
-    S.st.ur = sn.ur;
-    S.st.uphi = sn.uphi;
-    S.st.uz = sn.uz;
-    S.st.alive = sn.alive;
+    S.st = slot_view(a, j, cap);
     adj_launch_particles(ctx->g, E3, E3 + 3 * ng, S, a->A, a->face_terms, st);
     if (sp.is_bunch) {
       long long start, count;
@@ -1627,9 +1662,9 @@ pdp3g_status pdp3g_adjoint_create(pdp3g_ctx *ctx, int32_t window_steps,
   for (int c = 0; c <= a->nwin; c++)
     for (size_t j = 0; j < nsp; j++) ACK(snap_alloc(a, ctx->species[j].f32, a->ck_parts[c][j]));
   ACK(aalloc(a, &a->cap_fields, (size_t)a->interval * 6 * ng));
-  a->cap_parts.assign(a->interval, std::vector<AdjSnap>(nsp));
+  a->cap_parts.assign(a->interval + 1, std::vector<AdjSnap>(nsp));
   a->cap_t.assign(a->interval, 0.0);
-  for (int c = 0; c < a->interval; c++)
+  for (int c = 0; c <= a->interval; c++)
     for (size_t j = 0; j < nsp; j++) ACK(snap_alloc(a, ctx->species[j].f32, a->cap_parts[c][j]));
   ACK(cudaEventCreate(&a->ev0));
   ACK(cudaEventCreate(&a->ev1));
@@ -1695,6 +1730,8 @@ pdp3g_status pdp3g_backward_window(pdp3g_adjoint *a) {
     const int s0 = w * a->interval, s1 = std::min(a->window, s0 + a->interval);
     rs = adj_restore_checkpoint(a, w);
     if (rs != PDP3G_OK) return rs;
+    for (size_t j = 0; j < ctx->species.size(); j++)
+      CK(snap_copy(slot_view(a, j, 0), a->ck_parts[w][j], 1, st));
     for (int s = s0; s < s1; s++) {
       pdp3g_status fs = adj_forward_step(a, s - s0);
       if (fs != PDP3G_OK) return fs;

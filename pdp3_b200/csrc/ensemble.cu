@@ -127,7 +127,8 @@ __global__ void __launch_bounds__(F32_THREADS, 4) k_ensemble(EnsembleDev E) {
         desc.pusher = E.runs[E.species[sp].run].pusher;
       }
       __syncthreads();
-      for (long long c = first; c < ce; c += gridDim.x) f32_chunk(desc.g, desc.s, desc.pusher, c - cb, sm);
+      for (long long c = first; c < ce; c += gridDim.x)
+        f32_chunk<false>(desc.g, desc.s, SpeciesOut{}, desc.pusher, c - cb, sm);
     }
     grid.sync();
     // ---- phase C: E update, t += dt

@@ -40,14 +40,15 @@
 
 namespace pdp3g {
 
+template <bool OUT>
 __global__ void __launch_bounds__(F32_THREADS, 4) k_push_deposit_f32(GridDev g, SpeciesF32 s,
-                                                                   int pusher) {
+                                                                   SpeciesOut o, int pusher) {
   __shared__ F32Shared sm;
   const long long nchunks = (s.n + F32_THREADS - 1) / F32_THREADS;
   for (int idx = threadIdx.x; idx < 3 * TILE_CAP; idx += F32_THREADS) sm.acc[idx] = 0.0f;
   __syncthreads();
   for (long long chunk = blockIdx.x; chunk < nchunks; chunk += gridDim.x)
-    f32_chunk(g, s, pusher, chunk, sm);
+    f32_chunk<OUT>(g, s, o, pusher, chunk, sm);
 }
 
 // Bunch::bunch_inject in the cell-local form: z = dl * random_reverse(idx, 11)
@@ -203,7 +204,16 @@ void launch_push_deposit_f32(const GridDev &g, const SpeciesF32 &s, int pusher, 
   long long chunks = (s.n + F32_THREADS - 1) / F32_THREADS;
   long long blocks = (long long)n_sm * (blocks_per_sm > 0 ? blocks_per_sm : 4);
   if (blocks > chunks) blocks = chunks;
-  k_push_deposit_f32<<<(int)blocks, F32_THREADS, 0, st>>>(g, s, pusher);
+  k_push_deposit_f32<false><<<(int)blocks, F32_THREADS, 0, st>>>(g, s, in_place(s), pusher);
+}
+
+void launch_push_deposit_f32_to(const GridDev &g, const SpeciesF32 &s, const SpeciesOut &o,
+                                int pusher, int n_sm, int blocks_per_sm, cudaStream_t st) {
+  if (s.n <= 0) return;
+  long long chunks = (s.n + F32_THREADS - 1) / F32_THREADS;
+  long long blocks = (long long)n_sm * (blocks_per_sm > 0 ? blocks_per_sm : 4);
+  if (blocks > chunks) blocks = chunks;
+  k_push_deposit_f32<true><<<(int)blocks, F32_THREADS, 0, st>>>(g, s, o, pusher);
 }
 
 void launch_bunch_inject_f32(const SpeciesF32 &s, long long start, long long count, double dl,

@@ -249,8 +249,11 @@ struct F32Shared {
 // deposit (warp run-reduction -> shared tile -> FP64 grid) and store.
 // Called by every thread of the CTA (it synchronises the CTA); acc must be
 // zero on entry and is left zero.
-__device__ __forceinline__ void f32_chunk(const GridDev &g, const SpeciesF32 &s, int pusher,
-                                          long long chunk, F32Shared &sm) {
+// OUT = false: the step in place (o unused); OUT = true: results go to o.
+template <bool OUT>
+__device__ __forceinline__ void f32_chunk(const GridDev &g, const SpeciesF32 &s,
+                                          const SpeciesOut &o, int pusher, long long chunk,
+                                          F32Shared &sm) {
   float *acc = sm.acc;
   auto &red = sm.red;
   auto &box = sm.box;
@@ -427,7 +430,10 @@ __device__ __forceinline__ void f32_chunk(const GridDev &g, const SpeciesF32 &s,
         const float u1 = st * u[0] + ct * u[1];
         u[0] = u0;
         u[1] = u1;
-      } else {
+      }
+      if (OUT) {
+        if (s.alive != nullptr) o.alive[p] = alive_now ? 1 : 0;
+      } else if (!alive_now) {
         s.alive[p] = 0;
       }
       if (in > g.nr - 2 || kn > g.nz - 2) {
@@ -435,12 +441,23 @@ __device__ __forceinline__ void f32_chunk(const GridDev &g, const SpeciesF32 &s,
         in = min(in, g.nr - 2);
         kn = min(kn, g.nz - 2);
       }
-      s.cell[p] = in * ncz + kn;
-      s.fr[p] = an;
-      s.fz[p] = bn;
-      s.ur[p] = u[0];
-      s.uphi[p] = u[1];
-      s.uz[p] = u[2];
+      int *cell_o = OUT ? o.cell : s.cell;
+      float *fr_o = OUT ? o.fr : s.fr, *fz_o = OUT ? o.fz : s.fz;
+      float *ur_o = OUT ? o.ur : s.ur, *uphi_o = OUT ? o.uphi : s.uphi, *uz_o = OUT ? o.uz : s.uz;
+      cell_o[p] = in * ncz + kn;
+      fr_o[p] = an;
+      fz_o[p] = bn;
+      ur_o[p] = u[0];
+      uphi_o[p] = u[1];
+      uz_o[p] = u[2];
+    } else if (OUT && p < s.n) {
+      o.cell[p] = s.cell[p];
+      o.fr[p] = s.fr[p];
+      o.fz[p] = s.fz[p];
+      o.ur[p] = s.ur[p];
+      o.uphi[p] = s.uphi[p];
+      o.uz[p] = s.uz[p];
+      if (s.alive != nullptr) o.alive[p] = s.alive[p];
     }
     warp_run_deposit<0>(g, t, key_phi, phi_i, phi_k, vphi4);
     warp_run_deposit<1>(g, t, key_rz, rz_i, rz_k, vrz4);

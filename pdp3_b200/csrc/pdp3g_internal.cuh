@@ -66,6 +66,20 @@ struct SpeciesF32 {
   float inv_c2; // 1 / c^2
 };
 
+// Where the FP32 particle phase writes its result: the input arrays (the
+// step in place) or another state of the same species (the adjoint's
+// recompute writes step s+1's state next to step s's; then particles the
+// step skips, dead or not yet injected, are copied across).
+struct SpeciesOut {
+  int *cell;
+  float *fr, *fz, *ur, *uphi, *uz;
+  uint8_t *alive;
+};
+
+__host__ __device__ inline SpeciesOut in_place(const SpeciesF32 &s) {
+  return SpeciesOut{s.cell, s.fr, s.fz, s.ur, s.uphi, s.uz, s.alive};
+}
+
 // Particles::charge_weighting per particle, src/particles.cpp:101-226
 // (adds q at (r, z) into rho with the upstream volume weights).
 __device__ __forceinline__ void charge_weight_one(const GridDev &g, double *rho, double r,
@@ -172,6 +186,8 @@ int diag_blocks();
 void launch_finalize(const double *partials, int nblocks, int nv, double *out, cudaStream_t st);
 void launch_push_deposit_f32(const GridDev &g, const SpeciesF32 &s, int pusher, int n_sm,
                              int blocks_per_sm, cudaStream_t st);
+void launch_push_deposit_f32_to(const GridDev &g, const SpeciesF32 &s, const SpeciesOut &o,
+                                int pusher, int n_sm, int blocks_per_sm, cudaStream_t st);
 void launch_bunch_inject_f32(const SpeciesF32 &s, long long start, long long count, double dl,
                              double half_dz, double dz, int ncz, float uz,
                              const double *inv_pow11, cudaStream_t st);
