@@ -264,6 +264,9 @@ def main():
     ap.add_argument("--ppc", type=int, default=None,
                     help="macroparticles per cell (profiling runs on a smaller case)")
     ap.add_argument("--e2e-steps", type=int, default=3)
+    ap.add_argument("--accuracy-steps", type=int, default=1000,
+                    help="untimed FP32-vs-FP64 run of this many steps after the timing "
+                         "(0: skip)")
     ap.add_argument("--cpu-fraction", type=float, default=1.0 / 32)
     ap.add_argument("--cpu-steps", type=int, default=3)
     ap.add_argument("--no-cpu-baseline", action="store_true")
@@ -395,6 +398,14 @@ def main():
             cpu = {"value": None, "unit": UNIT, "cores": None, "kind": None,
                    "sample": "failed: %s" % exc}
 
+    # accuracy over a long run (untimed): both forms from the same initial
+    # state, FP64 diagnostics of each every `every` steps
+    accuracy = None
+    if world == 1 and args.accuracy_steps > 0:
+        sim.close()
+        accuracy = run_accuracy(api, wl, local_rank, args.accuracy_steps,
+                                max(1, args.accuracy_steps // 10))
+
     traffic = load_traffic(args.workload, head_prec, wl)
     if rank == 0:
         line = {
@@ -409,6 +420,7 @@ def main():
                        "l2": "inputs larger than L2 (particle state %.2f GB)"
                              % (bytes_particle_phase / 1e9)},
             "forms": forms,
+            "accuracy": accuracy,
             "cell_updates_per_s": n_nodes / (ms_fields / 1000.0) if ms_fields > 0 else None,
             "cell_updates_per_s_step": n_nodes * args.steps * world / (ms_max / 1000.0),
             "kernel_ms": {"particles": ms_part, "fields": ms_fields,
@@ -425,11 +437,42 @@ def main():
             "clocks": clk,
         }
         print(json.dumps(line), flush=True)
-    sim.close()
+    if accuracy is None:
+        sim.close()
     if dist is not None:
         dist.barrier()
         dist.destroy_process_group()
     return 0
+
+
+def run_accuracy(api, wl, device, steps, every):
+    """The FP32 cell-local form against the FP64 plain form over `steps`
+    steps from identical inputs: Gauss-law relative residual of each form and
+    the relative difference of their total field energies, every `every`
+    steps."""
+    sims = {p: api.from_workload(wl, precision=p, device=device) for p in ("fp32", "fp64")}
+    for s_ in sims.values():
+        s_.mark_initial_charge()
+    rows = []
+    done = 0
+    while done < steps:
+        k = min(every, steps - done)
+        for s_ in sims.values():
+            s_.step(k)
+        done += k
+        d = {p: s_.diagnostics() for p, s_ in sims.items()}
+        g = {p: d[p]["gauss_residual"] / d[p]["gauss_norm"] for p in d}
+        fe = abs(d["fp32"]["field_energy"] - d["fp64"]["field_energy"]) / d["fp64"]["field_energy"]
+        ke = abs(d["fp32"]["kinetic_energy"] - d["fp64"]["kinetic_energy"]) / \
+            d["fp64"]["kinetic_energy"]
+        rows.append({"step": done, "gauss_rel_fp32": g["fp32"], "gauss_rel_fp64": g["fp64"],
+                     "field_energy_rel_diff": fe, "kinetic_energy_rel_diff": ke})
+    for s_ in sims.values():
+        s_.close()
+    return {"steps": steps, "every": every,
+            "max_gauss_rel_fp32": max(r["gauss_rel_fp32"] for r in rows),
+            "max_field_energy_rel_diff": max(r["field_energy_rel_diff"] for r in rows),
+            "final": rows[-1], "trace": rows}
 
 
 def run_ensemble(args, rank, world, local_rank):
@@ -450,13 +493,22 @@ def run_ensemble(args, rank, world, local_rank):
     for s_ in sims:
         s_.step(args.warmup)
         s_.sync()
-    seq_ms = 0.0
+    # each run stepped alone, one after another: device time from the first
+    # to the last launch of each run's K steps (CUDA events on its stream),
+    # summed; the sum of its kernels' own times is reported beside it
+    seq_ms = seq_kernel_ms = 0.0
     for s_ in sims:
+        st_ = torch.cuda.ExternalStream(s_.stream_ptr, device=torch.device("cuda", local_rank))
+        e0 = torch.cuda.Event(enable_timing=True)
+        e1 = torch.cuda.Event(enable_timing=True)
         s_.reset_timing()
         s_.set_timing(True)
+        e0.record(st_)
         s_.step(args.steps)
+        e1.record(st_)
         s_.sync()
-        seq_ms += s_.timing()["ms_step_total"]
+        seq_ms += e0.elapsed_time(e1)
+        seq_kernel_ms += s_.timing()["ms_step_total"]
         s_.set_timing(False)
     ens = api.Ensemble(sims)
     bpsm = ens.autotune(2)
@@ -488,7 +540,10 @@ def run_ensemble(args, rank, world, local_rank):
             "ensemble": {"blocks_per_sm": bpsm, "blocks": info["blocks"],
                          "cuda_graph": bool(info["used_graph"]), "ms_per_step": ms / args.steps},
             "sequential": {"value": seq_value, "ms_per_step": seq_ms / args.steps,
-                           "note": "same runs, each stepped alone with per-run launches"},
+                           "kernel_ms_per_step": seq_kernel_ms / args.steps,
+                           "note": "same runs, each stepped alone with per-run launches; "
+                                   "ms_per_step spans each run's launches on its stream, "
+                                   "kernel_ms_per_step sums the kernels alone"},
             "ensemble_over_sequential": value / seq_value,
             "clocks": clk}), flush=True)
     ens.close()

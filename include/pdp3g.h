@@ -78,7 +78,9 @@ typedef struct {
   double field_energy;      /* 1/2 sum (eps0 E^2 + mu0 H^2) dV over node volumes */
   double kinetic_energy;    /* sum m_i c^2 (gamma_i - 1) over alive particles */
   double gauss_residual;    /* ||eps0 div E - (rho - rho_0)||_2 over the nodes
-                               2 <= i <= nr-3, 2 <= k <= nz-3 with sigma == 0 */
+                               2 <= i <= nr-3, 2 <= k <= nz-3 whose divergence
+                               stencil is undamped: sigma == 0 at (i,k), (i-1,k)
+                               and (i,k-1) (where the update conserves it) */
   double gauss_norm;        /* sqrt(sum over species ||rho_s||_2^2), same nodes:
                                the charge-density scale the residual is relative to */
   double charge_total;      /* sum rho dV */
@@ -113,9 +115,10 @@ pdp3g_status pdp3g_add_species(pdp3g_ctx *ctx, double charge_e, double mass_me, 
                                const double *vphi, const double *vz, const double *w,
                                const uint8_t *alive, int32_t *id);
 /* The same with the six FP64 arrays in device memory of the context's
-   device (e.g. generated there), all particles alive; the arrays are read
-   before the call returns.  No upstream counterpart (the upstream fills its
-   host arrays in place). */
+   device (e.g. generated there), all particles alive.  The call first waits
+   for all work on the device (the arrays may come from any stream) and has
+   read the arrays when it returns.  No upstream counterpart (the upstream
+   fills its host arrays in place). */
 pdp3g_status pdp3g_add_species_device(pdp3g_ctx *ctx, double charge_e, double mass_me,
                                       int64_t n, const double *r, const double *z,
                                       const double *vr, const double *vphi, const double *vz,

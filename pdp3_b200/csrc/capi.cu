@@ -41,6 +41,7 @@ struct pdp3g_ctx {
   cudaStream_t stream = nullptr;
   double dr = 0, dz = 0, t = 0;
   double *grid_mem = nullptr;
+  float *mirror = nullptr;       // FP32 contexts: E and half-step H in FP32 (6 grids)
   GridDev g{};
   unsigned *d_err = nullptr;
   double *d_inv_pow11 = nullptr;
@@ -134,6 +135,18 @@ double *comp_ptr(pdp3g_ctx *ctx, int comp) {
   size_t ng = (size_t)ctx->cfg.n_grid_r * ctx->cfg.n_grid_z;
   if (comp < 0 || comp >= PDP3G_NCOMP) return nullptr;
   return ctx->grid_mem + (size_t)comp * ng;
+}
+
+// keeps the FP32 copy of a gathered component (E, half-step H) equal to the
+// FP64 grid after the grid was written outside the Yee updates
+void refresh_mirror(pdp3g_ctx *ctx, int comp) {
+  if (!ctx->mirror) return;
+  const size_t ng = (size_t)ctx->cfg.n_grid_r * ctx->cfg.n_grid_z;
+  int slot = -1;
+  if (comp >= PDP3G_E_R && comp <= PDP3G_E_Z) slot = comp - PDP3G_E_R;
+  if (comp >= PDP3G_H_R_HALF && comp <= PDP3G_H_Z_HALF) slot = 3 + comp - PDP3G_H_R_HALF;
+  if (slot < 0) return;
+  launch_to_f32(comp_ptr(ctx, comp), ctx->mirror + (size_t)slot * ng, ng, ctx->stream);
 }
 
 // random_reverse(i, 9), src/math/rand.cpp:40-53 (host libm)
@@ -272,6 +285,14 @@ pdp3g_status pdp3g_create(const pdp3g_config *cfg, pdp3g_ctx **out) {
   g.jz = comp_ptr(ctx, PDP3G_J_Z);
   g.sigma = comp_ptr(ctx, PDP3G_SIGMA);
   g.err = ctx->d_err;
+  if (cfg->precision == PDP3G_FP32_CELL) {
+    if ((e = dalloc(ctx, &ctx->mirror, 6 * ng)) != cudaSuccess)
+      return bail(e == cudaErrorMemoryAllocation ? PDP3G_NO_MEMORY : PDP3G_CUDA_ERROR);
+    if ((e = cudaMemset(ctx->mirror, 0, sizeof(float) * 6 * ng)) != cudaSuccess)
+      return bail(PDP3G_CUDA_ERROR);
+    g.e32 = ctx->mirror;
+    g.hh32 = ctx->mirror + 3 * ng;
+  }
   if ((e = cudaDeviceSynchronize()) != cudaSuccess) return bail(PDP3G_CUDA_ERROR);
   *out = ctx;
   return PDP3G_OK;
@@ -301,6 +322,7 @@ void pdp3g_destroy(pdp3g_ctx *ctx) {
   for (auto &se : ctx->step_events)
     for (auto &e : se.ev) cudaEventDestroy(e);
   cudaFree(ctx->grid_mem);
+  cudaFree(ctx->mirror);
   cudaFree(ctx->d_err);
   cudaFree(ctx->d_inv_pow11);
   cudaFree(ctx->d_rho0);
@@ -453,6 +475,9 @@ pdp3g_status pdp3g_add_species_device(pdp3g_ctx *ctx, double charge_e, double ma
     return fail(ctx, PDP3G_INVALID_ARG, "add_species_device: null array");
   if (n > (int64_t)1 << 40) return fail(ctx, PDP3G_INVALID_ARG, "add_species_device: n too large");
   CK(cudaSetDevice(ctx->device));
+  // the arrays may have been written on any stream of the device: wait for
+  // all of it before reading them on the context's stream
+  CK(cudaDeviceSynchronize());
   const double *src[6] = {r, z, vr, vphi, vz, w};
   for (const double *p : src) {
     cudaPointerAttributes at{};
@@ -800,6 +825,8 @@ pdp3g_status pdp3g_set_field(pdp3g_ctx *ctx, int32_t comp, const double *host_in
   size_t ng = (size_t)ctx->cfg.n_grid_r * ctx->cfg.n_grid_z;
   CK(cudaMemcpyAsync(comp_ptr(ctx, comp), host_in, sizeof(double) * ng, cudaMemcpyHostToDevice,
                      ctx->stream));
+  refresh_mirror(ctx, comp);
+  CK(cudaGetLastError());
   CK(cudaStreamSynchronize(ctx->stream));
   return PDP3G_OK;
 }
@@ -1502,6 +1529,7 @@ pdp3g_status adj_restore_checkpoint(pdp3g_adjoint *a, int idx) {
   const size_t ng = (size_t)ctx->cfg.n_grid_r * ctx->cfg.n_grid_z;
   CK(cudaMemcpyAsync(comp_ptr(ctx, PDP3G_E_R), a->ck_fields + (size_t)idx * 6 * ng,
                      sizeof(double) * 6 * ng, cudaMemcpyDeviceToDevice, ctx->stream));
+  for (int c = PDP3G_E_R; c <= PDP3G_E_Z; c++) refresh_mirror(ctx, c);
   for (size_t j = 0; j < ctx->species.size(); j++)
     CK(snap_copy(ctx->species[j].f32, a->ck_parts[idx][j], 1, ctx->stream));
   ctx->t = a->ck_t[idx];
@@ -1547,8 +1575,9 @@ pdp3g_status adj_forward_step(pdp3g_adjoint *a, int cap) {
   for (size_t j = 0; j < ctx->species.size(); j++)
     if (ctx->species[j].is_bunch) inject_f32(ctx, ctx->species[j], slot_view(a, j, cap));
   phase_calc_h(ctx);
-  adj_launch_capture_fields(comp_ptr(ctx, PDP3G_E_R), comp_ptr(ctx, PDP3G_H_R_HALF),
-                            a->cap_fields + (size_t)cap * 6 * ng, ng, ctx->stream);
+  // the FP32 copies of E and the half-step H are current after the H update
+  CK(cudaMemcpyAsync(a->cap_fields + (size_t)cap * 6 * ng, ctx->mirror, sizeof(float) * 6 * ng,
+                     cudaMemcpyDeviceToDevice, ctx->stream));
   CK(phase_reset_j(ctx));
   for (size_t j = 0; j < ctx->species.size(); j++) {
     const SpeciesF32 in = slot_view(a, j, cap), nx = slot_view(a, j, cap + 1);

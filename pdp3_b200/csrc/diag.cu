@@ -56,6 +56,15 @@ __global__ void k_finalize(const double *partials, int nblocks, int nv, double *
   }
 }
 
+// Nodes where the discrete Gauss law is conserved by the update: the node's
+// divergence reads E_r at (i +- 1/2, k) and E_z at (i, k +- 1/2), stored at
+// nodes (i, k), (i-1, k) and (i, k), (i, k-1); when all of them are updated
+// without the absorbing layer's damping the curl-H terms cancel in the
+// divergence and the charge-conserving deposition keeps the residual.
+__device__ __forceinline__ bool gauss_node(const double *sigma, long long t, int nz) {
+  return sigma[t] == 0.0 && sigma[t - nz] == 0.0 && sigma[t - 1] == 0.0;
+}
+
 // v0: field energy, v1: sum res^2, v2: sum rho dV
 __global__ void __launch_bounds__(RED_THREADS) k_grid_diag(GridDev g, const double *rho,
                                                            const double *rho0,
@@ -72,7 +81,7 @@ __global__ void __launch_bounds__(RED_THREADS) k_grid_diag(GridDev g, const doub
     const double h2 = g.hr[t] * g.hr[t] + g.hphi[t] * g.hphi[t] + g.hz[t] * g.hz[t];
     v[0] += 0.5 * (EPSILON0 * e2 + MAGN_CONST * h2) * vol;
     v[2] += rho[t] * vol;
-    if (i >= 2 && i <= nr - 3 && k >= 2 && k <= nz - 3 && g.sigma[t] == 0.0) {
+    if (i >= 2 && i <= nr - 3 && k >= 2 && k <= nz - 3 && gauss_node(g.sigma, t, nz)) {
       const double div = (g.er[t] * (i + 0.5) - g.er[t - nz] * (i - 0.5)) / (i * dr) +
                          (g.ez[t] - g.ez[t - 1]) / dz;
       const double res = EPSILON0 * div - (rho[t] - (rho0 ? rho0[t] : 0.0));
@@ -91,7 +100,7 @@ __global__ void __launch_bounds__(RED_THREADS) k_rho_norm(GridDev g, const doubl
   for (long long t = blockIdx.x * (long long)blockDim.x + threadIdx.x; t < total;
        t += (long long)gridDim.x * blockDim.x) {
     const int i = (int)(t / nz), k = (int)(t - (long long)i * nz);
-    if (i >= 2 && i <= nr - 3 && k >= 2 && k <= nz - 3 && g.sigma[t] == 0.0)
+    if (i >= 2 && i <= nr - 3 && k >= 2 && k <= nz - 3 && gauss_node(g.sigma, t, nz))
       v[0] += rho[t] * rho[t];
   }
   block_reduce_store<1>(v, partials);

@@ -34,6 +34,12 @@ __global__ void __launch_bounds__(256) k_yee_e(GridDev g) {
   }
 }
 
+__global__ void k_to_f32(const double *src, float *dst, size_t n) {
+  for (size_t t = blockIdx.x * (size_t)blockDim.x + threadIdx.x; t < n;
+       t += (size_t)gridDim.x * blockDim.x)
+    dst[t] = (float)src[t];
+}
+
 static int grid_blocks(long long total) {
   long long b = (total + 255) / 256;
   if (b > 148 * 16) b = 148 * 16;
@@ -49,4 +55,13 @@ void launch_yee_e(const GridDev &g, cudaStream_t st) {
   k_yee_e<<<grid_blocks((long long)(g.nr - 1) * (g.nz - 1)), 256, 0, st>>>(g);
 }
 
+}  // namespace pdp3g
+
+namespace pdp3g {
+void launch_to_f32(const double *src, float *dst, size_t n, cudaStream_t st) {
+  long long b = ((long long)n + 255) / 256;
+  if (b > 148 * 16) b = 148 * 16;
+  if (b < 1) b = 1;
+  k_to_f32<<<(int)b, 256, 0, st>>>(src, dst, n);
+}
 }  // namespace pdp3g

@@ -18,19 +18,23 @@ __device__ __forceinline__ void yee_h_node(const GridDev &g, int i, int k) {
   const double ephi_ik1 = g.ephi[FIDX(i, k + 1)];
   const double a = dt * (ephi_ik1 - ephi_ik) / (dz * MAGN_CONST);
   const double hr = g.hr[FIDX(i, k)];
+  const size_t ng = (size_t)nr * nz;
   g.hrh[FIDX(i, k)] = hr + a / 2;
+  if (g.hh32) g.hh32[FIDX(i, k)] = (float)(hr + a / 2);
   g.hr[FIDX(i, k)] = hr + a;
   if (i < nr - 1) {
     const double b = dt * ((g.ez[FIDX(i + 1, k)] - g.ez[FIDX(i, k)]) / dr -
                            (g.er[FIDX(i, k + 1)] - g.er[FIDX(i, k)]) / dz) / MAGN_CONST;
     const double hphi = g.hphi[FIDX(i, k)];
     g.hphih[FIDX(i, k)] = hphi + b / 2;
+    if (g.hh32) g.hh32[ng + FIDX(i, k)] = (float)(hphi + b / 2);
     g.hphi[FIDX(i, k)] = hphi + b;
     const double ephi_i1k = g.ephi[FIDX(i + 1, k)];
     const double c = dt * ((ephi_i1k + ephi_ik) / (2.0 * dr * (i + 0.5)) +
                            (ephi_i1k - ephi_ik) / dr) / MAGN_CONST;
     const double hz = g.hz[FIDX(i, k)];
     g.hzh[FIDX(i, k)] = hz - c / 2;
+    if (g.hh32) g.hh32[2 * ng + FIDX(i, k)] = (float)(hz - c / 2);
     g.hz[FIDX(i, k)] = hz - c;
   }
 }
@@ -49,21 +53,31 @@ __device__ __forceinline__ void yee_e_node(const GridDev &g, int i, int k) {
   const double koef_e = (epsx2 - sigma_t) / (epsx2 + sigma_t);
   const double koef_h = 2 * dt / (epsx2 + sigma_t);
   const double hphi_ik = g.hphi[FIDX(i, k)];
+  const size_t ng = (size_t)g.nr * nz;
   if (k >= 1) {
-    g.er[FIDX(i, k)] = g.er[FIDX(i, k)] * koef_e -
-                       (g.jr[FIDX(i, k)] + (hphi_ik - g.hphi[FIDX(i, k - 1)]) / dz) * koef_h;
+    const double v = g.er[FIDX(i, k)] * koef_e -
+                     (g.jr[FIDX(i, k)] + (hphi_ik - g.hphi[FIDX(i, k - 1)]) / dz) * koef_h;
+    g.er[FIDX(i, k)] = v;
+    if (g.e32) g.e32[FIDX(i, k)] = (float)v;
   }
   if (i == 0) {
-    g.ez[FIDX(i, k)] = g.ez[FIDX(i, k)] * koef_e - (g.jz[FIDX(i, k)] - 4.0 / dr * hphi_ik) * koef_h;
+    const double v =
+        g.ez[FIDX(i, k)] * koef_e - (g.jz[FIDX(i, k)] - 4.0 / dr * hphi_ik) * koef_h;
+    g.ez[FIDX(i, k)] = v;
+    if (g.e32) g.e32[2 * ng + FIDX(i, k)] = (float)v;
   } else {
     const double hphi_m = g.hphi[FIDX(i - 1, k)];
-    g.ez[FIDX(i, k)] = g.ez[FIDX(i, k)] * koef_e -
-                       (g.jz[FIDX(i, k)] - (hphi_ik - hphi_m) / dr -
-                        (hphi_ik + hphi_m) / (2.0 * dr * i)) * koef_h;
+    const double v = g.ez[FIDX(i, k)] * koef_e -
+                     (g.jz[FIDX(i, k)] - (hphi_ik - hphi_m) / dr -
+                      (hphi_ik + hphi_m) / (2.0 * dr * i)) * koef_h;
+    g.ez[FIDX(i, k)] = v;
+    if (g.e32) g.e32[2 * ng + FIDX(i, k)] = (float)v;
     if (k >= 1) {
-      g.ephi[FIDX(i, k)] = g.ephi[FIDX(i, k)] * koef_e -
-                           (g.jphi[FIDX(i, k)] - (g.hr[FIDX(i, k)] - g.hr[FIDX(i, k - 1)]) / dz +
-                            (g.hz[FIDX(i, k)] - g.hz[FIDX(i - 1, k)]) / dr) * koef_h;
+      const double w = g.ephi[FIDX(i, k)] * koef_e -
+                       (g.jphi[FIDX(i, k)] - (g.hr[FIDX(i, k)] - g.hr[FIDX(i, k - 1)]) / dz +
+                        (g.hz[FIDX(i, k)] - g.hz[FIDX(i - 1, k)]) / dr) * koef_h;
+      g.ephi[FIDX(i, k)] = w;
+      if (g.e32) g.e32[ng + FIDX(i, k)] = (float)w;
     }
   }
 }

@@ -35,7 +35,8 @@ double *g_scratch_addr[NA_MAX_DEVICES] = {nullptr};
 // Block b sums nodes [b*NA_CHUNK, (b+1)*NA_CHUNK) and writes its three
 // partial sums to scratch[3b .. 3b+2].  The per-node terms are those of
 // pdp3g_diagnostics: 1/2 (eps0 E^2 + mu0 H^2) dV, the squared Gauss
-// residual eps0 div E - (rho - rho0) on the interior sigma == 0 nodes, and
+// residual eps0 div E - (rho - rho0) on the interior nodes whose divergence
+// stencil has sigma == 0 (node (i,k) and the nodes (i-1,k), (i,k-1)), and
 // rho dV.
 __global__ void __launch_bounds__(NA_THREADS)
     k_field_diag_chunks(const double *er, const double *ephi, const double *ez,
@@ -53,7 +54,9 @@ __global__ void __launch_bounds__(NA_THREADS)
     const double h2 = hr[t] * hr[t] + hphi[t] * hphi[t] + hz[t] * hz[t];
     v[0] += 0.5 * (EPSILON0 * e2 + MAGN_CONST * h2) * vol;
     v[2] += rho[t] * vol;
-    if (i >= 2 && i <= nr - 3 && k >= 2 && k <= nz - 3 && sigma[t] == 0.0) {
+    // nodes whose whole divergence stencil is updated without damping
+    if (i >= 2 && i <= nr - 3 && k >= 2 && k <= nz - 3 && sigma[t] == 0.0 &&
+        sigma[t - nz] == 0.0 && sigma[t - 1] == 0.0) {
       const double div = (er[t] * (i + 0.5) - er[t - nz] * (i - 0.5)) / (i * dr) +
                          (ez[t] - ez[t - 1]) / dz;
       const double res = EPSILON0 * div - (rho[t] - (rho0 ? rho0[t] : 0.0));

@@ -227,13 +227,15 @@ __device__ __forceinline__ void weights_zhalf(int k, float b, int &kz, float &w0
   w1 = (float)(k - kz) + b - 0.5f;
 }
 
-__device__ __forceinline__ float gather4(const GridDev &g, const double *__restrict__ f, int ir,
+// f: the FP32 copy of the component (GridDev::e32 / hh32), the same values
+// the FP64 grid rounds to
+__device__ __forceinline__ float gather4(const GridDev &g, const float *__restrict__ f, int ir,
                                          int kz, float wr0, float wr1, float wz0, float wz1) {
   if (ir > g.nr - 2) { flag32(g, ERR_OUT_OF_GRID); ir = g.nr - 2; }
   if (kz > g.nz - 2) { flag32(g, ERR_OUT_OF_GRID); kz = g.nz - 2; }
-  const float f00 = (float)__ldg(f + GIDX(ir, kz)), f10 = (float)__ldg(f + GIDX(ir + 1, kz));
-  const float f01 = (float)__ldg(f + GIDX(ir, kz + 1));
-  const float f11 = (float)__ldg(f + GIDX(ir + 1, kz + 1));
+  const float f00 = __ldg(f + GIDX(ir, kz)), f10 = __ldg(f + GIDX(ir + 1, kz));
+  const float f01 = __ldg(f + GIDX(ir, kz + 1));
+  const float f11 = __ldg(f + GIDX(ir + 1, kz + 1));
   return wz0 * (f00 * wr0 + f10 * wr1) + wz1 * (f01 * wr0 + f11 * wr1);
 }
 
@@ -308,12 +310,13 @@ __device__ __forceinline__ void f32_chunk(const GridDev &g, const SpeciesF32 &s,
       const float wzn0 = 1.0f - b, wzn1 = b;
       const int ir_n = i, kz_n = k;
       float e[3], h[3];
-      e[0] = gather4(g, g.er, ir_h, kz_n, wrh0, wrh1, wzn0, wzn1);
-      e[1] = gather4(g, g.ephi, ir_n, kz_n, wrn0, wrn1, wzn0, wzn1);
-      e[2] = gather4(g, g.ez, ir_n, kz_h, wrn0, wrn1, wzh0, wzh1);
-      h[0] = gather4(g, g.hrh, ir_n, kz_h, wrn0, wrn1, wzh0, wzh1);
-      h[1] = gather4(g, g.hphih, ir_h, kz_h, wrh0, wrh1, wzh0, wzh1);
-      h[2] = gather4(g, g.hzh, ir_h, kz_n, wrh0, wrh1, wzn0, wzn1);
+      const size_t ng = (size_t)g.nr * g.nz;
+      e[0] = gather4(g, g.e32, ir_h, kz_n, wrh0, wrh1, wzn0, wzn1);
+      e[1] = gather4(g, g.e32 + ng, ir_n, kz_n, wrn0, wrn1, wzn0, wzn1);
+      e[2] = gather4(g, g.e32 + 2 * ng, ir_n, kz_h, wrn0, wrn1, wzh0, wzh1);
+      h[0] = gather4(g, g.hh32, ir_n, kz_h, wrn0, wrn1, wzh0, wzh1);
+      h[1] = gather4(g, g.hh32 + ng, ir_h, kz_h, wrh0, wrh1, wzh0, wzh1);
+      h[2] = gather4(g, g.hh32 + 2 * ng, ir_h, kz_n, wrh0, wrh1, wzn0, wzn1);
       // ---- push
       float inv_g = 1.0f;
       if (pusher == 1) {

@@ -33,6 +33,10 @@ struct GridDev {
   double *jr, *jphi, *jz;
   const double *sigma;
   unsigned *err;
+  // FP32 contexts only (else null): FP32 copies of E (3 grids) and of the
+  // half-step H (3 grids, right after them), written by the Yee updates
+  // beside the FP64 values, gathered by the FP32 particle phase
+  float *e32, *hh32;
 };
 
 // FP64 structure-of-arrays species (the plain form).
@@ -176,6 +180,7 @@ int sort_keys(const unsigned *keys, long long n, int key_bits, char *scratch,
               unsigned *perm_out, cudaStream_t st);
 
 // host-side launchers (fields.cu, particles_f64.cu, particles_f32.cu, diag.cu)
+void launch_to_f32(const double *src, float *dst, size_t n, cudaStream_t st);
 void launch_yee_h(const GridDev &g, cudaStream_t st);
 void launch_yee_e(const GridDev &g, cudaStream_t st);
 void launch_push_deposit_f64(const GridDev &g, const SpeciesDev &s, int pusher, int n_sm,

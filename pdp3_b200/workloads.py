@@ -477,9 +477,11 @@ class DevicePlasma:
         sig = math.sqrt(self.t_ev * EL_CHARGE / EL_MASS)
         v = [torch.randn(n, generator=gen, device=dev, dtype=torch.float64) * sig
              for _ in range(3)]
+        torch.cuda.synchronize(dev)  # the library reads them on its own stream
         sim.add_species_device(-1.0, 1.0, r, z, v[0], v[1], v[2], w)
         del v
         zero = torch.zeros(n, device=dev, dtype=torch.float64)
+        torch.cuda.synchronize(dev)
         sim.add_species_device(1.0, self.ion_mass_me, r, z, zero, zero, zero, w)
         del r, z, w, zero, u
         torch.cuda.synchronize(dev)

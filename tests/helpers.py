@@ -111,6 +111,8 @@ def diagnostics_np(sim, n_species, rho0=None):
     mask = np.zeros((nr, nz), dtype=bool)
     mask[2:nr - 2, 2:nz - 2] = True
     mask &= sig == 0.0
+    mask[1:, :] &= sig[:-1, :] == 0.0   # E_r(i - 1/2) stored at node (i-1, k)
+    mask[:, 1:] &= sig[:, :-1] == 0.0   # E_z(k - 1/2) stored at node (i, k-1)
     div = np.zeros((nr, nz))
     div[1:, 1:] = (er[1:, 1:] * (i[1:] + 0.5) - er[:-1, 1:] * (i[1:] - 0.5)) / (i[1:] * dr) + \
         (ez[1:, 1:] - ez[1:, :-1]) / dz
