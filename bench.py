@@ -455,11 +455,16 @@ def run_accuracy(api, wl, device, steps, every):
         s_.mark_initial_charge()
     rows = []
     done = 0
+    first_status = {}
     while done < steps:
         k = min(every, steps - done)
         for s_ in sims.values():
             s_.step(k)
         done += k
+        for p, s_ in sims.items():
+            st = s_.status()   # device error flags (e.g. v >= c in the FP64 velocity form)
+            if st != 0 and p not in first_status:
+                first_status[p] = {"step": done, "status": st}
         d = {p: s_.diagnostics() for p, s_ in sims.items()}
         g = {p: d[p]["gauss_residual"] / d[p]["gauss_norm"] for p in d}
         fe = abs(d["fp32"]["field_energy"] - d["fp64"]["field_energy"]) / d["fp64"]["field_energy"]
@@ -469,7 +474,7 @@ def run_accuracy(api, wl, device, steps, every):
                      "field_energy_rel_diff": fe, "kinetic_energy_rel_diff": ke})
     for s_ in sims.values():
         s_.close()
-    return {"steps": steps, "every": every,
+    return {"steps": steps, "every": every, "status_events": first_status,
             "max_gauss_rel_fp32": max(r["gauss_rel_fp32"] for r in rows),
             "max_field_energy_rel_diff": max(r["field_energy_rel_diff"] for r in rows),
             "final": rows[-1], "trace": rows}

@@ -52,7 +52,6 @@ struct Tape {
   T f1, g1, wa, wb, dwa, dwb, pref;
   // second half move, walls, rotation
   T sr, sz, ur_sign, uz_sign, x2, r2, A, B;
-  T xa2_pre;  // radial end offset before the walls (relative to cell i)
   bool alive_now;
   int in, kn;
   T an, bn, st, ct, uout[3];
@@ -326,7 +325,6 @@ PDP3_HD void forward(const Consts<T> &C, Tape<T> &tp) {
   }
   // second half move and walls (positions relative to the start cell)
   T xa2 = tp.rr - T(tp.i) + tp.dr_h, b2 = tp.b1 + tp.dz_h;
-  tp.xa2_pre = xa2;
   tp.sr = 1;
   tp.sz = 1;
   tp.ur_sign = 1;
@@ -465,25 +463,6 @@ PDP3_HD void gather_rev(const Consts<T> &C, const Tape<T> &tp, const T f[4], boo
   if (C.face) l_a += lv * radial_jump(tp, f0, f1, f2, f3, wz0, wz1, rh);
 }
 
-// Reflection at the axis wall r = dr/2 flips u_r (src/particles.cpp:1318-
-// 1353): the step's output momentum jumps by 2 u_r (ct, st) when the
-// end point crosses the wall, while the position and the deposits are
-// continuous there.  A particle of cell 0 moving inward by d (|d| < 1/2)
-// would land on the wall from the start offset a* = 1/2 - d; with cell 0's
-// particles spread uniformly in volume over its domain [1/2, 1] (pdf a/0.375
-// per unit offset), its expected share of the jump per unit offset is
-// pdf(a*) (lambda_u . jump).
-template <typename T>
-PDP3_HD T axis_reflection_term(const Tape<T> &tp, const T l_uout[3]) {
-  if (tp.i != 0 || !tp.alive_now) return T(0);
-  const T d = tp.xa2_pre - tp.a;
-  if (!(d < T(0) && d > T(-0.5))) return T(0);
-  const T a_star = T(0.5) - d;
-  const T pdf = a_star / T(0.375);
-  const T j = T(2) * tp.up[0];
-  return pdf * j * (l_uout[0] * tp.ct + l_uout[1] * tp.st);
-}
-
 // ----------------------------------------------------------------- reverse
 
 // Inputs: l_an, l_bn, l_uout[3] (adjoints of the stored outputs), l_jphi[4]
@@ -577,7 +556,6 @@ PDP3_HD void reverse(const Consts<T> &C, const Tape<T> &tp, T l_an, T l_bn, cons
     l_up[1] += l_uout[1];
     l_up[2] += tp.uz_sign * l_uout[2];
   }
-  if (C.face) l_a += axis_reflection_term(tp, l_uout);
   // A = r2 - i, B = b2 (after walls), r2 = sqrt(x2^2 + dy^2), x2 = i + xa2
   l_r2 += l_A;
   l_x2 += l_r2 * tp.x2 / tp.r2;

@@ -10,8 +10,6 @@
 //    pathwise gather derivative plus radial_jump() equals the central
 //    difference of the particles' mean gathered value under a common radial
 //    shift, which includes the weights' jumps at faces and cell middles.
-// 3. axis reflection: the same with the momentum jump of the reflection at
-//    the axis wall (axis_reflection_term).
 // Prints one line per check and exits non-zero on failure.
 #include <cmath>
 #include <cstdio>
@@ -205,74 +203,8 @@ static int mean_field() {
   return worst < 1e-4 ? 0 : 1;
 }
 
-// 3. axis reflection: particles of cell 0 spread uniformly in volume over
-//    [1/2, 1] (pdf a/0.375), no fields (so no gather jump), moving inward
-//    with one momentum: the derivative of the mean of lambda . u_out under a
-//    common radial shift equals the mean of the pathwise l_a plus
-//    axis_reflection_term (the pathwise part alone misses the reflections).
-static int axis_reflection() {
-  Consts<T> C;
-  C.ke = 0.3; C.kb = 0.7; C.cr = 0.11; C.cz = 0.13; C.kphi = 1.3; C.kz = 0.9; C.kr = 1.1;
-  C.nr = 40; C.nz = 60; C.bunch = 0; C.face = 1;
-  double worst = 0, worst_pathwise = 0;
-  for (int trial = 0; trial < 6; trial++) {
-    const T u[3] = {-U(0.4, 1.6), U(-0.5, 0.5), U(-0.5, 0.5)};
-    const T lu[3] = {U(-1, 1), U(-1, 1), U(-1, 1)};
-    auto out = [&](T x, T *l_a_path, T *term) {
-      Tape<T> tp;
-      tp.i = (int)std::ceil(x) - 1;
-      tp.a = x - tp.i;
-      tp.k = 20;
-      tp.b = 0.4;
-      tp.w = 1.0;
-      for (int c = 0; c < 3; c++) {
-        tp.u[c] = u[c];
-        for (int n = 0; n < 4; n++) tp.fe[c][n] = tp.fh[c][n] = 0;
-      }
-      forward(C, tp);
-      if (l_a_path) {
-        const T zj[4] = {0, 0, 0, 0}, zp[3][4] = {{0, 0, 0, 0}, {0, 0, 0, 0}, {0, 0, 0, 0}};
-        T la, lb, l_u[3], lw, lfe[3][4], lfh[3][4];
-        Consts<T> Cp = C;
-        Cp.face = 0;
-        reverse(Cp, tp, T(0), T(0), lu, zj, zp, la, lb, l_u, lw, lfe, lfh);
-        *l_a_path = la;
-        *term = axis_reflection_term(tp, lu);
-      }
-      return lu[0] * tp.uout[0] + lu[1] * tp.uout[1] + lu[2] * tp.uout[2];
-    };
-    const int n = 400000;
-    const T h = 2e-4;
-    double mp = 0, mm = 0, mp2 = 0, mm2 = 0, path = 0, est = 0;
-    for (int q = 0; q < n; q++) {
-      const T v = (q + 0.5) / n;
-      const T x = std::sqrt(0.25 + 0.75 * v);  // pdf a / 0.375 on [1/2, 1]
-      T la, term;
-      out(x, &la, &term);
-      path += la;
-      est += la + term;
-      mp += out(x + h, nullptr, nullptr);
-      mm += out(x - h, nullptr, nullptr);
-      mp2 += out(x + 2 * h, nullptr, nullptr);
-      mm2 += out(x - 2 * h, nullptr, nullptr);
-    }
-    const double d1 = (mp - mm) / (2 * h) / n, d2 = (mp2 - mm2) / (4 * h) / n;
-    const double fd = 2 * d1 - d2;
-    const double e = std::fabs(fd - est / n) / std::fmax(std::fabs(fd), 1e-6);
-    const double ep = std::fabs(fd - path / n) / std::fmax(std::fabs(fd), 1e-6);
-    if (getenv("ADJ_VERBOSE")) printf("  fd %.6g est %.6g pathwise %.6g\n", fd, est / n, path / n);
-    worst = std::fmax(worst, e);
-    worst_pathwise = std::fmax(worst_pathwise, ep);
-  }
-  printf("axis reflection: worst rel err %.3g (pathwise alone %.3g)\n", worst, worst_pathwise);
-  // the term is an estimate: it uses the particle's own momentum rotation
-  // (ct, st at its own end point) for the one at the wall
-  return (worst < 3e-2 && worst_pathwise > 0.5) ? 0 : 1;
-}
-
 int main() {
   const int a = pathwise();
   const int b = mean_field();
-  const int c = axis_reflection();
-  return a | b | c;
+  return a | b;
 }

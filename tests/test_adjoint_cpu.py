@@ -4,8 +4,7 @@ central finite differences (tests/cpp/adjoint_particle_fd.cpp): the
 pathwise derivative to 1e-6 over 48,000 derivatives including face
 crossings, wall reflections and removed bunch particles, and the expected
 gather-jump terms against the mean gathered field of particles spread over
-whole cells to 1e-4, and the axis-reflection term against the mean output
-momentum of particles spread over cell 0 to 3e-2."""
+whole cells to 1e-4."""
 import os
 import shutil
 import subprocess
