@@ -191,6 +191,30 @@ pdp3g_status pdp3g_charge_density(pdp3g_ctx *ctx, uint32_t species_mask, double 
 pdp3g_status pdp3g_mark_initial_charge(pdp3g_ctx *ctx);
 pdp3g_status pdp3g_diagnostics(pdp3g_ctx *ctx, pdp3g_diag *out);
 
+/* ---- Probes (ProbePlain, src/probePlain.cpp:80-224; LoadInitParam::dump_data,
+   src/loadInitParam.cpp:319-398).  pdp3g_probe_read copies one probe's values
+   of a component, in the order ProbePlain::write prints them:
+     type 0 frame  rows start_r..end_r-1, each start_z..end_z-1
+     type 1 col    start_r..end_r-1 at start_z
+     type 2 row    start_z..end_z-1 at start_r
+     type 3 dot    (start_r, start_z)
+   comp is a grid component (PDP3G_E_R .. PDP3G_SIGMA) or
+   PDP3G_PROBE_RHO_BEAM (the charge weighting of every bunch, as dump_data's
+   rho_beam).  *count receives the number of values (at most capacity).
+   pdp3g_probe_particles is ProbePlain::mpwrite's selection (type 4): the
+   slots of species id, in slot order, whose cell (CELL_NUMBER of r and z)
+   lies in [start_r, end_r] x [start_z, end_z] (inclusive, as upstream),
+   alive or not; positions and velocities in the upstream units.  When more
+   than capacity match, *count receives the number needed and the call
+   returns PDP3G_INVALID_ARG. */
+#define PDP3G_PROBE_RHO_BEAM 100
+pdp3g_status pdp3g_probe_read(pdp3g_ctx *ctx, int32_t comp, int32_t type, int32_t start_r,
+                              int32_t start_z, int32_t end_r, int32_t end_z, double *host_out,
+                              int64_t capacity, int64_t *count);
+pdp3g_status pdp3g_probe_particles(pdp3g_ctx *ctx, int32_t id, int32_t start_r, int32_t start_z,
+                                   int32_t end_r, int32_t end_z, double *r, double *z, double *vr,
+                                   double *vphi, double *vz, int64_t capacity, int64_t *count);
+
 /* Per-kernel device timing with CUDA events on the context's stream. */
 pdp3g_status pdp3g_set_timing(pdp3g_ctx *ctx, int32_t enabled);
 pdp3g_status pdp3g_get_timing(pdp3g_ctx *ctx, pdp3g_timing *out);

@@ -17,6 +17,7 @@ COMP = {"E_r": E_R, "E_phi": E_PHI, "E_z": E_Z, "H_r": H_R, "H_phi": H_PHI, "H_z
         "H_r_half": H_R_HALF, "H_phi_half": H_PHI_HALF, "H_z_half": H_Z_HALF,
         "J_r": J_R, "J_phi": J_PHI, "J_z": J_Z, "sigma": SIGMA}
 PUSHERS = {"boris": 0, "vay": 1, "boris_classic": 2}
+PROBE_RHO_BEAM = 100
 PRECISIONS = {"fp64": 0, "fp32": 1}
 STATUS = {0: "ok", 1: "invalid argument", 2: "CUDA error", 3: "NaN position",
           4: "velocity >= c", 5: "particle outside the grid", 6: "timeout",
@@ -115,6 +116,10 @@ EXPORTS = [
     ("pdp3g_ensemble_destroy", None, [_VP]),
     ("pdp3g_field_diagnostics_noalloc", _I32, [_VP] * 9 + [_I32, _I32, ctypes.c_double,
                                                           ctypes.c_double, _VP, _VP]),
+    ("pdp3g_probe_read", _I32, [_VP] + [_I32] * 6 + [_D, ctypes.c_int64,
+                                                      ctypes.POINTER(ctypes.c_int64)]),
+    ("pdp3g_probe_particles", _I32, [_VP] + [_I32] * 5 + [_D] * 5 +
+     [ctypes.c_int64, ctypes.POINTER(ctypes.c_int64)]),
     ("pdp3g_adjoint_create", _I32, [_VP] + [_I32] * 6 + [ctypes.POINTER(_VP)]),
     ("pdp3g_forward_window", _I32, [_VP, _D]),
     ("pdp3g_backward_window", _I32, [_VP]),
@@ -255,6 +260,30 @@ class Simulation:
         out = np.empty(self.nr * self.nz)
         self._check(self.L.pdp3g_charge_density(self.h, mask, _p(out)), "charge_density")
         return out.reshape(self.nr, self.nz)
+
+    def probe(self, name, kind, start_r, start_z, end_r=0, end_z=0):
+        """ProbePlain's values of component `name` ("E_r" .. "J_z", "rho_beam")
+        for a probe of `kind` ("frame", "col", "row", "dot"), in write order."""
+        t = {"frame": 0, "col": 1, "row": 2, "dot": 3}[kind]
+        comp = PROBE_RHO_BEAM if name == "rho_beam" else COMP[name]
+        cap = max(1, (end_r - start_r) * max(end_z - start_z, 1)) if t == 0 else \
+            max(1, end_r - start_r, end_z - start_z)
+        out = np.empty(cap)
+        n = ctypes.c_int64()
+        self._check(self.L.pdp3g_probe_read(self.h, comp, t, start_r, start_z, end_r, end_z,
+                                            _p(out), cap, ctypes.byref(n)), "probe_read")
+        return out[:n.value]
+
+    def probe_particles(self, sid, start_r, start_z, end_r, end_z):
+        """ProbePlain::mpwrite's selection: dict r, z, vr, vphi, vz."""
+        cap = self.species_size(sid)
+        out = {k: np.empty(max(cap, 1)) for k in ("r", "z", "vr", "vphi", "vz")}
+        n = ctypes.c_int64()
+        self._check(self.L.pdp3g_probe_particles(
+            self.h, sid, start_r, start_z, end_r, end_z,
+            *[_p(out[k]) for k in ("r", "z", "vr", "vphi", "vz")], cap, ctypes.byref(n)),
+            "probe_particles")
+        return {k: v[:n.value] for k, v in out.items()}
 
     def mark_initial_charge(self):
         self._check(self.L.pdp3g_mark_initial_charge(self.h), "mark_initial_charge")

@@ -33,6 +33,7 @@ UNITS = {
     "diag.cu": [],
     "noalloc.cu": [],
     "adjoint.cu": ["--prec-div=false", "--prec-sqrt=false"],
+    "probe.cu": [],
 }
 HEADERS = ["pdp3g_internal.cuh", "particles_f32.cuh", "fields_body.cuh", "adjoint_particle.cuh"]
 

@@ -966,6 +966,139 @@ pdp3g_status pdp3g_charge_density(pdp3g_ctx *ctx, uint32_t mask, double *host_ou
   return PDP3G_OK;
 }
 
+// ProbePlain::write's region (src/probePlain.cpp:80-170) of one component
+pdp3g_status pdp3g_probe_read(pdp3g_ctx *ctx, int32_t comp, int32_t type, int32_t r0, int32_t z0,
+                              int32_t r1, int32_t z1, double *host_out, int64_t capacity,
+                              int64_t *count) {
+  if (!ctx || !host_out) return PDP3G_INVALID_ARG;
+  const int nr = ctx->cfg.n_grid_r, nz = ctx->cfg.n_grid_z;
+  long long n = 0;
+  bool ok = false;
+  switch (type) {
+    case 0:
+      ok = 0 <= r0 && r0 < r1 && r1 <= nr && 0 <= z0 && z0 < z1 && z1 <= nz;
+      n = (long long)(r1 - r0) * (z1 - z0);
+      break;
+    case 1:
+      ok = 0 <= r0 && r0 < r1 && r1 <= nr && 0 <= z0 && z0 < nz;
+      n = r1 - r0;
+      break;
+    case 2:
+      ok = 0 <= r0 && r0 < nr && 0 <= z0 && z0 < z1 && z1 <= nz;
+      n = z1 - z0;
+      break;
+    case 3:
+      ok = 0 <= r0 && r0 < nr && 0 <= z0 && z0 < nz;
+      n = 1;
+      break;
+  }
+  if (!ok) return fail(ctx, PDP3G_INVALID_ARG, "probe_read: region outside the grid");
+  if (capacity < n) return fail(ctx, PDP3G_INVALID_ARG, "probe_read: output too small");
+  const bool rho_beam = comp == PDP3G_PROBE_RHO_BEAM;
+  if (!rho_beam && (comp < 0 || comp >= PDP3G_NCOMP))
+    return fail(ctx, PDP3G_INVALID_ARG, "probe_read: unknown component");
+  CK(cudaSetDevice(ctx->device));
+  pdp3g_status es = ensure_scratch(ctx);
+  if (es != PDP3G_OK) return es;
+  const double *src = comp_ptr(ctx, rho_beam ? 0 : comp);
+  if (rho_beam) {
+    // LoadInitParam::dump_data: every bunch's charge_weighting into c_rho_bunch
+    uint32_t mask = 0;
+    for (size_t s = 0; s < ctx->species.size() && s < 32; s++)
+      if (ctx->species[s].is_bunch) mask |= 1u << s;
+    pdp3g_status rs = rho_into(ctx, mask, ctx->d_scratch2);
+    if (rs != PDP3G_OK) return rs;
+    src = ctx->d_scratch2;
+  }
+  launch_probe_gather(src, nz, type, r0, z0, r1, z1, n, ctx->d_scratch, ctx->stream);
+  ctx->launches++;
+  CK(cudaMemcpyAsync(host_out, ctx->d_scratch, sizeof(double) * (size_t)n, cudaMemcpyDeviceToHost,
+                     ctx->stream));
+  CK(cudaStreamSynchronize(ctx->stream));
+  if (count) *count = n;
+  return PDP3G_OK;
+}
+
+// ProbePlain::mpwrite's selection (src/probePlain.cpp:172-224)
+pdp3g_status pdp3g_probe_particles(pdp3g_ctx *ctx, int32_t id, int32_t r0, int32_t z0, int32_t r1,
+                                   int32_t z1, double *r, double *z, double *vr, double *vphi,
+                                   double *vz, int64_t capacity, int64_t *count) {
+  if (!ctx || !count || id < 0 || id >= (int32_t)ctx->species.size()) return PDP3G_INVALID_ARG;
+  CK(cudaSetDevice(ctx->device));
+  cudaStream_t st = ctx->stream;
+  const Species &sp = ctx->species[id];
+  const long long n = sp.fp32 ? sp.f32.n : sp.dev.n;
+  *count = 0;
+  if (n <= 0) return PDP3G_OK;
+  // the species in the upstream units: FP64 arrays in place, or the FP32
+  // cell-local state converted into the staging buffer
+  const double *src[5];
+  pdp3g_status rs = stage_reserve(ctx, (size_t)n * 2);  // 6n for the state, the rest for output
+  if (rs != PDP3G_OK) return rs;
+  double *S = ctx->d_stage;
+  if (sp.fp32) {
+    launch_cell_to_f64(sp.f32, ctx->dr, ctx->dz, ctx->cfg.n_grid_z - 1, S, S + n, S + 2 * n,
+                       S + 3 * n, S + 4 * n, nullptr, st);
+    ctx->launches++;
+    for (int a = 0; a < 5; a++) src[a] = S + (size_t)a * n;
+  } else {
+    src[0] = sp.dev.r;
+    src[1] = sp.dev.z;
+    src[2] = sp.dev.vr;
+    src[3] = sp.dev.vphi;
+    src[4] = sp.dev.vz;
+  }
+  const long long nb = mp_blocks(n);
+  unsigned *d_counts = nullptr;
+  unsigned long long *d_off = nullptr;
+  CK(cudaMalloc(&d_counts, sizeof(unsigned) * (size_t)nb));
+  cudaError_t e = cudaMalloc(&d_off, sizeof(unsigned long long) * (size_t)nb);
+  if (e != cudaSuccess) {
+    cudaFree(d_counts);
+    return cuda_fail(ctx, e, "probe_particles");
+  }
+  launch_mp_count(src[0], src[1], n, ctx->dr, ctx->dz, r0, z0, r1, z1, d_counts, st);
+  std::vector<unsigned> counts((size_t)nb);
+  std::vector<unsigned long long> off((size_t)nb);
+  e = cudaMemcpyAsync(counts.data(), d_counts, sizeof(unsigned) * (size_t)nb,
+                      cudaMemcpyDeviceToHost, st);
+  if (e == cudaSuccess) e = cudaStreamSynchronize(st);
+  unsigned long long total = 0;
+  for (long long b = 0; b < nb; b++) {
+    off[(size_t)b] = total;
+    total += counts[(size_t)b];
+  }
+  if (e == cudaSuccess && (long long)total <= capacity && total > 0) {
+    // the selected particles land after the converted state (6n staging holds 12n doubles
+    // after the reserve above)
+    double *D = S + (size_t)6 * n;
+    MpArrays arr;
+    for (int a = 0; a < 5; a++) {
+      arr.src[a] = src[a];
+      arr.dst[a] = D + (size_t)a * total;
+    }
+    e = cudaMemcpyAsync(d_off, off.data(), sizeof(unsigned long long) * (size_t)nb,
+                        cudaMemcpyHostToDevice, st);
+    if (e == cudaSuccess) {
+      launch_mp_write(arr, n, ctx->dr, ctx->dz, r0, z0, r1, z1, d_off, st);
+      ctx->launches++;
+      double *outs[5] = {r, z, vr, vphi, vz};
+      for (int a = 0; a < 5 && e == cudaSuccess; a++)
+        if (outs[a])
+          e = cudaMemcpyAsync(outs[a], arr.dst[a], sizeof(double) * (size_t)total,
+                              cudaMemcpyDeviceToHost, st);
+      if (e == cudaSuccess) e = cudaStreamSynchronize(st);
+    }
+  }
+  cudaFree(d_counts);
+  cudaFree(d_off);
+  if (e != cudaSuccess) return cuda_fail(ctx, e, "probe_particles");
+  *count = (int64_t)total;
+  if ((long long)total > capacity)
+    return fail(ctx, PDP3G_INVALID_ARG, "probe_particles: output too small (count holds the need)");
+  return PDP3G_OK;
+}
+
 pdp3g_status pdp3g_mark_initial_charge(pdp3g_ctx *ctx) {
   if (!ctx) return PDP3G_INVALID_ARG;
   CK(cudaSetDevice(ctx->device));

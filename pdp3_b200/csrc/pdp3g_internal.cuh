@@ -230,6 +230,19 @@ struct AdjSpeciesDev {
   double *lw;                          // adjoint of w (accumulated over steps)
 };
 
+// probes (probe.cu)
+struct MpArrays {
+  const double *src[5];  // r, z, v_r, v_phi, v_z of every slot
+  double *dst[5];        // the selected slots, compacted in slot order
+};
+void launch_probe_gather(const double *f, int nz, int type, int r0, int z0, int r1, int z1,
+                         long long n, double *out, cudaStream_t st);
+long long mp_blocks(long long n);
+void launch_mp_count(const double *r, const double *z, long long n, double dr, double dz, int r0,
+                     int z0, int r1, int z1, unsigned *counts, cudaStream_t st);
+void launch_mp_write(const MpArrays &arr, long long n, double dr, double dz, int r0, int z0,
+                     int r1, int z1, const unsigned long long *offsets, cudaStream_t st);
+
 void adj_launch_e(const GridDev &g, const AdjGrids &A, cudaStream_t st);
 void adj_launch_h(const GridDev &g, const AdjGrids &A, cudaStream_t st);
 void adj_launch_particles(const GridDev &g, const float *E3, const float *Hh3,

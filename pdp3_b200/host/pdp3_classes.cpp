@@ -1,8 +1,14 @@
 // Upstream-style C++ classes over the pdp3g C ABI (see pdp3_classes.h).
 #include "pdp3_classes.h"
 
+#include <sys/stat.h>
+
+#include <algorithm>
 #include <cmath>
+#include <cstdio>
 #include <cstring>
+#include <fstream>
+#include <iostream>
 #include <map>
 #include <memory>
 
@@ -384,6 +390,134 @@ void BoundaryMaxwellConditions::specify_initial_field(Geometry *cyl_geom, double
   }
   for (int k = 0; k < n2; k++) e_fld->field_phi[n1 - 1][k] = E_fi_upper;
   check(pdp3g_set_field(c, PDP3G_E_PHI, e_fld->field_phi[0]), c, "specify_initial_field");
+}
+
+
+
+// ------------------------------------------------------------------ probes
+
+namespace {
+
+void make_directory(const std::string &path) {  // lib::make_directory (mkdir -p)
+  std::string cur;
+  for (size_t i = 0; i <= path.size(); i++) {
+    if (i == path.size() || path[i] == '/') {
+      if (!cur.empty()) mkdir(cur.c_str(), 0755);
+    }
+    if (i < path.size()) cur += path[i];
+  }
+}
+
+}  // namespace
+
+ProbePlain::ProbePlain(const char *c_path, const char *c_component, int c_type, int c_start_r,
+                       int c_start_z, int c_end_r, int c_end_z, bool c_compress,
+                       int c_compress_level, int c_schedule, const char *c_specie) {
+  snprintf(path, sizeof(path), "%s", c_path);
+  snprintf(component, sizeof(component), "%s", c_component);
+  snprintf(specie, sizeof(specie), "%s", c_specie);
+  type = c_type;
+  start_r = c_start_r;
+  start_z = c_start_z;
+  end_r = c_end_r;
+  end_z = c_end_z;
+  schedule = c_schedule;
+  compress = c_compress;
+  compress_level = c_compress_level;
+  if (compress) std::cerr << "WARNING! compression is not supported by plaintext backend" << std::endl;
+  std::string result_component = c_component;
+  if (strcmp(c_specie, "none") != 0) result_component += std::string("/") + c_specie;
+  char buf[512];
+  switch (type) {
+    case 0:
+      snprintf(buf, sizeof(buf), "%s/%s/frame_%d:%d_%d:%d", c_path, result_component.c_str(),
+               c_start_r, c_start_z, c_end_r, c_end_z);
+      break;
+    case 1:
+      snprintf(buf, sizeof(buf), "%s/%s/col_%d", c_path, result_component.c_str(), c_start_z);
+      break;
+    case 2:
+      snprintf(buf, sizeof(buf), "%s/%s/row_%d", c_path, result_component.c_str(), c_start_r);
+      break;
+    case 3:
+      snprintf(buf, sizeof(buf), "%s/%s/dot_%d_%d", c_path, result_component.c_str(), c_start_r,
+               c_start_z);
+      break;
+    default:
+      snprintf(buf, sizeof(buf), "%s/%s/mpframe_%d:%d_%d:%d", c_path, result_component.c_str(),
+               c_start_r, c_start_z, c_end_r, c_end_z);
+      break;
+  }
+  path_result_ = buf;
+  make_directory(path_result_);
+}
+
+std::string ProbePlain::get_data_path(const char *name) const {
+  return path_result_ + "/" + name + ".dat";
+}
+
+static int probe_component(const char *c) {
+  static const char *names[] = {"E_r", "E_phi", "E_z", "H_r", "H_phi", "H_z"};
+  for (int i = 0; i < 6; i++)
+    if (strcmp(c, names[i]) == 0) return PDP3G_E_R + i;
+  if (strcmp(c, "J_r") == 0) return PDP3G_J_R;
+  if (strcmp(c, "J_phi") == 0) return PDP3G_J_PHI;
+  if (strcmp(c, "J_z") == 0) return PDP3G_J_Z;
+  if (strcmp(c, "rho_beam") == 0) return PDP3G_PROBE_RHO_BEAM;
+  return -1;
+}
+
+void ProbePlain::write(const char *name, pdp3g_ctx *ctx) {
+  const int comp = probe_component(component);
+  if (comp < 0) {
+    std::cerr << "WARNING! probe for component ``" << component << "'' does not exist. Skipping"
+              << std::endl;
+    return;
+  }
+  long long cap = 1;
+  if (type == 0) cap = (long long)(end_r - start_r) * (end_z - start_z);
+  if (type == 1) cap = end_r - start_r;
+  if (type == 2) cap = end_z - start_z;
+  std::vector<double> v((size_t)std::max<long long>(cap, 1));
+  int64_t n = 0;
+  check(pdp3g_probe_read(ctx, comp, type, start_r, start_z, end_r, end_z, v.data(),
+                         (int64_t)v.size(), &n),
+        ctx, "probe_read");
+  std::ofstream out_file(get_data_path(name), std::ios::app);
+  for (int64_t i = 0; i < n; i++) out_file << v[(size_t)i] << " ";
+}
+
+void ProbePlain::mpwrite(const char *name, pdp3g_ctx *ctx, int species_id) {
+  const int64_t cap = pdp3g_species_size(ctx, species_id);
+  std::vector<double> a[5];
+  for (auto &x : a) x.resize((size_t)std::max<int64_t>(cap, 1));
+  int64_t n = 0;
+  check(pdp3g_probe_particles(ctx, species_id, start_r, start_z, end_r, end_z, a[0].data(),
+                              a[1].data(), a[2].data(), a[3].data(), a[4].data(), cap, &n),
+        ctx, "probe_particles");
+  static const char *suffix[5] = {"_pos_r", "_pos_z", "_vel_r", "_vel_phi", "_vel_z"};
+  for (int c = 0; c < 5; c++) {
+    std::ofstream f(get_data_path((std::string(name) + suffix[c]).c_str()), std::ios::app);
+    for (int64_t i = 0; i < n; i++) f << a[c][(size_t)i] << " ";
+  }
+}
+
+void dump_probes(std::vector<ProbePlain *> &probes, pdp3g_ctx *ctx, Time *time,
+                 int frames_per_file, const std::vector<std::string> &species_names) {
+  for (ProbePlain *w : probes) {
+    if ((int)(time->current_time / time->delta_t) % w->schedule != 0) continue;
+    char file_name[64];
+    snprintf(file_name, sizeof(file_name), "%d", (int)floor(w->step_number / frames_per_file));
+    if (w->type == 4) {
+      // mpframes are named by their step number (no frames per file)
+      snprintf(file_name, sizeof(file_name), "%d", w->step_number);
+      for (size_t s = 0; s < species_names.size(); s++)
+        if (species_names[s] == w->component) w->mpwrite(file_name, ctx, (int)s);
+    } else {
+      w->write(file_name, ctx);
+    }
+    ++w->step_number;
+  }
 }
 
 }  // namespace pdp3gpu

@@ -196,6 +196,43 @@ class ParticlesList {
   void charge_weighting(ChargeDensity *rho);
 };
 
+// ProbePlain, include/probePlain.h:7-33 and src/probePlain.cpp:1-224: the
+// plain-text probe.  Files and formats are the upstream's: the result path
+// <path>/<component>[/<specie>]/{frame_R0:Z0_R1:Z1, col_Z, row_R, dot_R_Z,
+// mpframe_R0:Z0_R1:Z1}/<name>.dat, values printed with the stream's default
+// format and a trailing space, appended per dump.  write() reads only the
+// probe's region from the GPU (pdp3g_probe_read) instead of a host grid.
+class ProbePlain {
+ public:
+  char path[256];
+  char component[16];
+  char specie[100];
+  int type;  // 0 frame, 1 col, 2 row, 3 dot, 4 mpframe
+  int start_r, start_z, end_r, end_z;
+  bool compress;
+  int compress_level;
+  int schedule;
+  int step_number = 0;
+  ProbePlain(const char *c_path, const char *c_component, int c_type, int c_start_r,
+             int c_start_z, int c_end_r, int c_end_z, bool c_compress, int c_compress_level,
+             int c_schedule, const char *c_specie = "none");
+  std::string get_data_path(const char *name) const;
+  void write(const char *name, pdp3g_ctx *ctx);                  // types 0-3
+  void mpwrite(const char *name, pdp3g_ctx *ctx, int species_id);  // type 4
+  const std::string &result_path() const { return path_result_; }
+
+ private:
+  std::string path_result_;
+};
+
+// LoadInitParam::dump_data's probe loop (src/loadInitParam.cpp:319-398) for
+// the grid components and mpframes: each probe whose schedule divides
+// (int)(t / dt) writes file floor(step_number / frames_per_file).
+// species_names: the species of the device context in order (mpframe probes
+// name one as their component).
+void dump_probes(std::vector<ProbePlain *> &probes, pdp3g_ctx *ctx, Time *time,
+                 int frames_per_file, const std::vector<std::string> &species_names);
+
 // BoundaryMaxwellConditions, include/boundaryMaxwellConditions.h:6-16
 // (never instantiated by the upstream loop; kept for interface parity)
 class BoundaryMaxwellConditions {

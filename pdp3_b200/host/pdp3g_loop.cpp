@@ -11,8 +11,14 @@
 // and optionally beam_charge beam_mass beam_number_macro beam_length
 // beam_radius beam_density beam_velocity beam_number_bunches beam_distance.
 // Species arrays are raw float64 files species<s>_{r,z,vr,vphi,vz,w}.f64.
-// The loop writes E_r.. J_z (raw float64 [n_grid_r*n_grid_z]) and every
-// species' r, z, vr, vphi, vz, alive to <out_dir>, and prints one JSON line.
+// Optional <case_dir>/probes.txt: one ProbePlain per line,
+//   <type> <component> <start_r> <start_z> <end_r> <end_z> <schedule>
+// (type 0 frame, 1 col, 2 row, 3 dot, 4 mpframe; an mpframe's component
+// names a species: species<s> or Beam#<k>), written under <out_dir>/probes
+// by dump_data's schedule test after every step (key dump_frames_per_file,
+// default 1).  The loop writes E_r.. J_z (raw float64
+// [n_grid_r*n_grid_z]) and every species' r, z, vr, vphi, vz, alive to
+// <out_dir>, and prints one JSON line.
 #include <chrono>
 #include <cmath>
 #include <cstdio>
@@ -90,8 +96,10 @@ int main(int argc, char **argv) {
     Current c_current(&geom);
     std::vector<std::unique_ptr<Particles>> owned;
     const int nsp = (int)get("n_species");
+    std::vector<std::string> species_names;
     for (int s = 0; s < nsp; s++) {
       const std::string p = "species" + std::to_string(s) + "_";
+      species_names.push_back("species" + std::to_string(s));
       const size_t n = (size_t)get(p + "n");
       auto r = read_f64(cdir + "/" + p + "r.f64", n), z = read_f64(cdir + "/" + p + "z.f64", n);
       auto vr = read_f64(cdir + "/" + p + "vr.f64", n);
@@ -130,11 +138,26 @@ int main(int argc, char **argv) {
                                      get("beam_velocity"), current_bunch_number, hole_duration));
         Bunch *b = static_cast<Bunch *>(owned.back().get());
         p_list.part_list.push_back(b);
+        species_names.push_back(name);
         c_bunches.push_back(b);
         ++current_bunch_number;
       }
       for (Bunch *b : c_bunches) b->bunch_inject(&time);
     };
+    // probes (LoadInitParam::init_probes / dump_data)
+    std::vector<std::unique_ptr<ProbePlain>> probe_store;
+    std::vector<ProbePlain *> probes;
+    {
+      std::ifstream pf(cdir + "/probes.txt");
+      int type, r0, z0, r1, z1, sched;
+      std::string comp;
+      while (pf >> type >> comp >> r0 >> z0 >> r1 >> z1 >> sched) {
+        probe_store.emplace_back(new ProbePlain((odir + "/probes").c_str(), comp.c_str(), type, r0,
+                                                z0, r1, z1, false, 0, sched));
+        probes.push_back(probe_store.back().get());
+      }
+    }
+    const int frames_per_file = (int)get("dump_frames_per_file", 1);
     // LoadInitParam::run (src/loadInitParam.cpp:471-587)
     auto t0 = std::chrono::steady_clock::now();
     int done = 0;
@@ -148,6 +171,8 @@ int main(int argc, char **argv) {
       p_list.full_current_distribution(&c_current, &time);
       efield.calc_field(&hfield, &time, &c_current);
       c_rho_new.reset_rho();
+      if (!probes.empty())
+        dump_probes(probes, Device::of(&geom).ctx(&time), &time, frames_per_file, species_names);
       time.current_time = time.current_time + time.delta_t;
       ++done;
     }
