@@ -208,9 +208,25 @@ pdp3g_status pdp3g_diagnostics(pdp3g_ctx *ctx, pdp3g_diag *out);
    than capacity match, *count receives the number needed and the call
    returns PDP3G_INVALID_ARG. */
 #define PDP3G_PROBE_RHO_BEAM 100
+#define PDP3G_PROBE_T 101        /* per species: pdp3g_probe_read_species */
+#define PDP3G_PROBE_DENSITY 102  /* per species: pdp3g_probe_read_species */
 pdp3g_status pdp3g_probe_read(pdp3g_ctx *ctx, int32_t comp, int32_t type, int32_t start_r,
                               int32_t start_z, int32_t end_r, int32_t end_z, double *host_out,
                               int64_t capacity, int64_t *count);
+/* dump_data's per-species components (src/loadInitParam.cpp:369-390):
+   comp PDP3G_PROBE_T: TemperatureClassic, src/temperatureClassic.cpp:57-159,
+   in eV, empty cells NaN as upstream; comp PDP3G_PROBE_DENSITY:
+   ParticlesDensity::calc_density, src/particlesDensity.cpp:45-257. */
+pdp3g_status pdp3g_probe_read_species(pdp3g_ctx *ctx, int32_t comp, int32_t id, int32_t type,
+                                      int32_t start_r, int32_t start_z, int32_t end_r,
+                                      int32_t end_z, double *host_out, int64_t capacity,
+                                      int64_t *count);
+/* TemperatureClassic::calc_t + normalize of species id: [n_grid_r][n_grid_z]
+   host grid, values for i < n_grid_r-1, k < n_grid_z-1 (the rest 0). */
+pdp3g_status pdp3g_temperature(pdp3g_ctx *ctx, int32_t id, double *host_out);
+/* ParticlesDensity::calc_density of species id: [n_grid_r][n_grid_z] host
+   grid (mass_array / EL_MASS per m^3 over the four nodes of each particle). */
+pdp3g_status pdp3g_density(pdp3g_ctx *ctx, int32_t id, double *host_out);
 pdp3g_status pdp3g_probe_particles(pdp3g_ctx *ctx, int32_t id, int32_t start_r, int32_t start_z,
                                    int32_t end_r, int32_t end_z, double *r, double *z, double *vr,
                                    double *vphi, double *vz, int64_t capacity, int64_t *count);

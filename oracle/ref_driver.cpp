@@ -35,6 +35,8 @@
 #include "particles.h"
 #include "particlesList.h"
 #include "bunch.h"
+#include "particlesDensity.h"
+#include "temperatureClassic.h"
 
 namespace {
 
@@ -59,7 +61,22 @@ struct RefSim {
   BeamParams beam;
   int current_bunch_number = 0;
   std::vector<char *> names;
+  TemperatureClassic *temperature = nullptr;  // LoadInitParam's diagnostics
+  ParticlesDensity *density = nullptr;
 };
+
+// The upstream diagnostics index CELL_NUMBER(r), CELL_NUMBER(z) (and +1)
+// unchecked: a particle at r <= 0 or z <= 0, or beyond the grid, would write
+// outside their arrays.  The driver refuses such species instead.
+bool cells_inside(RefSim *s, Particles *p) {
+  const double dr = s->geom->dr, dz = s->geom->dz;
+  for (unsigned int i = 0; i < p->number; i++) {
+    const int ri = CELL_NUMBER(p->pos[i][0], dr), zk = CELL_NUMBER(p->pos[i][2], dz);
+    if (ri < 0 || zk < 0 || ri + 1 >= (int)s->geom->n_grid_r || zk + 1 >= (int)s->geom->n_grid_z)
+      return false;
+  }
+  return true;
+}
 
 char *keep_name(RefSim *s, const char *name) {
   char *c = strdup(name ? name : "species");
@@ -318,6 +335,41 @@ void ref_charge_density(void *h, double *out) {
   s->plist->charge_weighting(s->rho_new);
   int nr = s->geom->n_grid_r, nz = s->geom->n_grid_z;
   copy_rows(s->rho_new->get_rho(), nr, nz, nz, out);
+}
+
+// The dump_data diagnostics (src/loadInitParam.cpp:369-390) of list entry
+// idx: TemperatureClassic reset/calc_t/normalize (t: [n_grid_r-1][n_grid_z-1])
+// and ParticlesDensity reset/calc_density (density, rows i <= n_grid_r-1,
+// columns k <= n_grid_z-1 as written).  Both constructors size their arrays
+// one row and one column short of what reset() and the weighting write; the
+// handle keeps one instance of each and the tests use grids whose
+// n_grid_r - 1 and n_grid_z - 1 are even, where glibc's 16-byte chunk
+// rounding leaves the extra element inside each allocation.
+int ref_temperature(void *h, int idx, double *out) {
+  RefSim *s = (RefSim *)h;
+  if (idx < 0 || idx >= (int)s->plist->part_list.size()) return -1;
+  Particles *p = s->plist->part_list[idx];
+  if (!cells_inside(s, p)) return -2;
+  if (!s->temperature) s->temperature = new TemperatureClassic(s->geom);
+  s->temperature->reset();
+  s->temperature->calc_t(p);
+  s->temperature->normalize(p);
+  const int nr = s->geom->n_grid_r, nz = s->geom->n_grid_z;
+  copy_rows(s->temperature->t, nr - 1, nz - 1, nz - 1, out);
+  return 0;
+}
+
+int ref_density(void *h, int idx, double *out) {
+  RefSim *s = (RefSim *)h;
+  if (idx < 0 || idx >= (int)s->plist->part_list.size()) return -1;
+  Particles *p = s->plist->part_list[idx];
+  if (!cells_inside(s, p)) return -2;
+  if (!s->density) s->density = new ParticlesDensity(s->geom);
+  s->density->reset();
+  s->density->calc_density(p);
+  const int nr = s->geom->n_grid_r, nz = s->geom->n_grid_z;
+  copy_rows(s->density->density, nr, nz, nz, out);
+  return 0;
 }
 
 double ref_sigma(void *h, int i, int k) { return ((RefSim *)h)->geom->sigma[i][k]; }

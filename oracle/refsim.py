@@ -72,6 +72,9 @@ def load(pusher="boris"):
     L.ref_get_species.argtypes = [ctypes.c_void_p, ctypes.c_int] + [_D] * 7 + [_U8]
     L.ref_charge_density.restype = None
     L.ref_charge_density.argtypes = [ctypes.c_void_p, _D]
+    for f in (L.ref_temperature, L.ref_density):
+        f.restype = ctypes.c_int
+        f.argtypes = [ctypes.c_void_p, ctypes.c_int, _D]
     L.ref_sigma.restype = ctypes.c_double
     L.ref_sigma.argtypes = [ctypes.c_void_p, ctypes.c_int, ctypes.c_int]
     L.ref_destroy.restype = None
@@ -152,6 +155,20 @@ class RefSim:
     def charge_density(self):
         out = np.zeros(self.nr * self.nz)
         self.L.ref_charge_density(self.h, _p(out))
+        return out.reshape(self.nr, self.nz)
+
+    def temperature(self, idx):
+        """TemperatureClassic of list entry idx: [n_grid_r-1, n_grid_z-1]."""
+        out = np.zeros((self.nr - 1) * (self.nz - 1))
+        rc = self.L.ref_temperature(self.h, idx, _p(out))
+        assert rc == 0, rc
+        return out.reshape(self.nr - 1, self.nz - 1)
+
+    def density(self, idx):
+        """ParticlesDensity of list entry idx: [n_grid_r, n_grid_z]."""
+        out = np.zeros(self.nr * self.nz)
+        rc = self.L.ref_density(self.h, idx, _p(out))
+        assert rc == 0, rc
         return out.reshape(self.nr, self.nz)
 
     def close(self):

@@ -18,6 +18,8 @@ COMP = {"E_r": E_R, "E_phi": E_PHI, "E_z": E_Z, "H_r": H_R, "H_phi": H_PHI, "H_z
         "J_r": J_R, "J_phi": J_PHI, "J_z": J_Z, "sigma": SIGMA}
 PUSHERS = {"boris": 0, "vay": 1, "boris_classic": 2}
 PROBE_RHO_BEAM = 100
+PROBE_T = 101
+PROBE_DENSITY = 102
 PRECISIONS = {"fp64": 0, "fp32": 1}
 STATUS = {0: "ok", 1: "invalid argument", 2: "CUDA error", 3: "NaN position",
           4: "velocity >= c", 5: "particle outside the grid", 6: "timeout",
@@ -118,6 +120,10 @@ EXPORTS = [
                                                           ctypes.c_double, _VP, _VP]),
     ("pdp3g_probe_read", _I32, [_VP] + [_I32] * 6 + [_D, ctypes.c_int64,
                                                       ctypes.POINTER(ctypes.c_int64)]),
+    ("pdp3g_probe_read_species", _I32, [_VP] + [_I32] * 7 + [_D, ctypes.c_int64,
+                                                              ctypes.POINTER(ctypes.c_int64)]),
+    ("pdp3g_temperature", _I32, [_VP, _I32, _D]),
+    ("pdp3g_density", _I32, [_VP, _I32, _D]),
     ("pdp3g_probe_particles", _I32, [_VP] + [_I32] * 5 + [_D] * 5 +
      [ctypes.c_int64, ctypes.POINTER(ctypes.c_int64)]),
     ("pdp3g_adjoint_create", _I32, [_VP] + [_I32] * 6 + [ctypes.POINTER(_VP)]),
@@ -272,6 +278,32 @@ class Simulation:
         n = ctypes.c_int64()
         self._check(self.L.pdp3g_probe_read(self.h, comp, t, start_r, start_z, end_r, end_z,
                                             _p(out), cap, ctypes.byref(n)), "probe_read")
+        return out[:n.value]
+
+    def temperature(self, sid):
+        """TemperatureClassic of species sid (eV, NaN in empty cells)."""
+        out = np.empty(self.nr * self.nz)
+        self._check(self.L.pdp3g_temperature(self.h, sid, _p(out)), "temperature")
+        return out.reshape(self.nr, self.nz)
+
+    def density(self, sid):
+        """ParticlesDensity of species sid: [n_grid_r, n_grid_z]."""
+        out = np.empty(self.nr * self.nz)
+        self._check(self.L.pdp3g_density(self.h, sid, _p(out)), "density")
+        return out.reshape(self.nr, self.nz)
+
+    def probe_species(self, name, sid, kind, start_r, start_z, end_r=0, end_z=0):
+        """A per-species probe ("T" or "density") of species sid, in write
+        order."""
+        t = {"frame": 0, "col": 1, "row": 2, "dot": 3}[kind]
+        comp = {"T": PROBE_T, "density": PROBE_DENSITY}[name]
+        cap = max(1, (end_r - start_r) * max(end_z - start_z, 1)) if t == 0 else \
+            max(1, end_r - start_r, end_z - start_z)
+        out = np.empty(cap)
+        n = ctypes.c_int64()
+        self._check(self.L.pdp3g_probe_read_species(self.h, comp, sid, t, start_r, start_z,
+                                                    end_r, end_z, _p(out), cap, ctypes.byref(n)),
+                    "probe_read_species")
         return out[:n.value]
 
     def probe_particles(self, sid, start_r, start_z, end_r, end_z):

@@ -34,6 +34,7 @@ UNITS = {
     "noalloc.cu": [],
     "adjoint.cu": ["--prec-div=false", "--prec-sqrt=false"],
     "probe.cu": [],
+    "species_diag.cu": ["--fmad=false"],
 }
 HEADERS = ["pdp3g_internal.cuh", "particles_f32.cuh", "fields_body.cuh", "adjoint_particle.cuh"]
 

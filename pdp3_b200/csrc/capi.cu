@@ -48,6 +48,7 @@ struct pdp3g_ctx {
   double *d_rho0 = nullptr;
   double *d_scratch = nullptr;   // one grid (charge density)
   double *d_scratch2 = nullptr;  // one grid (per-species charge density)
+  double *d_temp_acc = nullptr;  // 5 grids: the temperature probe's sums
   double *d_partials = nullptr;  // per-block reduction partials
   double *d_red = nullptr;       // reduction results
   char *d_sort = nullptr;        // radix-sort scratch
@@ -328,6 +329,7 @@ void pdp3g_destroy(pdp3g_ctx *ctx) {
   cudaFree(ctx->d_rho0);
   cudaFree(ctx->d_scratch);
   cudaFree(ctx->d_scratch2);
+  cudaFree(ctx->d_temp_acc);
   cudaFree(ctx->d_partials);
   cudaFree(ctx->d_red);
   cudaFree(ctx->d_sort);
@@ -966,33 +968,80 @@ pdp3g_status pdp3g_charge_density(pdp3g_ctx *ctx, uint32_t mask, double *host_ou
   return PDP3G_OK;
 }
 
+// number of values of a probe region (0: outside the grid)
+static long long probe_count(const pdp3g_ctx *ctx, int type, int r0, int z0, int r1, int z1) {
+  const int nr = ctx->cfg.n_grid_r, nz = ctx->cfg.n_grid_z;
+  switch (type) {
+    case 0:
+      return (0 <= r0 && r0 < r1 && r1 <= nr && 0 <= z0 && z0 < z1 && z1 <= nz)
+                 ? (long long)(r1 - r0) * (z1 - z0) : 0;
+    case 1:
+      return (0 <= r0 && r0 < r1 && r1 <= nr && 0 <= z0 && z0 < nz) ? r1 - r0 : 0;
+    case 2:
+      return (0 <= r0 && r0 < nr && 0 <= z0 && z0 < z1 && z1 <= nz) ? z1 - z0 : 0;
+    case 3:
+      return (0 <= r0 && r0 < nr && 0 <= z0 && z0 < nz) ? 1 : 0;
+  }
+  return 0;
+}
+
+// gathers a probe region of the device grid src into host_out
+static pdp3g_status probe_to_host(pdp3g_ctx *ctx, const double *src, int type, int r0, int z0,
+                                  int r1, int z1, long long n, double *host_out, int64_t *count) {
+  launch_probe_gather(src, ctx->cfg.n_grid_z, type, r0, z0, r1, z1, n, ctx->d_scratch,
+                      ctx->stream);
+  ctx->launches++;
+  CK(cudaMemcpyAsync(host_out, ctx->d_scratch, sizeof(double) * (size_t)n, cudaMemcpyDeviceToHost,
+                     ctx->stream));
+  CK(cudaStreamSynchronize(ctx->stream));
+  if (count) *count = n;
+  return PDP3G_OK;
+}
+
+// TemperatureClassic::calc_t + normalize of species id into dst (device grid)
+static pdp3g_status temperature_into(pdp3g_ctx *ctx, int id, double *dst) {
+  const size_t ng = (size_t)ctx->cfg.n_grid_r * ctx->cfg.n_grid_z;
+  if (!ctx->d_temp_acc) CK(dalloc(ctx, &ctx->d_temp_acc, 5 * ng));
+  CK(cudaMemsetAsync(ctx->d_temp_acc, 0, sizeof(double) * 5 * ng, ctx->stream));
+  CK(cudaMemsetAsync(dst, 0, sizeof(double) * ng, ctx->stream));
+  const Species &sp = ctx->species[id];
+  if (sp.fp32)
+    launch_temperature_f32(ctx->g, sp.f32, ctx->d_temp_acc, ctx->stream);
+  else
+    launch_temperature_f64(ctx->g, sp.dev, ctx->d_temp_acc, ctx->stream);
+  launch_temperature_normalize(ctx->g, ctx->d_temp_acc, sp.mass_si, sp.charge_si, dst,
+                               ctx->stream);
+  ctx->launches += 2;
+  return PDP3G_OK;
+}
+
+// ParticlesDensity::reset + calc_density of species id into dst (device grid)
+static pdp3g_status density_into(pdp3g_ctx *ctx, int id, double *dst) {
+  const size_t ng = (size_t)ctx->cfg.n_grid_r * ctx->cfg.n_grid_z;
+  CK(cudaMemsetAsync(dst, 0, sizeof(double) * ng, ctx->stream));
+  const Species &sp = ctx->species[id];
+  if (sp.fp32)
+    launch_density_f32(ctx->g, sp.f32, sp.mass_si, dst, ctx->stream);
+  else
+    launch_density_f64(ctx->g, sp.dev, dst, ctx->stream);
+  ctx->launches++;
+  return PDP3G_OK;
+}
+
+// the per-species component comp of species id into ctx->d_scratch2
+static pdp3g_status species_diag_into(pdp3g_ctx *ctx, int32_t comp, int32_t id) {
+  if (comp == PDP3G_PROBE_T) return temperature_into(ctx, id, ctx->d_scratch2);
+  if (comp == PDP3G_PROBE_DENSITY) return density_into(ctx, id, ctx->d_scratch2);
+  return fail(ctx, PDP3G_INVALID_ARG, "unknown per-species component");
+}
+
 // ProbePlain::write's region (src/probePlain.cpp:80-170) of one component
 pdp3g_status pdp3g_probe_read(pdp3g_ctx *ctx, int32_t comp, int32_t type, int32_t r0, int32_t z0,
                               int32_t r1, int32_t z1, double *host_out, int64_t capacity,
                               int64_t *count) {
   if (!ctx || !host_out) return PDP3G_INVALID_ARG;
-  const int nr = ctx->cfg.n_grid_r, nz = ctx->cfg.n_grid_z;
-  long long n = 0;
-  bool ok = false;
-  switch (type) {
-    case 0:
-      ok = 0 <= r0 && r0 < r1 && r1 <= nr && 0 <= z0 && z0 < z1 && z1 <= nz;
-      n = (long long)(r1 - r0) * (z1 - z0);
-      break;
-    case 1:
-      ok = 0 <= r0 && r0 < r1 && r1 <= nr && 0 <= z0 && z0 < nz;
-      n = r1 - r0;
-      break;
-    case 2:
-      ok = 0 <= r0 && r0 < nr && 0 <= z0 && z0 < z1 && z1 <= nz;
-      n = z1 - z0;
-      break;
-    case 3:
-      ok = 0 <= r0 && r0 < nr && 0 <= z0 && z0 < nz;
-      n = 1;
-      break;
-  }
-  if (!ok) return fail(ctx, PDP3G_INVALID_ARG, "probe_read: region outside the grid");
+  const long long n = probe_count(ctx, type, r0, z0, r1, z1);
+  if (n == 0) return fail(ctx, PDP3G_INVALID_ARG, "probe_read: region outside the grid");
   if (capacity < n) return fail(ctx, PDP3G_INVALID_ARG, "probe_read: output too small");
   const bool rho_beam = comp == PDP3G_PROBE_RHO_BEAM;
   if (!rho_beam && (comp < 0 || comp >= PDP3G_NCOMP))
@@ -1010,13 +1059,50 @@ pdp3g_status pdp3g_probe_read(pdp3g_ctx *ctx, int32_t comp, int32_t type, int32_
     if (rs != PDP3G_OK) return rs;
     src = ctx->d_scratch2;
   }
-  launch_probe_gather(src, nz, type, r0, z0, r1, z1, n, ctx->d_scratch, ctx->stream);
-  ctx->launches++;
-  CK(cudaMemcpyAsync(host_out, ctx->d_scratch, sizeof(double) * (size_t)n, cudaMemcpyDeviceToHost,
+  return probe_to_host(ctx, src, type, r0, z0, r1, z1, n, host_out, count);
+}
+
+// dump_data's per-species probes: T (TemperatureClassic) or density
+// (ParticlesDensity) of species id
+pdp3g_status pdp3g_probe_read_species(pdp3g_ctx *ctx, int32_t comp, int32_t id, int32_t type,
+                                      int32_t r0, int32_t z0, int32_t r1, int32_t z1,
+                                      double *host_out, int64_t capacity, int64_t *count) {
+  if (!ctx || !host_out || id < 0 || id >= (int32_t)ctx->species.size())
+    return fail(ctx, PDP3G_INVALID_ARG, "probe_read_species: bad arguments");
+  if (comp != PDP3G_PROBE_T && comp != PDP3G_PROBE_DENSITY)
+    return fail(ctx, PDP3G_INVALID_ARG, "probe_read_species: unknown component");
+  const long long n = probe_count(ctx, type, r0, z0, r1, z1);
+  if (n == 0) return fail(ctx, PDP3G_INVALID_ARG, "probe_read_species: region outside the grid");
+  if (capacity < n) return fail(ctx, PDP3G_INVALID_ARG, "probe_read_species: output too small");
+  CK(cudaSetDevice(ctx->device));
+  pdp3g_status es = ensure_scratch(ctx);
+  if (es != PDP3G_OK) return es;
+  pdp3g_status ts = species_diag_into(ctx, comp, id);
+  if (ts != PDP3G_OK) return ts;
+  return probe_to_host(ctx, ctx->d_scratch2, type, r0, z0, r1, z1, n, host_out, count);
+}
+
+static pdp3g_status species_diag_to_host(pdp3g_ctx *ctx, int32_t comp, int32_t id,
+                                         double *host_out) {
+  if (!ctx || !host_out || id < 0 || id >= (int32_t)ctx->species.size()) return PDP3G_INVALID_ARG;
+  CK(cudaSetDevice(ctx->device));
+  pdp3g_status es = ensure_scratch(ctx);
+  if (es != PDP3G_OK) return es;
+  pdp3g_status ts = species_diag_into(ctx, comp, id);
+  if (ts != PDP3G_OK) return ts;
+  const size_t ng = (size_t)ctx->cfg.n_grid_r * ctx->cfg.n_grid_z;
+  CK(cudaMemcpyAsync(host_out, ctx->d_scratch2, sizeof(double) * ng, cudaMemcpyDeviceToHost,
                      ctx->stream));
   CK(cudaStreamSynchronize(ctx->stream));
-  if (count) *count = n;
   return PDP3G_OK;
+}
+
+pdp3g_status pdp3g_temperature(pdp3g_ctx *ctx, int32_t id, double *host_out) {
+  return species_diag_to_host(ctx, PDP3G_PROBE_T, id, host_out);
+}
+
+pdp3g_status pdp3g_density(pdp3g_ctx *ctx, int32_t id, double *host_out) {
+  return species_diag_to_host(ctx, PDP3G_PROBE_DENSITY, id, host_out);
 }
 
 // ProbePlain::mpwrite's selection (src/probePlain.cpp:172-224)

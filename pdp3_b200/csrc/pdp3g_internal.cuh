@@ -230,6 +230,15 @@ struct AdjSpeciesDev {
   double *lw;                          // adjoint of w (accumulated over steps)
 };
 
+// TemperatureClassic and ParticlesDensity (species_diag.cu)
+void launch_density_f64(const GridDev &g, const SpeciesDev &s, double *out, cudaStream_t st);
+void launch_density_f32(const GridDev &g, const SpeciesF32 &s, double mass, double *out,
+                        cudaStream_t st);
+void launch_temperature_f64(const GridDev &g, const SpeciesDev &s, double *acc, cudaStream_t st);
+void launch_temperature_f32(const GridDev &g, const SpeciesF32 &s, double *acc, cudaStream_t st);
+void launch_temperature_normalize(const GridDev &g, const double *acc, double mass, double charge,
+                                  double *t_out, cudaStream_t st);
+
 // probes (probe.cu)
 struct MpArrays {
   const double *src[5];  // r, z, v_r, v_phi, v_z of every slot

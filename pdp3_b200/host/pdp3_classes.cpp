@@ -467,8 +467,10 @@ static int probe_component(const char *c) {
   return -1;
 }
 
-void ProbePlain::write(const char *name, pdp3g_ctx *ctx) {
-  const int comp = probe_component(component);
+void ProbePlain::write(const char *name, pdp3g_ctx *ctx, int species_id) {
+  const bool is_t = strcmp(component, "T") == 0, is_density = strcmp(component, "density") == 0;
+  const bool per_species = is_t || is_density;
+  const int comp = is_t ? PDP3G_PROBE_T : is_density ? PDP3G_PROBE_DENSITY : probe_component(component);
   if (comp < 0) {
     std::cerr << "WARNING! probe for component ``" << component << "'' does not exist. Skipping"
               << std::endl;
@@ -480,9 +482,14 @@ void ProbePlain::write(const char *name, pdp3g_ctx *ctx) {
   if (type == 2) cap = end_z - start_z;
   std::vector<double> v((size_t)std::max<long long>(cap, 1));
   int64_t n = 0;
-  check(pdp3g_probe_read(ctx, comp, type, start_r, start_z, end_r, end_z, v.data(),
-                         (int64_t)v.size(), &n),
-        ctx, "probe_read");
+  if (per_species)
+    check(pdp3g_probe_read_species(ctx, comp, species_id, type, start_r, start_z, end_r, end_z,
+                                   v.data(), (int64_t)v.size(), &n),
+          ctx, "probe_read_species");
+  else
+    check(pdp3g_probe_read(ctx, comp, type, start_r, start_z, end_r, end_z, v.data(),
+                           (int64_t)v.size(), &n),
+          ctx, "probe_read");
   std::ofstream out_file(get_data_path(name), std::ios::app);
   for (int64_t i = 0; i < n; i++) out_file << v[(size_t)i] << " ";
 }
@@ -513,6 +520,10 @@ void dump_probes(std::vector<ProbePlain *> &probes, pdp3g_ctx *ctx, Time *time,
       snprintf(file_name, sizeof(file_name), "%d", w->step_number);
       for (size_t s = 0; s < species_names.size(); s++)
         if (species_names[s] == w->component) w->mpwrite(file_name, ctx, (int)s);
+    } else if (strcmp(w->component, "T") == 0 || strcmp(w->component, "density") == 0) {
+      // TemperatureClassic / ParticlesDensity of the species the probe names
+      for (size_t s = 0; s < species_names.size(); s++)
+        if (species_names[s] == w->specie) w->write(file_name, ctx, (int)s);
     } else {
       w->write(file_name, ctx);
     }

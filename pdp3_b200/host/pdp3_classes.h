@@ -217,7 +217,8 @@ class ProbePlain {
              int c_start_z, int c_end_r, int c_end_z, bool c_compress, int c_compress_level,
              int c_schedule, const char *c_specie = "none");
   std::string get_data_path(const char *name) const;
-  void write(const char *name, pdp3g_ctx *ctx);                  // types 0-3
+  // types 0-3; species_id: the species of a per-species component (T, density)
+  void write(const char *name, pdp3g_ctx *ctx, int species_id = -1);
   void mpwrite(const char *name, pdp3g_ctx *ctx, int species_id);  // type 4
   const std::string &result_path() const { return path_result_; }
 

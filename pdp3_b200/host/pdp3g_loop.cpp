@@ -11,10 +11,13 @@
 // and optionally beam_charge beam_mass beam_number_macro beam_length
 // beam_radius beam_density beam_velocity beam_number_bunches beam_distance.
 // Species arrays are raw float64 files species<s>_{r,z,vr,vphi,vz,w}.f64.
-// Optional <case_dir>/probes.txt: one ProbePlain per line,
-//   <type> <component> <start_r> <start_z> <end_r> <end_z> <schedule>
+// Optional <case_dir>/names.txt: the species' names, one per line (default
+// species<s>).  Optional <case_dir>/probes.txt: one ProbePlain per line,
+//   <type> <component> <start_r> <start_z> <end_r> <end_z> <schedule> [<specie>]
 // (type 0 frame, 1 col, 2 row, 3 dot, 4 mpframe; an mpframe's component
-// names a species: species<s> or Beam#<k>), written under <out_dir>/probes
+// names a species or Beam#<k>; components T and density take the species as
+// <specie>),
+// written under <out_dir>/probes
 // by dump_data's schedule test after every step (key dump_frames_per_file,
 // default 1).  The loop writes E_r.. J_z (raw float64
 // [n_grid_r*n_grid_z]) and every species' r, z, vr, vphi, vz, alive to
@@ -97,15 +100,22 @@ int main(int argc, char **argv) {
     std::vector<std::unique_ptr<Particles>> owned;
     const int nsp = (int)get("n_species");
     std::vector<std::string> species_names;
+    {
+      std::ifstream nf(cdir + "/names.txt");
+      std::string nm;
+      while ((int)species_names.size() < nsp && nf >> nm) species_names.push_back(nm);
+      for (int s = (int)species_names.size(); s < nsp; s++)
+        species_names.push_back("species" + std::to_string(s));
+    }
     for (int s = 0; s < nsp; s++) {
       const std::string p = "species" + std::to_string(s) + "_";
-      species_names.push_back("species" + std::to_string(s));
       const size_t n = (size_t)get(p + "n");
       auto r = read_f64(cdir + "/" + p + "r.f64", n), z = read_f64(cdir + "/" + p + "z.f64", n);
       auto vr = read_f64(cdir + "/" + p + "vr.f64", n);
       auto vp = read_f64(cdir + "/" + p + "vphi.f64", n);
       auto vz = read_f64(cdir + "/" + p + "vz.f64", n), w = read_f64(cdir + "/" + p + "w.f64", n);
-      owned.emplace_back(new Particles(p.c_str(), get(p + "charge"), get(p + "mass"), (int)n, &geom));
+      owned.emplace_back(new Particles(species_names[s].c_str(), get(p + "charge"), get(p + "mass"),
+                                       (int)n, &geom));
       Particles *prt = owned.back().get();
       for (size_t i = 0; i < n; i++) {
         prt->pos[i][0] = r[i];
@@ -149,11 +159,15 @@ int main(int argc, char **argv) {
     std::vector<ProbePlain *> probes;
     {
       std::ifstream pf(cdir + "/probes.txt");
-      int type, r0, z0, r1, z1, sched;
-      std::string comp;
-      while (pf >> type >> comp >> r0 >> z0 >> r1 >> z1 >> sched) {
+      std::string line;
+      while (std::getline(pf, line)) {
+        std::istringstream ls(line);
+        int type, r0, z0, r1, z1, sched;
+        std::string comp, specie = "none";
+        if (!(ls >> type >> comp >> r0 >> z0 >> r1 >> z1 >> sched)) continue;
+        ls >> specie;
         probe_store.emplace_back(new ProbePlain((odir + "/probes").c_str(), comp.c_str(), type, r0,
-                                                z0, r1, z1, false, 0, sched));
+                                                z0, r1, z1, false, 0, sched, specie.c_str()));
         probes.push_back(probe_store.back().get());
       }
     }

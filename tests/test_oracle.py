@@ -14,6 +14,7 @@ import pytest
 from helpers import (GOLDEN, GRIDS, SMOKE, golden_match, oracle_from_workload,
                      recover_weights, ref_from_workload, seed_fields)
 from oracle import refsim
+from oracle.diagnostics import particles_density, temperature_classic
 from oracle.oracle import OracleSim, random_reverse
 from pdp3_b200 import workloads as W
 
@@ -48,6 +49,29 @@ def _run_to_frame(sim, frame_idx, schedule=5):
             frame += 1
 
 
+def golden_temperature_ok(sim):
+    """The golden T/<specie> frames (TemperatureClassic of the species after
+    step 21) against temperature_classic of sim's species: NaN (empty) cells
+    at the same places, the rest at the golden files' 6 digits."""
+    g = np.load(GOLDEN)
+    for idx, (name, c, m, *_rest) in enumerate(SMOKE["species"]):
+        s = sim.species(idx)
+        t = temperature_classic(s["r"], s["z"], s["vr"], s["vphi"], s["vz"],
+                                SMOKE["r_size"] / (SMOKE["n_grid_r"] - 1),
+                                SMOKE["z_size"] / (SMOKE["n_grid_z"] - 1),
+                                SMOKE["n_grid_r"], SMOKE["n_grid_z"], m * 9.1e-31, c * 1.6e-19)
+        r0, z0, r1, z1 = g["T_%s__box" % name]
+        gold = g["T_" + name]
+        got = t[r0:r1, z0:z1]
+        assert np.array_equal(np.isnan(got), np.isnan(gold)), name
+        fin = ~np.isnan(gold)
+        ok = golden_match(got[fin], gold[fin])
+        assert ok.all(), (name, int((~ok).sum()))
+        assert fin.sum() > 300
+        if isinstance(sim, refsim.RefSim):  # the upstream class itself
+            assert np.array_equal(sim.temperature(idx), t, equal_nan=True), name
+
+
 @needs_ref
 def test_reference_build_reproduces_golden_smoke():
     g = np.load(GOLDEN)
@@ -65,6 +89,7 @@ def test_reference_build_reproduces_golden_smoke():
     ok = golden_match(ref.field("rho_bunch")[r0:r1, z0:z1], g["rho_beam"])
     assert ok.all()
     assert (g["rho_beam"] != 0).sum() > 100
+    golden_temperature_ok(ref)
 
 
 @needs_ref
@@ -92,6 +117,45 @@ def test_oracle_reproduces_golden_smoke():
     r0, z0, r1, z1 = g["rho_beam__box"]
     ok = golden_match(orc.charge_density(mask=1 << 2)[r0:r1, z0:z1], g["rho_beam"])
     assert ok.all()
+    golden_temperature_ok(orc)
+
+
+@needs_ref
+def test_diagnostics_restatement_equals_reference():
+    """temperature_classic and particles_density equal the upstream
+    TemperatureClassic and ParticlesDensity bit for bit (same slot order of
+    the sums) on a thermal plasma after 20 steps, absorbing layers included,
+    and on particles placed in all three radial branches of the density."""
+    wl = W.thermal_config(steps=20)
+    ref = ref_from_workload(wl)
+    for _ in range(20):
+        ref.step()
+    for idx, sp_init in enumerate(wl.species):
+        s = ref.species(idx)
+        t = temperature_classic(s["r"], s["z"], s["vr"], s["vphi"], s["vz"], wl.dr, wl.dz,
+                                wl.n_grid_r, wl.n_grid_z, sp_init.mass_me * 9.1e-31,
+                                sp_init.charge_e * 1.6e-19)
+        assert np.array_equal(ref.temperature(idx), t, equal_nan=True), idx
+        assert (~np.isnan(t)).sum() > 1000
+        d = particles_density(s["r"], s["z"], s["m"], wl.dr, wl.dz, wl.n_grid_r, wl.n_grid_z)
+        rd = ref.density(idx)
+        assert np.array_equal(rd, d), (idx, float(np.abs(rd - d).max()))
+        assert (d > 0).sum() > 1000
+    # the axis branches: r <= dr/2, dr/2 < r <= dr, r > dr, r == dr exactly
+    rng = np.random.default_rng(3)
+    n = 4000
+    r = np.concatenate([rng.uniform(1e-9, 0.5, n), rng.uniform(0.5, 1.0, n),
+                        rng.uniform(1.0, 6.0, n), [1.0, 0.5]]) * wl.dr
+    z = rng.uniform(0.01, 20.0, r.size) * wl.dz
+    w = rng.uniform(0.5, 2.0, r.size)
+    ref2 = refsim.RefSim(wl.r_size, wl.z_size, wl.n_grid_r, wl.n_grid_z, wl.dt)
+    ref2.add_species("probe", -1.0, 1.0, r, z, np.zeros_like(r), np.zeros_like(r),
+                     np.zeros_like(r), w)
+    s = ref2.species(0)
+    d = particles_density(s["r"], s["z"], s["m"], wl.dr, wl.dz, wl.n_grid_r, wl.n_grid_z)
+    assert np.array_equal(ref2.density(0), d)
+    ref2.close()
+    ref.close()
 
 
 def _bitwise(ref, orc, n_species):
