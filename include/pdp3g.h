@@ -123,6 +123,20 @@ pdp3g_status pdp3g_add_species_device(pdp3g_ctx *ctx, double charge_e, double ma
                                       int64_t n, const double *r, const double *z,
                                       const double *vr, const double *vphi, const double *vz,
                                       const double *w, int32_t *id);
+/* LoadInitParam::init_particles for one species (src/loadInitParam.cpp:
+   157-164): Particles(name, charge_e, mass_me, n, geom),
+   load_cylindrical_spatial_distribution(left_density, right_density,
+   left_plasma_boundary) (src/particles.cpp:278-331) and
+   velocity_distribution(temperature) (src/particles.cpp:228-276, TESTMODE
+   random_reverse sequences, Maxwell-Juttner sampler) generated on the device.
+   Positions and weights equal the upstream's bit for bit; velocities agree to
+   about 1e-13 relative (device log/exp/pow, sampler tables computed from
+   their definition).  n < 2^30.  PDP3G_TIMEOUT if the sampler's rejection
+   loop exceeds 100000 draws for a particle. */
+pdp3g_status pdp3g_add_species_upstream(pdp3g_ctx *ctx, double charge_e, double mass_me,
+                                        int64_t n, double left_density, double right_density,
+                                        double left_plasma_boundary, double temperature,
+                                        int32_t *id);
 
 /* Bunch(name, charge, mass, n, geom, duration, radius, density, velocity,
    bunch_number, hole_duration), src/bunch.cpp:6-80 (TESTMODE radial

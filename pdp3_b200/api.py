@@ -120,6 +120,8 @@ EXPORTS = [
                                                           ctypes.c_double, _VP, _VP]),
     ("pdp3g_probe_read", _I32, [_VP] + [_I32] * 6 + [_D, ctypes.c_int64,
                                                       ctypes.POINTER(ctypes.c_int64)]),
+    ("pdp3g_add_species_upstream", _I32, [_VP, ctypes.c_double, ctypes.c_double, ctypes.c_int64]
+     + [ctypes.c_double] * 4 + [ctypes.POINTER(_I32)]),
     ("pdp3g_probe_read_species", _I32, [_VP] + [_I32] * 7 + [_D, ctypes.c_int64,
                                                               ctypes.POINTER(ctypes.c_int64)]),
     ("pdp3g_temperature", _I32, [_VP, _I32, _D]),
@@ -209,6 +211,18 @@ class Simulation:
         self._check(self.L.pdp3g_add_species_device(self.h, float(charge_e), float(mass_me), n,
                                                     *[a.data_ptr() for a in arrs],
                                                     ctypes.byref(sid)), "add_species_device")
+        return sid.value
+
+    def add_species_upstream(self, charge_e, mass_me, n, left_density, right_density,
+                             temperature, left_plasma_boundary=0.0):
+        """The upstream's own initial state of a plasma species (cylindrical
+        load with a linear density ramp, Maxwell-Juttner velocities, TESTMODE
+        sequences) generated on the device."""
+        sid = _I32()
+        self._check(self.L.pdp3g_add_species_upstream(
+            self.h, float(charge_e), float(mass_me), int(n), float(left_density),
+            float(right_density), float(left_plasma_boundary), float(temperature),
+            ctypes.byref(sid)), "add_species_upstream")
         return sid.value
 
     def add_bunch(self, charge_e, mass_me, n, duration, radius, density, velocity,

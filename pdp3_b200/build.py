@@ -35,8 +35,10 @@ UNITS = {
     "adjoint.cu": ["--prec-div=false", "--prec-sqrt=false"],
     "probe.cu": [],
     "species_diag.cu": ["--fmad=false"],
+    "init.cu": ["--fmad=false"],
 }
-HEADERS = ["pdp3g_internal.cuh", "particles_f32.cuh", "fields_body.cuh", "adjoint_particle.cuh"]
+HEADERS = ["pdp3g_internal.cuh", "particles_f32.cuh", "fields_body.cuh", "adjoint_particle.cuh",
+           "mj_tables.h"]
 
 
 def nvcc():

@@ -532,6 +532,58 @@ pdp3g_status pdp3g_add_species_device(pdp3g_ctx *ctx, double charge_e, double ma
   return PDP3G_OK;
 }
 
+// LoadInitParam::init_particles for one species (src/loadInitParam.cpp:
+// 157-164): the upstream's own initial state generated on the device
+// (init.cu), then added as pdp3g_add_species_device adds device arrays.
+pdp3g_status pdp3g_add_species_upstream(pdp3g_ctx *ctx, double charge_e, double mass_me,
+                                        int64_t n, double left_density, double right_density,
+                                        double left_plasma_boundary, double temperature,
+                                        int32_t *id) {
+  if (!ctx || n <= 0) return fail(ctx, PDP3G_INVALID_ARG, "add_species_upstream: n <= 0");
+  // random_reverse takes (int) of npoints + i: the upstream's sequences are
+  // defined for 2 n < 2^31
+  if (n >= ((int64_t)1 << 30))
+    return fail(ctx, PDP3G_INVALID_ARG, "add_species_upstream: n must be below 2^30");
+  if (!(temperature >= 0))
+    return fail(ctx, PDP3G_INVALID_ARG, "add_species_upstream: temperature must be >= 0");
+  CK(cudaSetDevice(ctx->device));
+  const size_t nn = (size_t)n;
+  double *buf = nullptr, *inv_pow = nullptr;
+  unsigned *err = nullptr;
+  std::vector<double> tab((size_t)init_inv_pow_count());
+  init_inv_pow_table(tab.data());
+  cudaStream_t st = ctx->stream;
+  pdp3g_status rs = PDP3G_OK;
+  cudaError_t e = cudaMalloc((void **)&buf, sizeof(double) * (7 * nn + 1));
+  if (e == cudaSuccess) e = cudaMalloc((void **)&inv_pow, sizeof(double) * tab.size());
+  if (e == cudaSuccess) e = cudaMalloc((void **)&err, sizeof(unsigned));
+  if (e == cudaSuccess)
+    e = cudaMemcpyAsync(inv_pow, tab.data(), sizeof(double) * tab.size(), cudaMemcpyHostToDevice, st);
+  if (e == cudaSuccess) e = cudaMemsetAsync(err, 0, sizeof(unsigned), st);
+  unsigned herr = 0;
+  if (e == cudaSuccess) {
+    double *r = buf, *z = buf + nn, *vr = buf + 2 * nn, *vp = buf + 3 * nn, *vz = buf + 4 * nn;
+    double *w = buf + 5 * nn, *vol = buf + 6 * nn, *sum = buf + 7 * nn;
+    launch_init_species((unsigned)n, ctx->cfg.r_size, ctx->cfg.z_size, ctx->dr, ctx->dz,
+                        left_density, right_density, left_plasma_boundary, temperature,
+                        mass_me * EL_MASS, inv_pow, r, z, vr, vp, vz, w, vol, sum, err, st);
+    ctx->launches += 4;
+    e = cudaGetLastError();
+    if (e == cudaSuccess) e = cudaMemcpyAsync(&herr, err, sizeof(unsigned), cudaMemcpyDeviceToHost, st);
+    if (e == cudaSuccess) e = cudaStreamSynchronize(st);
+    if (e == cudaSuccess && herr)
+      rs = fail(ctx, PDP3G_TIMEOUT, "add_species_upstream: velocity sampler did not accept");
+    if (e == cudaSuccess && rs == PDP3G_OK)
+      rs = pdp3g_add_species_device(ctx, charge_e, mass_me, n, r, z, vr, vp, vz, w, id);
+    cudaStreamSynchronize(st);  // the copies out of buf have finished
+  }
+  cudaFree(buf);
+  cudaFree(inv_pow);
+  cudaFree(err);
+  if (e != cudaSuccess) return fail(ctx, PDP3G_CUDA_ERROR, cudaGetErrorString(e));
+  return rs;
+}
+
 pdp3g_status pdp3g_add_bunch(pdp3g_ctx *ctx, double charge_e, double mass_me, int64_t n,
                              double duration, double radius, double density, double velocity,
                              int32_t bunch_number, double hole_duration, int32_t *id) {

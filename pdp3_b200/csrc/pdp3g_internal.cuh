@@ -230,6 +230,15 @@ struct AdjSpeciesDev {
   double *lw;                          // adjoint of w (accumulated over steps)
 };
 
+// upstream initial state (init.cu)
+void launch_init_species(unsigned n, double r_size, double z_size, double dr, double dz,
+                         double n1, double n2, double left, double temperature, double mass,
+                         const double *inv_pow, double *r, double *z, double *vr, double *vphi,
+                         double *vz, double *w, double *scratch_vol, double *d_sum, unsigned *err,
+                         cudaStream_t st);
+void init_inv_pow_table(double *host);
+int init_inv_pow_count();
+
 // TemperatureClassic and ParticlesDensity (species_diag.cu)
 void launch_density_f64(const GridDev &g, const SpeciesDev &s, double *out, cudaStream_t st);
 void launch_density_f32(const GridDev &g, const SpeciesF32 &s, double mass, double *out,

@@ -10,6 +10,7 @@
 #include <fstream>
 #include <iostream>
 #include <map>
+#include <stdexcept>
 #include <memory>
 
 namespace pdp3gpu {
@@ -268,7 +269,33 @@ Particles::~Particles() {
   delete[] vel;
 }
 
+void Particles::load_cylindrical_spatial_distribution(double n1, double n2,
+                                                      double left_plasma_boundary) {
+  spatial_set_ = true;
+  init_n1_ = n1;
+  init_n2_ = n2;
+  init_left_ = left_plasma_boundary;
+}
+
+void Particles::velocity_distribution(double tempr_ev) {
+  velocity_set_ = true;
+  init_tempr_ = tempr_ev;
+}
+
 void Particles::upload(pdp3g_ctx *ctx) {
+  if (spatial_set_ || velocity_set_) {
+    if (!(spatial_set_ && velocity_set_))
+      throw std::runtime_error(std::string(name) +
+                               ": load_cylindrical_spatial_distribution and "
+                               "velocity_distribution are generated together");
+    int32_t sid = -1;
+    check(pdp3g_add_species_upstream(ctx, charge / EL_CHARGE, mass / EL_MASS, number, init_n1_,
+                                     init_n2_, init_left_, init_tempr_, &sid),
+          ctx, "pdp3g_add_species_upstream");
+    id = sid;
+    download();
+    return;
+  }
   std::vector<double> r(number), z(number), vr(number), vp(number), vz(number), w(number);
   std::vector<uint8_t> alive(number);
   bool all_alive = true;

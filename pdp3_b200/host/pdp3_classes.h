@@ -169,11 +169,18 @@ class Particles {
   Particles(const char *p_name, double p_charge, double p_mass, int p_number, Geometry *geom);
   virtual ~Particles();
   void charge_weighting(ChargeDensity *ro1);  // src/particles.cpp:101-226
+  // src/particles.cpp:278-331 and :228-276: recorded here and generated on
+  // the device when the species is uploaded (pdp3g_add_species_upstream);
+  // pos, vel, charge_array and mass_array are filled from the device then.
+  void load_cylindrical_spatial_distribution(double n1, double n2, double left_plasma_boundary);
+  void velocity_distribution(double tempr_ev);
   void download();                             // refresh pos/vel/is_alive
   virtual void upload(pdp3g_ctx *ctx);
 
  protected:
   std::vector<double> pos_store_, vel_store_;
+  bool spatial_set_ = false, velocity_set_ = false;
+  double init_n1_ = 0, init_n2_ = 0, init_left_ = 0, init_tempr_ = 0;
 };
 
 // Bunch, include/bunch.h:4-36

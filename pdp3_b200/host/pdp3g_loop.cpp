@@ -10,7 +10,10 @@
 // n_species, per species s: species<s>_charge species<s>_mass species<s>_n,
 // and optionally beam_charge beam_mass beam_number_macro beam_length
 // beam_radius beam_density beam_velocity beam_number_bunches beam_distance.
-// Species arrays are raw float64 files species<s>_{r,z,vr,vphi,vz,w}.f64.
+// Species arrays are raw float64 files species<s>_{r,z,vr,vphi,vz,w}.f64, or,
+// with keys species<s>_left_density species<s>_right_density
+// species<s>_temperature, the upstream's own initial state (init_particles:
+// load_cylindrical_spatial_distribution + velocity_distribution).
 // Optional <case_dir>/names.txt: the species' names, one per line (default
 // species<s>).  Optional <case_dir>/probes.txt: one ProbePlain per line,
 //   <type> <component> <start_r> <start_z> <end_r> <end_z> <schedule> [<specie>]
@@ -110,6 +113,17 @@ int main(int argc, char **argv) {
     for (int s = 0; s < nsp; s++) {
       const std::string p = "species" + std::to_string(s) + "_";
       const size_t n = (size_t)get(p + "n");
+      if (kv.count(p + "temperature")) {
+        // LoadInitParam::init_particles (src/loadInitParam.cpp:157-164)
+        owned.emplace_back(new Particles(species_names[s].c_str(), get(p + "charge"),
+                                         get(p + "mass"), (int)n, &geom));
+        Particles *prt = owned.back().get();
+        prt->load_cylindrical_spatial_distribution(get(p + "left_density"),
+                                                   get(p + "right_density"), 0);
+        prt->velocity_distribution(get(p + "temperature"));
+        p_list.part_list.push_back(prt);
+        continue;
+      }
       auto r = read_f64(cdir + "/" + p + "r.f64", n), z = read_f64(cdir + "/" + p + "z.f64", n);
       auto vr = read_f64(cdir + "/" + p + "vr.f64", n);
       auto vp = read_f64(cdir + "/" + p + "vphi.f64", n);
