@@ -241,6 +241,17 @@ pdp3g_status pdp3g_temperature(pdp3g_ctx *ctx, int32_t id, double *host_out);
 /* ParticlesDensity::calc_density of species id: [n_grid_r][n_grid_z] host
    grid (mass_array / EL_MASS per m^3 over the four nodes of each particle). */
 pdp3g_status pdp3g_density(pdp3g_ctx *ctx, int32_t id, double *host_out);
+
+/* PoissonDirichlet::poisson_solve(EField*, ChargeDensity*)
+   (src/poissonDirichlet.cpp:23-98): phi from rho by a sine transform along
+   z, a radial sweep per mode and the inverse transform, then E_r (rows
+   i < n_grid_r-1) and E_z (columns k < n_grid_z-1) from phi; the other E
+   values are kept.  host_rho: [n_grid_r][n_grid_z] charge density, or NULL
+   for the charge weighting of every species.  host_fi (optional) receives
+   phi.  Needs 2 n_grid_z + 2 a power of two <= 8192 (the upstream's radix-2
+   transform has the same restriction).  Not bit-identical: the transform's
+   twiddle factors come from the device sin/cos (about 1e-13 relative). */
+pdp3g_status pdp3g_poisson_solve(pdp3g_ctx *ctx, const double *host_rho, double *host_fi);
 pdp3g_status pdp3g_probe_particles(pdp3g_ctx *ctx, int32_t id, int32_t start_r, int32_t start_z,
                                    int32_t end_r, int32_t end_z, double *r, double *z, double *vr,
                                    double *vphi, double *vz, int64_t capacity, int64_t *count);

@@ -36,6 +36,7 @@
 #include "particlesList.h"
 #include "bunch.h"
 #include "particlesDensity.h"
+#include "poissonDirichlet.h"
 #include "temperatureClassic.h"
 
 namespace {
@@ -369,6 +370,22 @@ int ref_density(void *h, int idx, double *out) {
   s->density->calc_density(p);
   const int nr = s->geom->n_grid_r, nz = s->geom->n_grid_z;
   copy_rows(s->density->density, nr, nz, nz, out);
+  return 0;
+}
+
+// PoissonDirichlet::poisson_solve(efield, rho) with rho given
+// ([n_grid_r][n_grid_z]); returns phi, E_r and E_z after the solve.
+int ref_poisson_dirichlet(void *h, const double *rho, double *fi, double *er, double *ez) {
+  RefSim *s = (RefSim *)h;
+  const int nr = s->geom->n_grid_r, nz = s->geom->n_grid_z;
+  double **r = s->rho_new->get_rho();
+  for (int i = 0; i < nr; i++)
+    for (int k = 0; k < nz; k++) r[i][k] = rho[(size_t)i * nz + k];
+  PoissonDirichlet solver(s->geom);
+  solver.poisson_solve(s->efield, s->rho_new);
+  copy_rows(s->efield->fi, nr, nz, nz, fi);
+  copy_rows(s->efield->field_r, nr, nz, nz, er);
+  copy_rows(s->efield->field_z, nr, nz, nz, ez);
   return 0;
 }
 

@@ -75,6 +75,8 @@ def load(pusher="boris"):
     for f in (L.ref_temperature, L.ref_density):
         f.restype = ctypes.c_int
         f.argtypes = [ctypes.c_void_p, ctypes.c_int, _D]
+    L.ref_poisson_dirichlet.restype = ctypes.c_int
+    L.ref_poisson_dirichlet.argtypes = [ctypes.c_void_p] + [_D] * 4
     L.ref_sigma.restype = ctypes.c_double
     L.ref_sigma.argtypes = [ctypes.c_void_p, ctypes.c_int, ctypes.c_int]
     L.ref_destroy.restype = None
@@ -170,6 +172,13 @@ class RefSim:
         rc = self.L.ref_density(self.h, idx, _p(out))
         assert rc == 0, rc
         return out.reshape(self.nr, self.nz)
+
+    def poisson_dirichlet(self, rho):
+        """PoissonDirichlet::poisson_solve on rho: (phi, E_r, E_z)."""
+        rho = np.ascontiguousarray(rho, dtype=np.float64).reshape(-1)
+        outs = [np.zeros(self.nr * self.nz) for _ in range(3)]
+        assert self.L.ref_poisson_dirichlet(self.h, _p(rho), *[_p(o) for o in outs]) == 0
+        return tuple(o.reshape(self.nr, self.nz) for o in outs)
 
     def close(self):
         if self.h:

@@ -126,6 +126,7 @@ EXPORTS = [
                                                               ctypes.POINTER(ctypes.c_int64)]),
     ("pdp3g_temperature", _I32, [_VP, _I32, _D]),
     ("pdp3g_density", _I32, [_VP, _I32, _D]),
+    ("pdp3g_poisson_solve", _I32, [_VP, _D, _D]),
     ("pdp3g_probe_particles", _I32, [_VP] + [_I32] * 5 + [_D] * 5 +
      [ctypes.c_int64, ctypes.POINTER(ctypes.c_int64)]),
     ("pdp3g_adjoint_create", _I32, [_VP] + [_I32] * 6 + [ctypes.POINTER(_VP)]),
@@ -299,6 +300,19 @@ class Simulation:
         out = np.empty(self.nr * self.nz)
         self._check(self.L.pdp3g_temperature(self.h, sid, _p(out)), "temperature")
         return out.reshape(self.nr, self.nz)
+
+    def poisson_solve(self, rho=None):
+        """PoissonDirichlet::poisson_solve: writes E_r and E_z from rho (a
+        [n_grid_r, n_grid_z] array, or None for the charge density of every
+        species) and returns phi."""
+        fi = np.empty(self.nr * self.nz)
+        rp = None
+        if rho is not None:
+            rho = np.ascontiguousarray(rho, dtype=np.float64).reshape(-1)
+            assert rho.size == self.nr * self.nz
+            rp = _p(rho)
+        self._check(self.L.pdp3g_poisson_solve(self.h, rp, _p(fi)), "poisson_solve")
+        return fi.reshape(self.nr, self.nz)
 
     def density(self, sid):
         """ParticlesDensity of species sid: [n_grid_r, n_grid_z]."""

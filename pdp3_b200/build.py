@@ -36,6 +36,7 @@ UNITS = {
     "probe.cu": [],
     "species_diag.cu": ["--fmad=false"],
     "init.cu": ["--fmad=false"],
+    "poisson.cu": ["--fmad=false"],
 }
 HEADERS = ["pdp3g_internal.cuh", "particles_f32.cuh", "fields_body.cuh", "adjoint_particle.cuh",
            "mj_tables.h"]

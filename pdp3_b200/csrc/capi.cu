@@ -49,6 +49,7 @@ struct pdp3g_ctx {
   double *d_scratch = nullptr;   // one grid (charge density)
   double *d_scratch2 = nullptr;  // one grid (per-species charge density)
   double *d_temp_acc = nullptr;  // 5 grids: the temperature probe's sums
+  double *d_poisson = nullptr;   // the Poisson solve's t, phi, alpha, beta grids + modes
   double *d_partials = nullptr;  // per-block reduction partials
   double *d_red = nullptr;       // reduction results
   char *d_sort = nullptr;        // radix-sort scratch
@@ -330,6 +331,7 @@ void pdp3g_destroy(pdp3g_ctx *ctx) {
   cudaFree(ctx->d_scratch);
   cudaFree(ctx->d_scratch2);
   cudaFree(ctx->d_temp_acc);
+  cudaFree(ctx->d_poisson);
   cudaFree(ctx->d_partials);
   cudaFree(ctx->d_red);
   cudaFree(ctx->d_sort);
@@ -1155,6 +1157,54 @@ pdp3g_status pdp3g_temperature(pdp3g_ctx *ctx, int32_t id, double *host_out) {
 
 pdp3g_status pdp3g_density(pdp3g_ctx *ctx, int32_t id, double *host_out) {
   return species_diag_to_host(ctx, PDP3G_PROBE_DENSITY, id, host_out);
+}
+
+// PoissonDirichlet::poisson_solve (src/poissonDirichlet.cpp:23-98): phi from
+// rho (the given host grid, or the charge density of every species), then
+// E_r and E_z from phi (poisson.cu).  phi persists in the context with its
+// last row 0 (EField::set_fi_on_z).
+pdp3g_status pdp3g_poisson_solve(pdp3g_ctx *ctx, const double *host_rho, double *host_fi) {
+  if (!ctx) return PDP3G_INVALID_ARG;
+  const int nr = ctx->cfg.n_grid_r, nz = ctx->cfg.n_grid_z;
+  if (poisson_check(nz) != 0)
+    return fail(ctx, PDP3G_INVALID_ARG,
+                "poisson_solve: 2 n_grid_z + 2 must be a power of two <= 8192 (the radix-2 sine "
+                "transform)");
+  CK(cudaSetDevice(ctx->device));
+  pdp3g_status es = ensure_scratch(ctx);
+  if (es != PDP3G_OK) return es;
+  const size_t ng = (size_t)nr * nz;
+  cudaStream_t st = ctx->stream;
+  if (!ctx->d_poisson) {
+    // t, fi, alpha, beta grids and the nz mode constants
+    CK(dalloc(ctx, &ctx->d_poisson, 4 * ng + (size_t)nz));
+    CK(cudaMemsetAsync(ctx->d_poisson, 0, sizeof(double) * (4 * ng + (size_t)nz), st));
+    // b = 2 (1 - dr^2/dz^2 (cos(PI (k+1) / (n_grid_z+1)) - 1)) with the host libm
+    std::vector<double> b(nz);
+    const double dr = ctx->dr, dz = ctx->dz;
+    for (int k = 0; k < nz; k++)
+      b[k] = 2. * (1. - dr * dr / (dz * dz) * (std::cos(PI * (k + 1) / (nz + 1)) - 1));
+    CK(cudaMemcpyAsync(ctx->d_poisson + 4 * ng, b.data(), sizeof(double) * nz,
+                       cudaMemcpyHostToDevice, st));
+    CK(cudaStreamSynchronize(st));
+  }
+  double *t = ctx->d_poisson, *fi = t + ng, *alpha = t + 2 * ng, *beta = t + 3 * ng;
+  const double *b_mode = t + 4 * ng;
+  if (host_rho) {
+    CK(cudaMemcpyAsync(ctx->d_scratch2, host_rho, sizeof(double) * ng, cudaMemcpyHostToDevice, st));
+  } else {
+    pdp3g_status rs = rho_into(ctx, 0xFFFFFFFFu, ctx->d_scratch2);
+    if (rs != PDP3G_OK) return rs;
+  }
+  CK(launch_poisson(ctx->g, ctx->d_scratch2, t, fi, alpha, beta, b_mode,
+                    comp_ptr(ctx, PDP3G_E_R), comp_ptr(ctx, PDP3G_E_Z), st));
+  ctx->launches += 4;
+  refresh_mirror(ctx, PDP3G_E_R);
+  refresh_mirror(ctx, PDP3G_E_Z);
+  if (host_fi) CK(cudaMemcpyAsync(host_fi, fi, sizeof(double) * ng, cudaMemcpyDeviceToHost, st));
+  CK(cudaGetLastError());
+  CK(cudaStreamSynchronize(st));
+  return PDP3G_OK;
 }
 
 // ProbePlain::mpwrite's selection (src/probePlain.cpp:172-224)

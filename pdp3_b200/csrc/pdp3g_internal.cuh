@@ -230,6 +230,12 @@ struct AdjSpeciesDev {
   double *lw;                          // adjoint of w (accumulated over steps)
 };
 
+// PoissonDirichlet (poisson.cu)
+int poisson_check(int nz);
+cudaError_t launch_poisson(const GridDev &g, const double *rho, double *t, double *fi,
+                           double *alpha, double *beta, const double *b_mode, double *er,
+                           double *ez, cudaStream_t st);
+
 // upstream initial state (init.cu)
 void launch_init_species(unsigned n, double r_size, double z_size, double dr, double dz,
                          double n1, double n2, double left, double temperature, double mass,

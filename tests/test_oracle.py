@@ -15,6 +15,7 @@ from helpers import (GOLDEN, GRIDS, SMOKE, golden_match, oracle_from_workload,
                      recover_weights, ref_from_workload, seed_fields)
 from oracle import refsim
 from oracle.diagnostics import particles_density, temperature_classic
+from oracle.poisson import poisson_dirichlet
 from oracle.oracle import OracleSim, random_reverse
 from pdp3_b200 import workloads as W
 
@@ -155,6 +156,34 @@ def test_diagnostics_restatement_equals_reference():
     d = particles_density(s["r"], s["z"], s["m"], wl.dr, wl.dz, wl.n_grid_r, wl.n_grid_z)
     assert np.array_equal(ref2.density(0), d)
     ref2.close()
+    ref.close()
+
+
+@needs_ref
+@pytest.mark.parametrize("shape,size", [((33, 127), (0.02, 0.1)), ((255, 2047), (0.25, 2.0))])
+def test_poisson_restatement_matches_reference(shape, size):
+    """oracle.poisson equals the upstream PoissonDirichlet::poisson_solve to
+    rounding (the FFTs differ: numpy's vs the upstream radix-2 code) on a
+    random charge density and on a Gaussian blob."""
+    nr, nz = shape
+    dr, dz = size[0] / (nr - 1), size[1] / (nz - 1)
+    ref = refsim.RefSim(size[0], size[1], nr, nz, 1e-12)
+    rng = np.random.default_rng(11)
+    i, k = np.meshgrid(np.arange(nr), np.arange(nz), indexing="ij")
+    blob = 1e-3 * np.exp(-((i - nr / 3) ** 2 / (0.02 * nr * nr) + (k - nz / 2) ** 2 /
+                           (0.01 * nz * nz)))
+    for rho in (rng.normal(0.0, 1e-4, shape), blob):
+        want = ref.poisson_dirichlet(rho)
+        got = poisson_dirichlet(rho, dr, dz)
+        # the solve writes E_r rows i < nr-1 and E_z columns k < nz-1 only
+        # (the upstream leaves the rest as it was: there, uninitialised)
+        sel = (slice(None), slice(None)), (slice(0, nr - 1), slice(None)), \
+            (slice(None), slice(0, nz - 1))
+        for name, a, b, sl in zip(("phi", "E_r", "E_z"), got, want, sel):
+            a, b = a[sl], b[sl]
+            scale = np.abs(b).max()
+            assert scale > 0
+            assert np.abs(a - b).max() <= 1e-11 * scale, (name, np.abs(a - b).max() / scale)
     ref.close()
 
 
