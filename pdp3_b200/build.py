@@ -27,9 +27,9 @@ UNITS = {
     "particles_f64.cu": ["--fmad=false"],
     # approximate FP32 division and square root (<= 2 ulp): the form's error
     # budget is set by FP32 storage, not by these operations
-    "particles_f32.cu": ["--prec-div=false", "--prec-sqrt=false"],
+    "particles_f32.cu": ["--prec-div=false", "--prec-sqrt=false", "-ftz=true"],
     "sort.cu": [],
-    "ensemble.cu": ["--prec-div=false", "--prec-sqrt=false"],
+    "ensemble.cu": ["--prec-div=false", "--prec-sqrt=false", "-ftz=true"],
     "diag.cu": [],
     "noalloc.cu": [],
     "adjoint.cu": ["--prec-div=false", "--prec-sqrt=false"],

@@ -1476,7 +1476,7 @@ pdp3g_status pdp3g_ensemble_create(pdp3g_ctx *const *runs, int32_t n_runs, pdp3g
       if (sp.is_bunch)
         es.uz_beam = (float)(sp.velocity / (LIGHT_SPEED * std::sqrt(1.0 - sp.velocity * sp.velocity /
                                                                            LIGHT_SPEED_POW_2)));
-      ch += (sp.f32.n + 255) / 256;
+      ch += (sp.f32.n + F32_CHUNK - 1) / F32_CHUNK;
       e->total_particles += sp.f32.n;
       hs.push_back(es);
     }

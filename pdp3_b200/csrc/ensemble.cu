@@ -75,8 +75,6 @@ __global__ void __launch_bounds__(F32_THREADS, 4) k_ensemble(EnsembleDev E) {
     SpeciesF32 s;
     int pusher;
   } desc;
-  for (int idx = threadIdx.x; idx < 3 * TILE_CAP; idx += F32_THREADS) sm.acc[idx] = 0.0f;
-  __syncthreads();
   const long long gtid = (long long)blockIdx.x * blockDim.x + threadIdx.x;
   const long long gstride = (long long)gridDim.x * blockDim.x;
   const long long t_start = clock64();

@@ -32,10 +32,12 @@
 //   d_zeta -> 0, where the upstream switches to strict_motion_weighting
 //   (src/particles.cpp:786-988), whose z-only and i = 0 forms they equal.
 //
-// Deposition is accumulated in FP32 per CTA in shared memory over the
-// bounding box of the CTA's particles (particles sorted by cell keep the box
-// small) and flushed into the FP64 grid currents with FP64 atomics; a CTA
-// whose box does not fit adds straight into the FP64 grid.
+// Each warp stages 128 consecutive particles through shared memory (16-byte
+// coalesced loads and stores), each lane steps 4 consecutive particles and
+// keeps FP32 running sums of their deposits while the cell stays the same;
+// one segmented warp reduction per 128 particles then adds the runs into the
+// FP64 grid currents with FP64 atomics (particles sorted by cell make the
+// runs long).  Warps are independent: no CTA-wide synchronisation.
 #include "particles_f32.cuh"
 
 namespace pdp3g {
@@ -44,9 +46,7 @@ template <bool OUT>
 __global__ void __launch_bounds__(F32_THREADS, 4) k_push_deposit_f32(GridDev g, SpeciesF32 s,
                                                                    SpeciesOut o, int pusher) {
   __shared__ F32Shared sm;
-  const long long nchunks = (s.n + F32_THREADS - 1) / F32_THREADS;
-  for (int idx = threadIdx.x; idx < 3 * TILE_CAP; idx += F32_THREADS) sm.acc[idx] = 0.0f;
-  __syncthreads();
+  const long long nchunks = (s.n + F32_CHUNK - 1) / F32_CHUNK;
   for (long long chunk = blockIdx.x; chunk < nchunks; chunk += gridDim.x)
     f32_chunk<OUT>(g, s, o, pusher, chunk, sm);
 }
@@ -201,7 +201,7 @@ void launch_f64_to_cell(const SpeciesF32 &s, const double *r, const double *z, c
 void launch_push_deposit_f32(const GridDev &g, const SpeciesF32 &s, int pusher, int n_sm,
                              int blocks_per_sm, cudaStream_t st) {
   if (s.n <= 0) return;
-  long long chunks = (s.n + F32_THREADS - 1) / F32_THREADS;
+  long long chunks = (s.n + F32_CHUNK - 1) / F32_CHUNK;
   long long blocks = (long long)n_sm * (blocks_per_sm > 0 ? blocks_per_sm : 4);
   if (blocks > chunks) blocks = chunks;
   k_push_deposit_f32<false><<<(int)blocks, F32_THREADS, 0, st>>>(g, s, in_place(s), pusher);
@@ -210,7 +210,7 @@ void launch_push_deposit_f32(const GridDev &g, const SpeciesF32 &s, int pusher, 
 void launch_push_deposit_f32_to(const GridDev &g, const SpeciesF32 &s, const SpeciesOut &o,
                                 int pusher, int n_sm, int blocks_per_sm, cudaStream_t st) {
   if (s.n <= 0) return;
-  long long chunks = (s.n + F32_THREADS - 1) / F32_THREADS;
+  long long chunks = (s.n + F32_CHUNK - 1) / F32_CHUNK;
   long long blocks = (long long)n_sm * (blocks_per_sm > 0 ? blocks_per_sm : 4);
   if (blocks > chunks) blocks = chunks;
   k_push_deposit_f32<true><<<(int)blocks, F32_THREADS, 0, st>>>(g, s, o, pusher);

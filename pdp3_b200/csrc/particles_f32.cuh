@@ -8,7 +8,10 @@ namespace pdp3g {
 #define GIDX(i, k) ((size_t)(i) * (size_t)g.nz + (size_t)(k))
 
 constexpr int F32_THREADS = 256;
-constexpr int TILE_CAP = 1536;  // nodes per component in the shared accumulator
+constexpr int F32_WARPS = F32_THREADS / 32;
+constexpr int F32_PER_LANE = 4;                       // consecutive particles per thread
+constexpr int F32_WARP_CHUNK = 32 * F32_PER_LANE;     // particles per warp
+static_assert(F32_CHUNK == F32_WARPS * F32_WARP_CHUNK, "CTA chunk = its warps' chunks");
 
 __device__ __forceinline__ void flag32(const GridDev &g, unsigned bit) { atomicOr(g.err, bit); }
 
@@ -22,20 +25,8 @@ __device__ __forceinline__ void renorm(int &i, float &f) {
   if (i < 0) { f = f + (float)i; i = 0; }
 }
 
-struct Tile {
-  float *acc;  // [3][TILE_CAP]: j_r, j_phi, j_z
-  int r0, z0, nzb, nrb;
-  bool on;
-};
-
-// adds v into component comp (0 j_r, 1 j_phi, 2 j_z) at node (i, k)
-__device__ __forceinline__ void dep(const GridDev &g, const Tile &t, int comp, int i, int k,
-                                    float v) {
-  const int li = i - t.r0, lk = k - t.z0;
-  if (t.on && (unsigned)li < (unsigned)t.nrb && (unsigned)lk < (unsigned)t.nzb) {
-    atomicAdd(&t.acc[comp * TILE_CAP + li * t.nzb + lk], v);
-    return;
-  }
+// adds v into the FP64 grid current comp (0 j_r, 1 j_phi, 2 j_z) at node (i, k)
+__device__ __forceinline__ void dep(const GridDev &g, int comp, int i, int k, float v) {
   if ((unsigned)i >= (unsigned)g.nr || (unsigned)k >= (unsigned)g.nz) {
     flag32(g, ERR_OUT_OF_GRID);
     return;
@@ -85,23 +76,21 @@ __device__ __forceinline__ void piece_values(int ci, float ao, float co, float a
   }
 }
 
-__device__ __forceinline__ void dep_rz(const GridDev &g, const Tile &t, int ci, int ck,
-                                       const float v[4]) {
-  dep(g, t, 2, ci, ck, v[0]);
-  dep(g, t, 2, ci + 1, ck, v[1]);
-  dep(g, t, 0, ci, ck, v[2]);
-  dep(g, t, 0, ci, ck + 1, v[3]);
+__device__ __forceinline__ void dep_rz(const GridDev &g, int ci, int ck, const float v[4]) {
+  dep(g, 2, ci, ck, v[0]);
+  dep(g, 2, ci + 1, ck, v[1]);
+  dep(g, 0, ci, ck, v[2]);
+  dep(g, 0, ci, ck + 1, v[3]);
 }
 
 // The step's straight path from (i, a, k, b) to (in, an, kn, bn) split at the
 // cell faces it crosses (at most one r face and one z face).  The first
-// piece's cell and values are returned (the caller reduces them across the
-// warp); further pieces are deposited directly.  Returns false when the
-// path spans more than one cell in r or z (nothing is deposited, as upstream).
-__device__ __forceinline__ bool deposit_path(const GridDev &g, const Tile &t, int i, float a,
-                                             int k, float b, int in, float an, int kn, float bn,
-                                             float kz, float kr, int &c0i, int &c0k,
-                                             float first[4]) {
+// piece's cell and values are returned (the caller accumulates them); further
+// pieces are deposited directly.  Returns false when the path spans more than
+// one cell in r or z (nothing is deposited, as upstream).
+__device__ __forceinline__ bool deposit_path(const GridDev &g, int i, float a, int k, float b,
+                                             int in, float an, int kn, float bn, float kz,
+                                             float kr, int &c0i, int &c0k, float first[4]) {
   const int di = in - i, dk = kn - k;
   if (di < -1 || di > 1 || dk < -1 || dk > 1) return false;
   // end point relative to the start cell
@@ -109,18 +98,12 @@ __device__ __forceinline__ bool deposit_path(const GridDev &g, const Tile &t, in
   float tr = 2.0f, tz = 2.0f;
   if (di != 0) tr = ((di > 0 ? 1.0f : 0.0f) - a) / (A - a);
   if (dk != 0) tz = ((dk > 0 ? 1.0f : 0.0f) - b) / (B - b);
-  float ts[2];
-  int kind[2];  // 0: r face, 1: z face
-  int np = 0;
-  if (tr <= 1.0f && tz <= 1.0f) {
-    if (tr <= tz) { ts[0] = tr; kind[0] = 0; ts[1] = tz; kind[1] = 1; }
-    else { ts[0] = tz; kind[0] = 1; ts[1] = tr; kind[1] = 0; }
-    np = 2;
-  } else if (tr <= 1.0f) {
-    ts[0] = tr; kind[0] = 0; np = 1;
-  } else if (tz <= 1.0f) {
-    ts[0] = tz; kind[0] = 1; np = 1;
-  }
+  // crossings in path order: (t0, kind0), (t1, kind1); kind 0 r face, 1 z face
+  const bool cr_r = tr <= 1.0f, cr_z = tz <= 1.0f;
+  const int np = (cr_r ? 1 : 0) + (cr_z ? 1 : 0);
+  const bool r_first = cr_r && (!cr_z || tr <= tz);
+  const float t0 = r_first ? tr : tz, t1 = r_first ? tz : tr;
+  const int kind0 = r_first ? 0 : 1;
   int ci = i, ck = k;
   float pa = a, pb = b;  // current point relative to (i, k)
   c0i = i;
@@ -128,10 +111,11 @@ __device__ __forceinline__ bool deposit_path(const GridDev &g, const Tile &t, in
 #pragma unroll 1
   for (int p = 0; p <= np; p++) {
     float qa, qb;
+    const int kind = (p == 0) ? kind0 : 1 - kind0;
     if (p < np) {
       // crossing point: the crossed coordinate sits exactly on the face
-      const float tt = ts[p];
-      if (kind[p] == 0) {
+      const float tt = p == 0 ? t0 : t1;
+      if (kind == 0) {
         qa = di > 0 ? 1.0f : 0.0f;
         qb = b + tt * (B - b);
       } else {
@@ -148,10 +132,10 @@ __device__ __forceinline__ bool deposit_path(const GridDev &g, const Tile &t, in
     } else {
       float v[4];
       piece_values(ci, pa - oi, pb - ok, qa - oi, qb - ok, kz, kr, v);
-      dep_rz(g, t, ci, ck, v);
+      dep_rz(g, ci, ck, v);
     }
     if (p < np) {
-      if (kind[p] == 0) ci += di; else ck += dk;
+      if (kind == 0) ci += di; else ck += dk;
     }
     pa = qa;
     pb = qb;
@@ -159,16 +143,53 @@ __device__ __forceinline__ bool deposit_path(const GridDev &g, const Tile &t, in
   return true;
 }
 
-// Warp-level segmented sum of the 4 deposits of each run of consecutive
-// lanes with the same key (particles sorted by cell form long runs); the
-// last lane of a run adds the run's totals.  Lanes with key < 0 hold nothing.
+// A lane's running sum of the 4 deposits of consecutive particles with the
+// same key (node layout as in warp_run_deposit); key < 0: empty.
+struct RunAcc {
+  int key;  // node index i * n_grid_z + k of the run's cell
+  float v[4];
+};
+
+template <int MODE>
+__device__ __forceinline__ void acc_flush(const GridDev &g, const RunAcc &A) {
+  const int i = A.key / g.nz, k = A.key - i * g.nz;
+  if (MODE == 0) {
+    dep(g, 1, i, k, A.v[0]);
+    dep(g, 1, i + 1, k, A.v[1]);
+    dep(g, 1, i, k + 1, A.v[2]);
+    dep(g, 1, i + 1, k + 1, A.v[3]);
+  } else {
+    dep_rz(g, i, k, A.v);
+  }
+}
+
+// adds one particle's deposit; a new key flushes the previous run (runs end
+// inside a lane rarely when the particles are sorted by cell)
+template <int MODE>
+__device__ __forceinline__ void acc_add(const GridDev &g, RunAcc &A, int key, const float v[4]) {
+  if (key < 0) return;
+  if (key == A.key) {
+#pragma unroll
+    for (int j = 0; j < 4; j++) A.v[j] += v[j];
+    return;
+  }
+  if (A.key >= 0) acc_flush<MODE>(g, A);
+  A.key = key;
+#pragma unroll
+  for (int j = 0; j < 4; j++) A.v[j] = v[j];
+}
+
+// Warp-level segmented sum of the lanes' running sums: each run of
+// consecutive lanes with the same key (particles sorted by cell form long
+// runs) is added up and its last lane adds the totals into the FP64 grid.
+// Lanes with key < 0 hold nothing.
 // node layout: MODE 0 = j_phi at (i,k), (i+1,k), (i,k+1), (i+1,k+1);
 //              MODE 1 = j_z at (i,k), (i+1,k), j_r at (i,k), (i,k+1).
 template <int MODE>
-__device__ __forceinline__ void warp_run_deposit(const GridDev &g, const Tile &t, int key, int i,
-                                                 int k, float v[4]) {
+__device__ __forceinline__ void warp_run_deposit(const GridDev &g, const RunAcc &A) {
   const unsigned FULL = 0xffffffffu;
   const int lane = threadIdx.x & 31;
+  const int key = A.key;
   const int prev = __shfl_up_sync(FULL, key, 1);
   const int next = __shfl_down_sync(FULL, key, 1);
   const bool head = lane == 0 || prev != key;
@@ -176,26 +197,18 @@ __device__ __forceinline__ void warp_run_deposit(const GridDev &g, const Tile &t
   const unsigned heads = __ballot_sync(FULL, head);
   const unsigned le = lane == 31 ? FULL : ((2u << lane) - 1u);
   const int seg_start = 31 - __clz(heads & le);
+  RunAcc R = A;
 #pragma unroll
   for (int j = 0; j < 4; j++) {
-    float x = v[j];
+    float x = R.v[j];
 #pragma unroll
     for (int off = 1; off < 32; off <<= 1) {
       const float y = __shfl_up_sync(FULL, x, off);
       if (lane >= seg_start + off) x += y;
     }
-    v[j] = x;
+    R.v[j] = x;
   }
-  if (tail && key >= 0) {
-    if (MODE == 0) {
-      dep(g, t, 1, i, k, v[0]);
-      dep(g, t, 1, i + 1, k, v[1]);
-      dep(g, t, 1, i, k + 1, v[2]);
-      dep(g, t, 1, i + 1, k + 1, v[3]);
-    } else {
-      dep_rz(g, t, i, k, v);
-    }
-  }
+  if (tail && key >= 0) acc_flush<MODE>(g, R);
 }
 
 __device__ __forceinline__ void weights_rhalf(int i, float a, int &ir, float &w0, float &w1) {
@@ -240,67 +253,119 @@ __device__ __forceinline__ float gather4(const GridDev &g, const float *__restri
 }
 
 
-// Shared memory of one CTA of the FP32 particle phase.
-struct F32Shared {
-  float acc[3 * TILE_CAP];
-  int red[4][F32_THREADS / 32];
-  int box[4];
+// Per-warp staging of a warp chunk in shared memory: element e of the chunk
+// (particle base + e) sits at slot (e % 4) * 32 + e / 4, so lane l reads its
+// j-th particle (e = 4 l + j) at j * 32 + l and the coalesced 16-byte loads
+// and stores of elements 4 l .. 4 l + 3 land on consecutive slots: both are
+// free of bank conflicts.  Results overwrite the particle's own slots.
+struct WarpStage {
+  int cell[F32_WARP_CHUNK];
+  float fr[F32_WARP_CHUNK], fz[F32_WARP_CHUNK];
+  float ur[F32_WARP_CHUNK], uphi[F32_WARP_CHUNK], uz[F32_WARP_CHUNK];
+  float w[F32_WARP_CHUNK];
+  uint8_t alive[F32_WARP_CHUNK];
 };
 
-// One chunk of F32_THREADS consecutive particles of species s: push,
-// deposit (warp run-reduction -> shared tile -> FP64 grid) and store.
-// Called by every thread of the CTA (it synchronises the CTA); acc must be
-// zero on entry and is left zero.
+// Shared memory of one CTA of the FP32 particle phase.
+struct F32Shared {
+  WarpStage stage[F32_WARPS];
+};
+
+template <typename T>
+__device__ __forceinline__ void stage_in(T *dst, const T *src, long long base, long long n,
+                                         int lane) {
+  const long long e0 = base + F32_PER_LANE * lane;
+  if (base + F32_WARP_CHUNK <= n && ((uintptr_t)(src + base) & 15) == 0) {
+    const int4 v = reinterpret_cast<const int4 *>(src + base)[lane];
+    dst[lane] = reinterpret_cast<const T &>(v.x);
+    dst[32 + lane] = reinterpret_cast<const T &>(v.y);
+    dst[64 + lane] = reinterpret_cast<const T &>(v.z);
+    dst[96 + lane] = reinterpret_cast<const T &>(v.w);
+  } else {
+#pragma unroll
+    for (int j = 0; j < F32_PER_LANE; j++) dst[32 * j + lane] = e0 + j < n ? src[e0 + j] : T();
+  }
+}
+
+template <typename T>
+__device__ __forceinline__ void stage_out(T *dst, const T *src, long long base, long long n,
+                                          int lane) {
+  const long long e0 = base + F32_PER_LANE * lane;
+  if (base + F32_WARP_CHUNK <= n && ((uintptr_t)(dst + base) & 15) == 0) {
+    int4 v;
+    v.x = reinterpret_cast<const int &>(src[lane]);
+    v.y = reinterpret_cast<const int &>(src[32 + lane]);
+    v.z = reinterpret_cast<const int &>(src[64 + lane]);
+    v.w = reinterpret_cast<const int &>(src[96 + lane]);
+    reinterpret_cast<int4 *>(dst + base)[lane] = v;
+  } else {
+#pragma unroll
+    for (int j = 0; j < F32_PER_LANE; j++)
+      if (e0 + j < n) dst[e0 + j] = src[32 * j + lane];
+  }
+}
+
+// One warp chunk (F32_WARP_CHUNK consecutive particles of species s, lane l
+// taking particles 4 l .. 4 l + 3 in order): push, deposit and store.  Each
+// lane keeps running sums of its particles' deposits while their key (cell)
+// stays the same, and the warp adds the lanes' sums up with one segmented
+// reduction per chunk before the FP64 atomics.
 // OUT = false: the step in place (o unused); OUT = true: results go to o.
 template <bool OUT>
-__device__ __forceinline__ void f32_chunk(const GridDev &g, const SpeciesF32 &s,
-                                          const SpeciesOut &o, int pusher, long long chunk,
-                                          F32Shared &sm) {
-  float *acc = sm.acc;
-  auto &red = sm.red;
-  auto &box = sm.box;
+__device__ __forceinline__ void f32_warp_chunk(const GridDev &g, const SpeciesF32 &s,
+                                               const SpeciesOut &o, int pusher, long long wchunk,
+                                               WarpStage &ws) {
+  const int lane = threadIdx.x & 31;
   const int ncz = g.nz - 1;
-    const long long p = chunk * F32_THREADS + threadIdx.x;
+  const long long base = wchunk * F32_WARP_CHUNK;
+  if (base >= s.n) return;
+  const bool has_alive = s.alive != nullptr;
+  stage_in(ws.cell, s.cell, base, s.n, lane);
+  stage_in(ws.fr, s.fr, base, s.n, lane);
+  stage_in(ws.fz, s.fz, base, s.n, lane);
+  stage_in(ws.ur, s.ur, base, s.n, lane);
+  stage_in(ws.uphi, s.uphi, base, s.n, lane);
+  stage_in(ws.uz, s.uz, base, s.n, lane);
+  stage_in(ws.w, s.w, base, s.n, lane);
+  if (has_alive) {
+#pragma unroll
+    for (int j = 0; j < F32_PER_LANE; j++) {
+      const long long e = base + F32_PER_LANE * lane + j;
+      ws.alive[32 * j + lane] = e < s.n ? s.alive[e] : 0;
+    }
+  }
+  __syncwarp();
+  RunAcc acc_phi, acc_rz;
+  acc_phi.key = -1;
+  acc_rz.key = -1;
+#pragma unroll
+  for (int j = 0; j < 4; j++) acc_phi.v[j] = acc_rz.v[j] = 0.0f;
+#pragma unroll 1
+  for (int jp = 0; jp < F32_PER_LANE; jp++) {
+    const int slot = 32 * jp + lane;
+    const long long p = base + F32_PER_LANE * lane + jp;
     bool live = p < s.n;
-    if (live && s.alive != nullptr && !s.alive[p]) live = false;
-    int c = live ? s.cell[p] : 0;
+    if (live && has_alive && !ws.alive[slot]) live = false;
+    int c = live ? ws.cell[slot] : 0;
     if (live && (c < 0 || c >= (g.nr - 1) * ncz)) {
       flag32(g, ERR_OUT_OF_GRID);
       live = false;
     }
-    const int i = c / ncz, k = c - (c / ncz) * ncz;
-    // bounding box of the chunk's start cells (block min/max reduction)
-    int v4[4] = {live ? i : INT_MAX, live ? -i : INT_MAX, live ? k : INT_MAX,
-                 live ? -k : INT_MAX};
-#pragma unroll
-    for (int j = 0; j < 4; j++) {
-#pragma unroll
-      for (int o = 16; o > 0; o >>= 1) v4[j] = min(v4[j], __shfl_xor_sync(0xffffffffu, v4[j], o));
+    // c / ncz through the FP32 reciprocal (exact for c < 2^24), corrected to
+    // the exact quotient
+    int i;
+    if (c < (1 << 24)) {
+      i = (int)((float)c * (1.0f / (float)ncz));
+      if (i * ncz > c) i--;
+      if ((i + 1) * ncz <= c) i++;
+    } else {
+      i = c / ncz;
     }
-    if ((threadIdx.x & 31) == 0)
-#pragma unroll
-      for (int j = 0; j < 4; j++) red[j][threadIdx.x >> 5] = v4[j];
-    __syncthreads();
-    if (threadIdx.x < 4) {
-      int m = INT_MAX;
-      for (int w = 0; w < F32_THREADS / 32; w++) m = min(m, red[threadIdx.x][w]);
-      box[threadIdx.x] = m;
-    }
-    __syncthreads();
-    Tile t;
-    t.acc = acc;
-    t.r0 = box[0] - 1;
-    t.z0 = box[2] - 1;
-    t.nrb = -box[1] - box[0] + 4;
-    t.nzb = -box[3] - box[2] + 4;
-    t.on = box[0] != INT_MAX && t.nrb * t.nzb <= TILE_CAP;
-    // this lane's j_phi and first r-z piece, reduced across the warp below
-    int key_phi = -1, key_rz = -1, phi_i = 0, phi_k = 0, rz_i = 0, rz_k = 0;
-    float vphi4[4] = {0.f, 0.f, 0.f, 0.f}, vrz4[4] = {0.f, 0.f, 0.f, 0.f};
+    const int k = c - i * ncz;
     if (live) {
-      const float a = s.fr[p], b = s.fz[p];
-      float u[3] = {s.ur[p], s.uphi[p], s.uz[p]};
-      const float w = s.w[p];
+      const float a = ws.fr[slot], b = ws.fz[slot];
+      float u[3] = {ws.ur[slot], ws.uphi[slot], ws.uz[slot]};
+      const float w = ws.w[slot];
       // ---- gather E (time n) and H (time n+1/2)
       int ir_h, kz_h;
       float wrh0, wrh1, wrn0, wrn1, wzh0, wzh1;
@@ -393,13 +458,9 @@ __device__ __forceinline__ void f32_chunk(const GridDev &g, const SpeciesF32 &s,
         const float wa = (1.0f - f1) * (2.0f * fi1 + f1) / (rho1 * v1);
         const float wb = f1 * (2.0f * fi1 + 1.0f + f1) / (rho1 * 2.0f * (fi1 + 1.0f));
         const float pref = s.kphi * w * u[1] * inv_g;
-        vphi4[0] = pref * (1.0f - g1) * wa;
-        vphi4[1] = pref * (1.0f - g1) * wb;
-        vphi4[2] = pref * g1 * wa;
-        vphi4[3] = pref * g1 * wb;
-        phi_i = i1;
-        phi_k = k1;
-        key_phi = i1 * g.nz + k1;
+        const float vphi4[4] = {pref * (1.0f - g1) * wa, pref * (1.0f - g1) * wb,
+                                pref * g1 * wa, pref * g1 * wb};
+        acc_add<0>(g, acc_phi, i1 * g.nz + k1, vphi4);
       }
       // ---- second half move, walls, rz rotation (src/particles.cpp:1355-1365)
       float xa2 = a1 + dr_h;
@@ -424,8 +485,10 @@ __device__ __forceinline__ void f32_chunk(const GridDev &g, const SpeciesF32 &s,
       renorm(in, an);
       renorm(kn, bn);
       if (alive_now) {
-        if (deposit_path(g, t, i, a, k, b, in, an, kn, bn, s.kz * w, s.kr * w, rz_i, rz_k, vrz4))
-          key_rz = rz_i * g.nz + rz_k;
+        int rz_i, rz_k;
+        float vrz4[4];
+        if (deposit_path(g, i, a, k, b, in, an, kn, bn, s.kz * w, s.kr * w, rz_i, rz_k, vrz4))
+          acc_add<1>(g, acc_rz, rz_i * g.nz + rz_k, vrz4);
         // back_velocity_to_rz (src/particles.cpp:1005-1015): cos = x/r, sin = y/r
         const float inv_r2 = 1.0f / r2;
         const float st = dy * inv_r2, ct = x2 * inv_r2;
@@ -434,59 +497,52 @@ __device__ __forceinline__ void f32_chunk(const GridDev &g, const SpeciesF32 &s,
         u[0] = u0;
         u[1] = u1;
       }
-      if (OUT) {
-        if (s.alive != nullptr) o.alive[p] = alive_now ? 1 : 0;
-      } else if (!alive_now) {
-        s.alive[p] = 0;
-      }
+      if (has_alive) ws.alive[slot] = alive_now ? 1 : 0;
       if (in > g.nr - 2 || kn > g.nz - 2) {
         flag32(g, ERR_OUT_OF_GRID);
         in = min(in, g.nr - 2);
         kn = min(kn, g.nz - 2);
       }
-      int *cell_o = OUT ? o.cell : s.cell;
-      float *fr_o = OUT ? o.fr : s.fr, *fz_o = OUT ? o.fz : s.fz;
-      float *ur_o = OUT ? o.ur : s.ur, *uphi_o = OUT ? o.uphi : s.uphi, *uz_o = OUT ? o.uz : s.uz;
-      cell_o[p] = in * ncz + kn;
-      fr_o[p] = an;
-      fz_o[p] = bn;
-      ur_o[p] = u[0];
-      uphi_o[p] = u[1];
-      uz_o[p] = u[2];
-    } else if (OUT && p < s.n) {
-      o.cell[p] = s.cell[p];
-      o.fr[p] = s.fr[p];
-      o.fz[p] = s.fz[p];
-      o.ur[p] = s.ur[p];
-      o.uphi[p] = s.uphi[p];
-      o.uz[p] = s.uz[p];
-      if (s.alive != nullptr) o.alive[p] = s.alive[p];
+      ws.cell[slot] = in * ncz + kn;
+      ws.fr[slot] = an;
+      ws.fz[slot] = bn;
+      ws.ur[slot] = u[0];
+      ws.uphi[slot] = u[1];
+      ws.uz[slot] = u[2];
     }
-    warp_run_deposit<0>(g, t, key_phi, phi_i, phi_k, vphi4);
-    warp_run_deposit<1>(g, t, key_rz, rz_i, rz_k, vrz4);
-    __syncthreads();
-    // ---- flush the tile into the FP64 grid currents
-    if (t.on) {
-      const int nb = t.nrb * t.nzb;
-      for (int idx = threadIdx.x; idx < nb; idx += F32_THREADS) {
-        const int li = idx / t.nzb, lk = idx - li * t.nzb;
-        const int gi = t.r0 + li, gk = t.z0 + lk;
-#pragma unroll
-        for (int comp = 0; comp < 3; comp++) {
-          const float v = acc[comp * TILE_CAP + idx];
-          if (v != 0.0f) {
-            acc[comp * TILE_CAP + idx] = 0.0f;
-            if ((unsigned)gi < (unsigned)g.nr && (unsigned)gk < (unsigned)g.nz) {
-              double *base = comp == 0 ? g.jr : (comp == 1 ? g.jphi : g.jz);
-              atomicAdd(base + GIDX(gi, gk), (double)v);
-            } else {
-              flag32(g, ERR_OUT_OF_GRID);
-            }
-          }
-        }
-      }
-    }
-    __syncthreads();
   }
+  warp_run_deposit<0>(g, acc_phi);
+  warp_run_deposit<1>(g, acc_rz);
+  __syncwarp();
+  // particles skipped above (dead, not yet injected) keep their staged state
+  int *cell_o = OUT ? o.cell : s.cell;
+  float *fr_o = OUT ? o.fr : s.fr, *fz_o = OUT ? o.fz : s.fz;
+  float *ur_o = OUT ? o.ur : s.ur, *uphi_o = OUT ? o.uphi : s.uphi, *uz_o = OUT ? o.uz : s.uz;
+  stage_out(cell_o, ws.cell, base, s.n, lane);
+  stage_out(fr_o, ws.fr, base, s.n, lane);
+  stage_out(fz_o, ws.fz, base, s.n, lane);
+  stage_out(ur_o, ws.ur, base, s.n, lane);
+  stage_out(uphi_o, ws.uphi, base, s.n, lane);
+  stage_out(uz_o, ws.uz, base, s.n, lane);
+  if (has_alive) {
+    uint8_t *alive_o = OUT ? o.alive : s.alive;
+#pragma unroll
+    for (int j = 0; j < F32_PER_LANE; j++) {
+      const long long e = base + F32_PER_LANE * lane + j;
+      if (e < s.n) alive_o[e] = ws.alive[32 * j + lane];
+    }
+  }
+  __syncwarp();
+}
+
+// One CTA chunk of F32_CHUNK consecutive particles: warp w takes the w-th
+// warp chunk.  No CTA-wide synchronisation: warps are independent.
+template <bool OUT>
+__device__ __forceinline__ void f32_chunk(const GridDev &g, const SpeciesF32 &s,
+                                          const SpeciesOut &o, int pusher, long long chunk,
+                                          F32Shared &sm) {
+  const int warp = threadIdx.x >> 5;
+  f32_warp_chunk<OUT>(g, s, o, pusher, chunk * F32_WARPS + warp, sm.stage[warp]);
+}
 
 }  // namespace pdp3g

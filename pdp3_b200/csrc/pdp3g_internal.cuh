@@ -20,6 +20,9 @@ constexpr double LIGHT_SPEED_POW_2 = 9.0e16;  // pow(3e8, 2), exact in binary64
 // device error flags (the upstream code calls exit(1) in these cases)
 enum : unsigned { ERR_NAN = 1u, ERR_V_GE_C = 2u, ERR_OUT_OF_GRID = 4u };
 
+// particles per CTA chunk of the FP32 particle phase (particles_f32.cuh)
+constexpr int F32_CHUNK = 1024;
+
 enum { KIND_PLASMA = 0, KIND_BUNCH = 1 };
 
 // Grid view passed by value to kernels.  All component arrays are
