@@ -76,11 +76,42 @@ __device__ __forceinline__ void piece_values(int ci, float ao, float co, float a
   }
 }
 
+// the 4 deposits of a cell (i, k) into the nodes (i..i+1, k..k+1):
+// MODE 0 = j_phi at (i,k), (i+1,k), (i,k+1), (i+1,k+1);
+// MODE 1 = j_z at (i,k), (i+1,k), j_r at (i,k), (i,k+1).
+// One bounds test for the block; the per-node tests only at the grid edge.
+template <int MODE>
+__device__ __forceinline__ void dep_block(const GridDev &g, int i, int k, const float v[4]) {
+  if ((unsigned)i < (unsigned)(g.nr - 1) && (unsigned)k < (unsigned)(g.nz - 1)) {
+    const size_t n0 = GIDX(i, k);
+    if (MODE == 0) {
+      atomicAdd(g.jphi + n0, (double)v[0]);
+      atomicAdd(g.jphi + n0 + g.nz, (double)v[1]);
+      atomicAdd(g.jphi + n0 + 1, (double)v[2]);
+      atomicAdd(g.jphi + n0 + g.nz + 1, (double)v[3]);
+    } else {
+      atomicAdd(g.jz + n0, (double)v[0]);
+      atomicAdd(g.jz + n0 + g.nz, (double)v[1]);
+      atomicAdd(g.jr + n0, (double)v[2]);
+      atomicAdd(g.jr + n0 + 1, (double)v[3]);
+    }
+    return;
+  }
+  if (MODE == 0) {
+    dep(g, 1, i, k, v[0]);
+    dep(g, 1, i + 1, k, v[1]);
+    dep(g, 1, i, k + 1, v[2]);
+    dep(g, 1, i + 1, k + 1, v[3]);
+  } else {
+    dep(g, 2, i, k, v[0]);
+    dep(g, 2, i + 1, k, v[1]);
+    dep(g, 0, i, k, v[2]);
+    dep(g, 0, i, k + 1, v[3]);
+  }
+}
+
 __device__ __forceinline__ void dep_rz(const GridDev &g, int ci, int ck, const float v[4]) {
-  dep(g, 2, ci, ck, v[0]);
-  dep(g, 2, ci + 1, ck, v[1]);
-  dep(g, 0, ci, ck, v[2]);
-  dep(g, 0, ci, ck + 1, v[3]);
+  dep_block<1>(g, ci, ck, v);
 }
 
 // The step's straight path from (i, a, k, b) to (in, an, kn, bn) split at the
@@ -153,14 +184,7 @@ struct RunAcc {
 template <int MODE>
 __device__ __forceinline__ void acc_flush(const GridDev &g, const RunAcc &A) {
   const int i = A.key / g.nz, k = A.key - i * g.nz;
-  if (MODE == 0) {
-    dep(g, 1, i, k, A.v[0]);
-    dep(g, 1, i + 1, k, A.v[1]);
-    dep(g, 1, i, k + 1, A.v[2]);
-    dep(g, 1, i + 1, k + 1, A.v[3]);
-  } else {
-    dep_rz(g, i, k, A.v);
-  }
+  dep_block<MODE>(g, i, k, A.v);
 }
 
 // adds one particle's deposit; a new key flushes the previous run (runs end
@@ -241,11 +265,12 @@ __device__ __forceinline__ void weights_zhalf(int k, float b, int &kz, float &w0
 }
 
 // f: the FP32 copy of the component (GridDev::e32 / hh32), the same values
-// the FP64 grid rounds to
+// the FP64 grid rounds to.  No bounds test: the caller gathers only for a
+// valid cell (0 <= i <= n_grid_r-2, 0 <= k <= n_grid_z-2), and every ir, kz
+// it passes is i or k, or one less clamped at 0, so the four nodes lie in the
+// grid.
 __device__ __forceinline__ float gather4(const GridDev &g, const float *__restrict__ f, int ir,
                                          int kz, float wr0, float wr1, float wz0, float wz1) {
-  if (ir > g.nr - 2) { flag32(g, ERR_OUT_OF_GRID); ir = g.nr - 2; }
-  if (kz > g.nz - 2) { flag32(g, ERR_OUT_OF_GRID); kz = g.nz - 2; }
   const float f00 = __ldg(f + GIDX(ir, kz)), f10 = __ldg(f + GIDX(ir + 1, kz));
   const float f01 = __ldg(f + GIDX(ir, kz + 1));
   const float f11 = __ldg(f + GIDX(ir + 1, kz + 1));
