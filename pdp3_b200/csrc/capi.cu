@@ -68,7 +68,7 @@ struct pdp3g_ctx {
   int64_t launches = 0, particle_launches = 0, steps = 0;
   std::string last_error;
   int64_t bytes = 0;
-  int f32_blocks_per_sm = 4;  // CTAs per SM for the FP32 particle kernel
+  int f32_blocks_per_sm = 0;  // CTAs per SM for the FP32 particle kernel (0: its default)
 };
 
 namespace {

@@ -65,7 +65,7 @@ __device__ void ens_inject(const EnsembleDev &E, const EnsSpecies &sp) {
 
 // The step count is read from E.status[2] (written before each launch), so
 // one captured graph serves every segment length.
-__global__ void __launch_bounds__(F32_THREADS, 4) k_ensemble(EnsembleDev E) {
+__global__ void __launch_bounds__(F32_THREADS, F32_MIN_BLOCKS) k_ensemble(EnsembleDev E) {
   const int nsteps = *(volatile int *)&E.status[2];
   const long long budget = *(volatile const long long *)E.budget_cycles;
   cg::grid_group grid = cg::this_grid();

@@ -42,13 +42,25 @@
 
 namespace pdp3g {
 
-template <bool OUT>
-__global__ void __launch_bounds__(F32_THREADS, 4) k_push_deposit_f32(GridDev g, SpeciesF32 s,
-                                                                   SpeciesOut o, int pusher) {
+template <bool OUT, int PUSHER>
+__global__ void __launch_bounds__(F32_THREADS, F32_MIN_BLOCKS) k_push_deposit_f32(GridDev g, SpeciesF32 s,
+                                                                   SpeciesOut o) {
   __shared__ F32Shared sm;
   const long long nchunks = (s.n + F32_CHUNK - 1) / F32_CHUNK;
   for (long long chunk = blockIdx.x; chunk < nchunks; chunk += gridDim.x)
-    f32_chunk<OUT>(g, s, o, pusher, chunk, sm);
+    f32_chunk<OUT, PUSHER>(g, s, o, PUSHER, chunk, sm);
+}
+
+// one kernel per pusher (0 relativistic Boris, 1 upstream Vay, 2 classic Boris)
+template <bool OUT>
+static void launch_f32_kernel(const GridDev &g, const SpeciesF32 &s, const SpeciesOut &o,
+                              int pusher, int blocks, cudaStream_t st) {
+  if (pusher == 1)
+    k_push_deposit_f32<OUT, 1><<<blocks, F32_THREADS, 0, st>>>(g, s, o);
+  else if (pusher == 2)
+    k_push_deposit_f32<OUT, 2><<<blocks, F32_THREADS, 0, st>>>(g, s, o);
+  else
+    k_push_deposit_f32<OUT, 0><<<blocks, F32_THREADS, 0, st>>>(g, s, o);
 }
 
 // Bunch::bunch_inject in the cell-local form: z = dl * random_reverse(idx, 11)
@@ -202,18 +214,18 @@ void launch_push_deposit_f32(const GridDev &g, const SpeciesF32 &s, int pusher, 
                              int blocks_per_sm, cudaStream_t st) {
   if (s.n <= 0) return;
   long long chunks = (s.n + F32_CHUNK - 1) / F32_CHUNK;
-  long long blocks = (long long)n_sm * (blocks_per_sm > 0 ? blocks_per_sm : 4);
+  long long blocks = (long long)n_sm * (blocks_per_sm > 0 ? blocks_per_sm : F32_MIN_BLOCKS);
   if (blocks > chunks) blocks = chunks;
-  k_push_deposit_f32<false><<<(int)blocks, F32_THREADS, 0, st>>>(g, s, in_place(s), pusher);
+  launch_f32_kernel<false>(g, s, in_place(s), pusher, (int)blocks, st);
 }
 
 void launch_push_deposit_f32_to(const GridDev &g, const SpeciesF32 &s, const SpeciesOut &o,
                                 int pusher, int n_sm, int blocks_per_sm, cudaStream_t st) {
   if (s.n <= 0) return;
   long long chunks = (s.n + F32_CHUNK - 1) / F32_CHUNK;
-  long long blocks = (long long)n_sm * (blocks_per_sm > 0 ? blocks_per_sm : 4);
+  long long blocks = (long long)n_sm * (blocks_per_sm > 0 ? blocks_per_sm : F32_MIN_BLOCKS);
   if (blocks > chunks) blocks = chunks;
-  k_push_deposit_f32<true><<<(int)blocks, F32_THREADS, 0, st>>>(g, s, o, pusher);
+  launch_f32_kernel<true>(g, s, o, pusher, (int)blocks, st);
 }
 
 void launch_bunch_inject_f32(const SpeciesF32 &s, long long start, long long count, double dl,

@@ -8,6 +8,7 @@ namespace pdp3g {
 #define GIDX(i, k) ((size_t)(i) * (size_t)g.nz + (size_t)(k))
 
 constexpr int F32_THREADS = 256;
+constexpr int F32_MIN_BLOCKS = 4;                     // CTAs per SM (64 registers)
 constexpr int F32_WARPS = F32_THREADS / 32;
 constexpr int F32_PER_LANE = 4;                       // consecutive particles per thread
 constexpr int F32_WARP_CHUNK = 32 * F32_PER_LANE;     // particles per warp
@@ -18,10 +19,19 @@ __device__ __forceinline__ void flag32(const GridDev &g, unsigned bit) { atomicO
 // moves (i, f) so that f is in (0, 1] (CELL_NUMBER semantics); cells below
 // 0 clamp to 0 like the upstream "sometimes it gives -1" workaround.
 __device__ __forceinline__ void renorm(int &i, float &f) {
+  // one cell is the usual move; up to 4 in each direction
+  if (f > 1.0f) {
+    f -= 1.0f;
+    i += 1;
 #pragma unroll 1
-  for (int it = 0; it < 4 && f > 1.0f; it++) { f -= 1.0f; i += 1; }
+    for (int it = 1; it < 4 && f > 1.0f; it++) { f -= 1.0f; i += 1; }
+  }
+  if (f <= 0.0f) {
+    f += 1.0f;
+    i -= 1;
 #pragma unroll 1
-  for (int it = 0; it < 4 && f <= 0.0f; it++) { f += 1.0f; i -= 1; }
+    for (int it = 1; it < 4 && f <= 0.0f; it++) { f += 1.0f; i -= 1; }
+  }
   if (i < 0) { f = f + (float)i; i = 0; }
 }
 
@@ -279,10 +289,12 @@ __device__ __forceinline__ float gather4(const GridDev &g, const float *__restri
 
 
 // Per-warp staging of a warp chunk in shared memory: element e of the chunk
-// (particle base + e) sits at slot (e % 4) * 32 + e / 4, so lane l reads its
-// j-th particle (e = 4 l + j) at j * 32 + l and the coalesced 16-byte loads
-// and stores of elements 4 l .. 4 l + 3 land on consecutive slots: both are
-// free of bank conflicts.  Results overwrite the particle's own slots.
+// (particle base + e, lane e / F32_PER_LANE's j-th particle with
+// j = e % F32_PER_LANE) sits at slot j * 32 + e / F32_PER_LANE, so a lane
+// reads its j-th particle at j * 32 + lane and the 16-byte loads and stores
+// of a lane's consecutive elements land on consecutive slots across the
+// warp: both are free of bank conflicts.  Results overwrite the particle's
+// own slots.
 struct WarpStage {
   int cell[F32_WARP_CHUNK];
   float fr[F32_WARP_CHUNK], fz[F32_WARP_CHUNK];
@@ -296,16 +308,22 @@ struct F32Shared {
   WarpStage stage[F32_WARPS];
 };
 
+static_assert(F32_PER_LANE % 4 == 0, "16-byte staging loads");
+constexpr int F32_Q = F32_PER_LANE / 4;  // 16-byte vectors per lane and array
+
 template <typename T>
 __device__ __forceinline__ void stage_in(T *dst, const T *src, long long base, long long n,
                                          int lane) {
   const long long e0 = base + F32_PER_LANE * lane;
   if (base + F32_WARP_CHUNK <= n && ((uintptr_t)(src + base) & 15) == 0) {
-    const int4 v = reinterpret_cast<const int4 *>(src + base)[lane];
-    dst[lane] = reinterpret_cast<const T &>(v.x);
-    dst[32 + lane] = reinterpret_cast<const T &>(v.y);
-    dst[64 + lane] = reinterpret_cast<const T &>(v.z);
-    dst[96 + lane] = reinterpret_cast<const T &>(v.w);
+#pragma unroll
+    for (int q = 0; q < F32_Q; q++) {
+      const int4 v = reinterpret_cast<const int4 *>(src + base)[F32_Q * lane + q];
+      dst[(4 * q + 0) * 32 + lane] = reinterpret_cast<const T &>(v.x);
+      dst[(4 * q + 1) * 32 + lane] = reinterpret_cast<const T &>(v.y);
+      dst[(4 * q + 2) * 32 + lane] = reinterpret_cast<const T &>(v.z);
+      dst[(4 * q + 3) * 32 + lane] = reinterpret_cast<const T &>(v.w);
+    }
   } else {
 #pragma unroll
     for (int j = 0; j < F32_PER_LANE; j++) dst[32 * j + lane] = e0 + j < n ? src[e0 + j] : T();
@@ -317,12 +335,15 @@ __device__ __forceinline__ void stage_out(T *dst, const T *src, long long base, 
                                           int lane) {
   const long long e0 = base + F32_PER_LANE * lane;
   if (base + F32_WARP_CHUNK <= n && ((uintptr_t)(dst + base) & 15) == 0) {
-    int4 v;
-    v.x = reinterpret_cast<const int &>(src[lane]);
-    v.y = reinterpret_cast<const int &>(src[32 + lane]);
-    v.z = reinterpret_cast<const int &>(src[64 + lane]);
-    v.w = reinterpret_cast<const int &>(src[96 + lane]);
-    reinterpret_cast<int4 *>(dst + base)[lane] = v;
+#pragma unroll
+    for (int q = 0; q < F32_Q; q++) {
+      int4 v;
+      v.x = reinterpret_cast<const int &>(src[(4 * q + 0) * 32 + lane]);
+      v.y = reinterpret_cast<const int &>(src[(4 * q + 1) * 32 + lane]);
+      v.z = reinterpret_cast<const int &>(src[(4 * q + 2) * 32 + lane]);
+      v.w = reinterpret_cast<const int &>(src[(4 * q + 3) * 32 + lane]);
+      reinterpret_cast<int4 *>(dst + base)[F32_Q * lane + q] = v;
+    }
   } else {
 #pragma unroll
     for (int j = 0; j < F32_PER_LANE; j++)
@@ -336,10 +357,13 @@ __device__ __forceinline__ void stage_out(T *dst, const T *src, long long base, 
 // stays the same, and the warp adds the lanes' sums up with one segmented
 // reduction per chunk before the FP64 atomics.
 // OUT = false: the step in place (o unused); OUT = true: results go to o.
-template <bool OUT>
+template <bool OUT, int PUSHER>
 __device__ __forceinline__ void f32_warp_chunk(const GridDev &g, const SpeciesF32 &s,
-                                               const SpeciesOut &o, int pusher, long long wchunk,
-                                               WarpStage &ws) {
+                                               const SpeciesOut &o, int pusher_rt,
+                                               long long wchunk, WarpStage &ws) {
+  // PUSHER >= 0 fixes the pusher at compile time (one kernel per pusher keeps
+  // the code small); -1 takes it from pusher_rt
+  const int pusher = PUSHER >= 0 ? PUSHER : pusher_rt;
   const int lane = threadIdx.x & 31;
   const int ncz = g.nz - 1;
   const long long base = wchunk * F32_WARP_CHUNK;
@@ -562,12 +586,12 @@ __device__ __forceinline__ void f32_warp_chunk(const GridDev &g, const SpeciesF3
 
 // One CTA chunk of F32_CHUNK consecutive particles: warp w takes the w-th
 // warp chunk.  No CTA-wide synchronisation: warps are independent.
-template <bool OUT>
+template <bool OUT, int PUSHER = -1>
 __device__ __forceinline__ void f32_chunk(const GridDev &g, const SpeciesF32 &s,
                                           const SpeciesOut &o, int pusher, long long chunk,
                                           F32Shared &sm) {
   const int warp = threadIdx.x >> 5;
-  f32_warp_chunk<OUT>(g, s, o, pusher, chunk * F32_WARPS + warp, sm.stage[warp]);
+  f32_warp_chunk<OUT, PUSHER>(g, s, o, pusher, chunk * F32_WARPS + warp, sm.stage[warp]);
 }
 
 }  // namespace pdp3g
