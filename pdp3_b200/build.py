@@ -32,7 +32,7 @@ UNITS = {
     "ensemble.cu": ["--prec-div=false", "--prec-sqrt=false", "-ftz=true"],
     "diag.cu": [],
     "noalloc.cu": [],
-    "adjoint.cu": ["--prec-div=false", "--prec-sqrt=false"],
+    "adjoint.cu": ["--prec-div=false", "--prec-sqrt=false", "-ftz=true"],
     "probe.cu": [],
     "species_diag.cu": ["--fmad=false"],
     "init.cu": ["--fmad=false"],

@@ -130,46 +130,46 @@ __device__ __forceinline__ void ladd(const GridDev &g, double *f, int i, int k, 
 #define ADJ_THREADS_PER_CTA 256
 #endif
 #ifndef ADJ_MIN_BLOCKS
-#define ADJ_MIN_BLOCKS 4  // CTAs per SM the register budget is sized for (64 registers)
+#define ADJ_MIN_BLOCKS 2  // CTAs per SM the register budget is sized for (128 registers)
 #endif
-// the particle reverse is latency-bound (gathers and adjoint reads behind
-// long dependency chains): more resident warps beat fewer register spills
+// the particle reverse keeps its tape in registers: with the warp-level
+// reduction of the field-node adjoints (no shared tile, no barrier), 2 CTAs
+// of 128 registers per thread beat 4 CTAs of 64 with the tape spilled
 constexpr int ADJ_THREADS = ADJ_THREADS_PER_CTA;
-constexpr int ADJ_TILE = 1024;  // nodes per component in the shared accumulator
-
-struct AdjShared {
-  float acc[6][ADJ_TILE];  // adjoints of E_r, E_phi, E_z, Hh_r, Hh_phi, Hh_z
-  int red[4][ADJ_THREADS / 32];
-  int box[4];
-};
-
-struct AdjTile {
-  float (*acc)[ADJ_TILE];
-  int r0, z0, nrb, nzb;
-  bool on;
-};
-
-// adds v to component comp at node (i, k): the CTA's shared tile when the
-// node is inside it, else the FP64 grid
-__device__ __forceinline__ void tadd(const GridDev &g, const AdjTile &t, double *grid, int comp,
-                                     int i, int k, float v) {
-  if (v == 0.0f) return;
-  const int li = i - t.r0, lk = k - t.z0;
-  if (t.on && (unsigned)li < (unsigned)t.nrb && (unsigned)lk < (unsigned)t.nzb) {
-    atomicAdd(&t.acc[comp][li * t.nzb + lk], v);
-    return;
+// Warp-level segmented sum over runs of consecutive lanes with the same key
+// (particles sorted by cell, with the same half-cell quadrant, share their
+// 24 gather nodes); the last lane of each run holds the run's totals.
+template <int N>
+__device__ __forceinline__ bool warp_seg_sum(int key, float (&v)[N]) {
+  const unsigned FULL = 0xffffffffu;
+  const int lane = threadIdx.x & 31;
+  const int prev = __shfl_up_sync(FULL, key, 1);
+  const int next = __shfl_down_sync(FULL, key, 1);
+  const bool head = lane == 0 || prev != key;
+  const bool tail = lane == 31 || next != key;
+  const unsigned heads = __ballot_sync(FULL, head);
+  const unsigned le = lane == 31 ? FULL : ((2u << lane) - 1u);
+  const int seg_start = 31 - __clz(heads & le);
+#pragma unroll
+  for (int j = 0; j < N; j++) {
+    float x = v[j];
+#pragma unroll
+    for (int off = 1; off < 32; off <<= 1) {
+      const float y = __shfl_up_sync(FULL, x, off);
+      if (lane >= seg_start + off) x += y;
+    }
+    v[j] = x;
   }
-  ladd(g, grid, i, k, v);
+  return tail && key >= 0;
 }
 
 // step 2: particles.  E3 = E of step s, Hh3 = H half-time of step s (three
-// consecutive grids each).  One CTA takes chunks of ADJ_THREADS consecutive
-// particles; the field-node adjoints of a chunk are summed in FP32 in shared
-// memory over the bounding box of its cells (particles sorted by cell keep
-// it small) and added to the FP64 grids once per node.
+// consecutive grids each).  Each thread takes one particle; the 24
+// field-node adjoints of a warp's particles are summed over runs of lanes
+// that share their gather nodes (particles sorted by cell) and each run adds
+// its totals to the FP64 grids.  Warps are independent.
 __global__ void __launch_bounds__(ADJ_THREADS, ADJ_MIN_BLOCKS) k_adj_particles(
     GridDev g, const float *E3, const float *Hh3, AdjSpeciesDev S, AdjGrids A, int face) {
-  __shared__ AdjShared sm;
   const int ncz = g.nz - 1;
   const size_t ng = (size_t)g.nr * g.nz;
   adj::Consts<float> C;
@@ -184,8 +184,6 @@ __global__ void __launch_bounds__(ADJ_THREADS, ADJ_MIN_BLOCKS) k_adj_particles(
   C.nz = g.nz;
   C.bunch = S.st.kind == KIND_BUNCH;
   C.face = face;
-  for (int idx = threadIdx.x; idx < 6 * ADJ_TILE; idx += ADJ_THREADS) (&sm.acc[0][0])[idx] = 0.0f;
-  __syncthreads();
   const long long nchunks = (S.st.n + ADJ_THREADS - 1) / ADJ_THREADS;
   for (long long chunk = blockIdx.x; chunk < nchunks; chunk += gridDim.x) {
     const long long p = chunk * ADJ_THREADS + threadIdx.x;
@@ -193,31 +191,12 @@ __global__ void __launch_bounds__(ADJ_THREADS, ADJ_MIN_BLOCKS) k_adj_particles(
     const int c = live ? S.st.cell[p] : 0;
     if (c < 0 || c >= (g.nr - 1) * ncz) live = false;  // flagged by the forward step
     const int ci = c / ncz, ck = c - (c / ncz) * ncz;
-    // bounding box of the chunk's cells
-    int v4[4] = {live ? ci : INT_MAX, live ? -ci : INT_MAX, live ? ck : INT_MAX,
-                 live ? -ck : INT_MAX};
+    float lf[24];  // this lane's field-node adjoints, reduced across the warp
+    int key = -1, q_ir_h = 0, q_kz_h = 0;
+    if (!live) {
 #pragma unroll
-    for (int j = 0; j < 4; j++)
-#pragma unroll
-      for (int o = 16; o > 0; o >>= 1) v4[j] = min(v4[j], __shfl_xor_sync(0xffffffffu, v4[j], o));
-    if ((threadIdx.x & 31) == 0)
-#pragma unroll
-      for (int j = 0; j < 4; j++) sm.red[j][threadIdx.x >> 5] = v4[j];
-    __syncthreads();
-    if (threadIdx.x < 4) {
-      int m = INT_MAX;
-      for (int w = 0; w < ADJ_THREADS / 32; w++) m = min(m, sm.red[threadIdx.x][w]);
-      sm.box[threadIdx.x] = m;
-    }
-    __syncthreads();
-    AdjTile t;
-    t.acc = sm.acc;
-    t.r0 = sm.box[0] - 1;
-    t.z0 = sm.box[2] - 1;
-    t.nrb = -sm.box[1] - sm.box[0] + 4;
-    t.nzb = -sm.box[3] - sm.box[2] + 4;
-    t.on = sm.box[0] != INT_MAX && t.nrb * t.nzb <= ADJ_TILE;
-    if (live) {
+      for (int j = 0; j < 24; j++) lf[j] = 0.0f;
+    } else {
       adj::Tape<float> tp;
       tp.i = ci;
       tp.k = ck;
@@ -279,45 +258,41 @@ __global__ void __launch_bounds__(ADJ_THREADS, ADJ_MIN_BLOCKS) k_adj_particles(
       S.luz[p] = l_u[2];
       S.lw[p] += (double)l_w;
 #pragma unroll
+      for (int cc = 0; cc < 3; cc++)
+#pragma unroll
+        for (int q = 0; q < 4; q++) {
+          lf[cc * 4 + q] = l_fe[cc][q];
+          lf[12 + cc * 4 + q] = l_fh[cc][q];
+        }
+      // lanes with the same cell and half-cell quadrant share the 24 nodes
+      key = ((ci * ncz + ck) * 2 + (tp.ir_h == ci ? 1 : 0)) * 2 + (tp.kz_h == ck ? 1 : 0);
+      q_ir_h = ir_h;
+      q_kz_h = kz_h;
+    }
+    if (warp_seg_sum<24>(key, lf)) {
+      const int ir_n = ci, kz_n = ck;
+#pragma unroll
       for (int cc = 0; cc < 3; cc++) {
         {
-          const int ir = adj::comp_rhalf(0, cc) ? ir_h : ir_n;
-          const int kz = adj::comp_zhalf(0, cc) ? kz_h : kz_n;
+          const int ir = adj::comp_rhalf(0, cc) ? q_ir_h : ir_n;
+          const int kz = adj::comp_zhalf(0, cc) ? q_kz_h : kz_n;
           double *grid = cc == 0 ? A.lEr : (cc == 1 ? A.lEphi : A.lEz);
-          tadd(g, t, grid, cc, ir, kz, l_fe[cc][0]);
-          tadd(g, t, grid, cc, ir + 1, kz, l_fe[cc][1]);
-          tadd(g, t, grid, cc, ir, kz + 1, l_fe[cc][2]);
-          tadd(g, t, grid, cc, ir + 1, kz + 1, l_fe[cc][3]);
+          ladd(g, grid, ir, kz, lf[cc * 4 + 0]);
+          ladd(g, grid, ir + 1, kz, lf[cc * 4 + 1]);
+          ladd(g, grid, ir, kz + 1, lf[cc * 4 + 2]);
+          ladd(g, grid, ir + 1, kz + 1, lf[cc * 4 + 3]);
         }
         {
-          const int ir = adj::comp_rhalf(1, cc) ? ir_h : ir_n;
-          const int kz = adj::comp_zhalf(1, cc) ? kz_h : kz_n;
+          const int ir = adj::comp_rhalf(1, cc) ? q_ir_h : ir_n;
+          const int kz = adj::comp_zhalf(1, cc) ? q_kz_h : kz_n;
           double *grid = cc == 0 ? A.lHhr : (cc == 1 ? A.lHhphi : A.lHhz);
-          tadd(g, t, grid, 3 + cc, ir, kz, l_fh[cc][0]);
-          tadd(g, t, grid, 3 + cc, ir + 1, kz, l_fh[cc][1]);
-          tadd(g, t, grid, 3 + cc, ir, kz + 1, l_fh[cc][2]);
-          tadd(g, t, grid, 3 + cc, ir + 1, kz + 1, l_fh[cc][3]);
+          ladd(g, grid, ir, kz, lf[12 + cc * 4 + 0]);
+          ladd(g, grid, ir + 1, kz, lf[12 + cc * 4 + 1]);
+          ladd(g, grid, ir, kz + 1, lf[12 + cc * 4 + 2]);
+          ladd(g, grid, ir + 1, kz + 1, lf[12 + cc * 4 + 3]);
         }
       }
     }
-    __syncthreads();
-    if (t.on) {
-      const int nb = t.nrb * t.nzb;
-      for (int idx = threadIdx.x; idx < nb; idx += ADJ_THREADS) {
-        const int li = idx / t.nzb, lk = idx - li * t.nzb;
-#pragma unroll
-        for (int comp = 0; comp < 6; comp++) {
-          const float v = sm.acc[comp][idx];
-          if (v != 0.0f) {
-            sm.acc[comp][idx] = 0.0f;
-            double *grid = comp == 0 ? A.lEr : comp == 1 ? A.lEphi : comp == 2 ? A.lEz
-                         : comp == 3 ? A.lHhr : comp == 4 ? A.lHhphi : A.lHhz;
-            ladd(g, grid, t.r0 + li, t.z0 + lk, v);
-          }
-        }
-      }
-    }
-    __syncthreads();
   }
 }
 
