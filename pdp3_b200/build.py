@@ -25,14 +25,15 @@ UNITS = {
     "capi.cu": [],
     "fields.cu": ["--fmad=false"],
     "particles_f64.cu": ["--fmad=false"],
-    # approximate FP32 division and square root (<= 2 ulp): the form's error
+    # FP32 units: approximate division, square root and flush-to-zero (no
+    # quantity of the step is near the subnormal range); the form's error
     # budget is set by FP32 storage, not by these operations
     "particles_f32.cu": ["-use_fast_math"],
     "sort.cu": [],
     "ensemble.cu": ["-use_fast_math"],
     "diag.cu": [],
     "noalloc.cu": [],
-    "adjoint.cu": ["--prec-div=false", "--prec-sqrt=false", "-ftz=true"],
+    "adjoint.cu": ["-use_fast_math"],
     "probe.cu": [],
     "species_diag.cu": ["--fmad=false"],
     "init.cu": ["--fmad=false"],
