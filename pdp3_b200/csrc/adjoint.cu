@@ -113,14 +113,6 @@ __device__ __forceinline__ float lget(const GridDev &g, const float *f, int i, i
   return __ldg(f + (size_t)i * g.nz + k);
 }
 
-__global__ void k_capture_fields(const double *e3, const double *hh3, float *dst, size_t ng) {
-  for (size_t t = blockIdx.x * (size_t)blockDim.x + threadIdx.x; t < 3 * ng;
-       t += (size_t)gridDim.x * blockDim.x) {
-    dst[t] = (float)e3[t];
-    dst[3 * ng + t] = (float)hh3[t];
-  }
-}
-
 __device__ __forceinline__ void ladd(const GridDev &g, double *f, int i, int k, float v) {
   if (v == 0.0f || (unsigned)i >= (unsigned)g.nr || (unsigned)k >= (unsigned)g.nz) return;
   atomicAdd(f + (size_t)i * g.nz + k, (double)v);
@@ -356,11 +348,6 @@ void adj_launch_e(const GridDev &g, const AdjGrids &A, cudaStream_t st) {
 
 void adj_launch_h(const GridDev &g, const AdjGrids &A, cudaStream_t st) {
   k_adj_h<<<blocks_for((long long)g.nr * g.nz, 256), 256, 0, st>>>(g, A);
-}
-
-void adj_launch_capture_fields(const double *e3, const double *hh3, float *dst, size_t ng,
-                               cudaStream_t st) {
-  k_capture_fields<<<blocks_for((long long)(3 * ng), 256), 256, 0, st>>>(e3, hh3, dst, ng);
 }
 
 void adj_launch_particles(const GridDev &g, const float *E3, const float *Hh3,

@@ -274,10 +274,6 @@ void adj_launch_e(const GridDev &g, const AdjGrids &A, cudaStream_t st);
 void adj_launch_h(const GridDev &g, const AdjGrids &A, cudaStream_t st);
 void adj_launch_particles(const GridDev &g, const float *E3, const float *Hh3,
                           const AdjSpeciesDev &S, const AdjGrids &A, int face, cudaStream_t st);
-// FP32 copy of the particle phase's field inputs: E (3 grids from e3) and the
-// half-step H (3 grids from hh3) into dst (6 grids)
-void adj_launch_capture_fields(const double *e3, const double *hh3, float *dst, size_t ng,
-                               cudaStream_t st);
 void adj_launch_inject(const AdjSpeciesDev &S, long long start, long long count, double dt,
                        double dz, double velocity, const double *inv_pow11, double *lv,
                        cudaStream_t st);
