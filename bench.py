@@ -261,6 +261,8 @@ def main():
                          "'near' (the 4 density bumps nearest the probe, gamma, radius), "
                          "'all', or 'none'")
     ap.add_argument("--ensemble-runs", type=int, default=64)
+    ap.add_argument("--ensemble-scale", type=int, default=1,
+                    help="divide every ensemble run's grid by this (smaller runs)")
     ap.add_argument("--ppc", type=int, default=None,
                     help="macroparticles per cell (profiling runs on a smaller case)")
     ap.add_argument("--e2e-steps", type=int, default=3)
@@ -505,7 +507,8 @@ def run_ensemble(args, rank, world, local_rank, dist=None):
     from pdp3_b200 import api
     from pdp3_b200 import workloads as W
     torch.cuda.set_device(local_rank)
-    params = W.ensemble_params(seed=1005 + 100 * rank, n_runs=args.ensemble_runs)
+    params = W.ensemble_params(seed=1005 + 100 * rank, n_runs=args.ensemble_runs,
+                               scale=args.ensemble_scale)
     sims, n_slots = [], 0
     for p in params:
         wl = W.ensemble_run_workload(p, steps=500)
@@ -563,9 +566,13 @@ def run_ensemble(args, rank, world, local_rank, dist=None):
             "steps": args.steps, "warmup": args.warmup, "ms_per_step": ms_max / args.steps,
             "higher_is_better": True, "scaling": "weak", "vs_baseline": None,
             "dtype": "f32+f64acc", "data": "synthetic (seeded)",
-            "config": {"workload": "ensemble_%druns" % len(sims), "runs": len(sims),
+            "config": {"workload": "ensemble_%druns%s" % (
+                           len(sims), "" if args.ensemble_scale == 1 else
+                           "_scale%d" % args.ensemble_scale),
+                       "runs": len(sims),
                        "particle_slots": n_slots, "alive_particles": alive,
-                       "grids": "r in {64,128,256} x z in {256,512,1024} cells",
+                       "grids": "r in {64,128,256} x z in {256,512,1024} cells / %d"
+                                % args.ensemble_scale,
                        "parallelism": "replicas x%d" % world},
             "ensemble": {"blocks_per_sm": bpsm, "blocks": info["blocks"],
                          "cuda_graph": bool(info["used_graph"]), "ms_per_step": ms / args.steps},

@@ -196,18 +196,19 @@ def small_config(seed=7, n_grid_r=17, n_grid_z=33, r_size=0.01, z_size=0.04, ppc
                     n_grid_z, courant_dt(dr, dz), steps, pml, pusher, sp, bm)
 
 
-def ensemble_params(seed=1005, n_runs=64, cell=3.90625e-4):
+def ensemble_params(seed=1005, n_runs=64, cell=3.90625e-4, scale=1):
     """Run parameters of the batched-ensemble case: grids drawn uniformly from
-    r in {64, 128, 256} x z in {256, 512, 1024} cells (cell size fixed), 16-64
-    ppc, density log-uniform in [1e15, 1e17] m^-3, an electron bunch with
-    gamma uniform in [3, 10] per run.  Returns one dict per run; build each
-    Workload with ensemble_run_workload (so only one run's arrays are on the
-    host at a time)."""
+    r in {64, 128, 256} x z in {256, 512, 1024} cells (cell size fixed; each
+    divided by scale for a case of smaller runs), 16-64 ppc, density
+    log-uniform in [1e15, 1e17] m^-3, an electron bunch with gamma uniform in
+    [3, 10] per run.  Returns one dict per run; build each Workload with
+    ensemble_run_workload (so only one run's arrays are on the host at a
+    time)."""
     rng = np.random.default_rng(seed)
     runs = []
     for r in range(n_runs):
-        nrc = int(rng.choice([64, 128, 256]))
-        nzc = int(rng.choice([256, 512, 1024]))
+        nrc = int(rng.choice([64, 128, 256])) // scale
+        nzc = int(rng.choice([256, 512, 1024])) // scale
         runs.append({"seed": seed * 1000 + r, "n_grid_r": nrc + 1, "n_grid_z": nzc + 1,
                      "r_size": nrc * cell, "z_size": nzc * cell,
                      "ppc": int(rng.integers(16, 65)),
