@@ -191,6 +191,20 @@ pdp3g_status pdp3g_set_field(pdp3g_ctx *ctx, int32_t comp, const double *host_in
    any pointer may be NULL. */
 pdp3g_status pdp3g_get_species(pdp3g_ctx *ctx, int32_t id, double *r, double *z, double *vr,
                                double *vphi, double *vz, double *w, uint8_t *alive);
+/* The species' state out to host arrays and the next state in, in one call:
+   the device->host and host->device copies run concurrently in chunks (both
+   PCIe directions at once; use pinned host memory for the overlap).  out_*
+   receive what pdp3g_get_species returns; in_* are then loaded as
+   pdp3g_set_species loads them (with the same checks).  in may equal out: a
+   chunk is read back in only after it was written out.  No counterpart in
+   the upstream, whose particles live in host memory; it serves a host that
+   keeps the authoritative particle state across steps.  alive arrays may be
+   NULL (out: all 1 when the species has no alive flags). */
+pdp3g_status pdp3g_exchange_species(pdp3g_ctx *ctx, int32_t id, double *out_r, double *out_z,
+                                    double *out_vr, double *out_vphi, double *out_vz,
+                                    uint8_t *out_alive, const double *in_r, const double *in_z,
+                                    const double *in_vr, const double *in_vphi,
+                                    const double *in_vz, const uint8_t *in_alive);
 pdp3g_status pdp3g_set_species(pdp3g_ctx *ctx, int32_t id, const double *r, const double *z,
                                const double *vr, const double *vphi, const double *vz,
                                const uint8_t *alive);

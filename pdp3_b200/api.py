@@ -126,6 +126,7 @@ EXPORTS = [
                                                               ctypes.POINTER(ctypes.c_int64)]),
     ("pdp3g_temperature", _I32, [_VP, _I32, _D]),
     ("pdp3g_density", _I32, [_VP, _I32, _D]),
+    ("pdp3g_exchange_species", _I32, [_VP, _I32] + [_D] * 5 + [_U8] + [_D] * 5 + [_U8]),
     ("pdp3g_poisson_solve", _I32, [_VP, _D, _D]),
     ("pdp3g_probe_particles", _I32, [_VP] + [_I32] * 5 + [_D] * 5 +
      [ctypes.c_int64, ctypes.POINTER(ctypes.c_int64)]),
@@ -269,6 +270,24 @@ class Simulation:
                                              alive.ctypes.data_as(_U8)), "get_species")
         out["alive"] = alive
         return out
+
+    def exchange_species(self, sid, out, inp):
+        """pdp3g_exchange_species: fills out (dict of float64 r, z, vr, vphi,
+        vz and uint8 alive arrays, each of the species' size; pinned memory
+        for the copy overlap) with the state and loads inp (same layout; may
+        be out itself) as the new state."""
+        keys = ("r", "z", "vr", "vphi", "vz")
+        n = self.species_size(sid)
+        for d in (out, inp):
+            for k in keys:
+                a = d[k]
+                assert a.dtype == np.float64 and a.flags.c_contiguous and a.size == n, k
+        oa, ia = out.get("alive"), inp.get("alive")
+        self._check(self.L.pdp3g_exchange_species(
+            self.h, sid, *[_p(out[k]) for k in keys],
+            oa.ctypes.data_as(_U8) if oa is not None else None,
+            *[_p(inp[k]) for k in keys],
+            ia.ctypes.data_as(_U8) if ia is not None else None), "exchange_species")
 
     def set_species(self, sid, r=None, z=None, vr=None, vphi=None, vz=None, alive=None):
         keep = [None if a is None else _f64(a) for a in (r, z, vr, vphi, vz)]

@@ -39,6 +39,8 @@ struct pdp3g_ctx {
   int device = 0;
   int n_sm = 148;
   cudaStream_t stream = nullptr;
+  cudaStream_t stream_up = nullptr;  // pdp3g_exchange_species' host->device copies
+  cudaEvent_t ev_chunk = nullptr, ev_up = nullptr;
   double dr = 0, dz = 0, t = 0;
   double *grid_mem = nullptr;
   float *mirror = nullptr;       // FP32 contexts: E and half-step H in FP32 (6 grids)
@@ -337,6 +339,9 @@ void pdp3g_destroy(pdp3g_ctx *ctx) {
   cudaFree(ctx->d_sort);
   cudaFree(ctx->d_stage);
   if (ctx->stream) cudaStreamDestroy(ctx->stream);
+  if (ctx->stream_up) cudaStreamDestroy(ctx->stream_up);
+  if (ctx->ev_chunk) cudaEventDestroy(ctx->ev_chunk);
+  if (ctx->ev_up) cudaEventDestroy(ctx->ev_up);
   delete ctx;
 }
 
@@ -930,6 +935,77 @@ pdp3g_status pdp3g_get_species(pdp3g_ctx *ctx, int32_t id, double *r, double *z,
       memset(alive, 1, (size_t)d.n);
   }
   CK(cudaStreamSynchronize(st));
+  return PDP3G_OK;
+}
+
+// pdp3g_exchange_species: the species' state out to host arrays and the
+// next state in, pipelined by chunks of EXCHANGE_CHUNK particles: chunk c's
+// device->host copies run on the context's stream, its host->device copies
+// on a second stream once chunk c has left, so both PCIe directions work at
+// once.  The host->device copy of a chunk overwrites the device staging (or,
+// in the FP64 form, the state arrays) only after that chunk was copied out,
+// which also makes in == out a correct round trip.
+constexpr size_t EXCHANGE_CHUNK = (size_t)1 << 20;
+
+pdp3g_status pdp3g_exchange_species(pdp3g_ctx *ctx, int32_t id, double *out_r, double *out_z,
+                                    double *out_vr, double *out_vphi, double *out_vz,
+                                    uint8_t *out_alive, const double *in_r, const double *in_z,
+                                    const double *in_vr, const double *in_vphi,
+                                    const double *in_vz, const uint8_t *in_alive) {
+  if (!ctx || id < 0 || id >= (int32_t)ctx->species.size()) return PDP3G_INVALID_ARG;
+  double *outs[5] = {out_r, out_z, out_vr, out_vphi, out_vz};
+  const double *ins[5] = {in_r, in_z, in_vr, in_vphi, in_vz};
+  for (int j = 0; j < 5; j++)
+    if (!outs[j] || !ins[j]) return fail(ctx, PDP3G_INVALID_ARG, "exchange_species: null array");
+  CK(cudaSetDevice(ctx->device));
+  if (!ctx->stream_up) {
+    CK(cudaStreamCreateWithFlags(&ctx->stream_up, cudaStreamNonBlocking));
+    CK(cudaEventCreateWithFlags(&ctx->ev_chunk, cudaEventDisableTiming));
+    CK(cudaEventCreateWithFlags(&ctx->ev_up, cudaEventDisableTiming));
+  }
+  Species &sp = ctx->species[id];
+  cudaStream_t down = ctx->stream, up = ctx->stream_up;
+  const size_t n = (size_t)(sp.fp32 ? sp.f32.n : sp.dev.n);
+  double *dev[5];
+  uint8_t *dev_alive = sp.fp32 ? sp.f32.alive : sp.dev.alive;
+  if (sp.fp32) {
+    pdp3g_status rs = stage_reserve(ctx, n);
+    if (rs != PDP3G_OK) return rs;
+    double *S = ctx->d_stage;
+    launch_cell_to_f64(sp.f32, ctx->dr, ctx->dz, ctx->cfg.n_grid_z - 1, S, S + n, S + 2 * n,
+                       S + 3 * n, S + 4 * n, nullptr, down);
+    ctx->launches++;
+    for (int j = 0; j < 5; j++) dev[j] = S + j * n;
+  } else {
+    SpeciesDev &d = sp.dev;
+    double *a[5] = {d.r, d.z, d.vr, d.vphi, d.vz};
+    for (int j = 0; j < 5; j++) dev[j] = a[j];
+  }
+  // the upload stream starts after everything queued on the context's stream
+  CK(cudaEventRecord(ctx->ev_up, down));
+  CK(cudaStreamWaitEvent(up, ctx->ev_up, 0));
+  for (size_t c0 = 0; c0 < n; c0 += EXCHANGE_CHUNK) {
+    const size_t cn = std::min(EXCHANGE_CHUNK, n - c0), b = sizeof(double) * cn;
+    for (int j = 0; j < 5; j++)
+      CK(cudaMemcpyAsync(outs[j] + c0, dev[j] + c0, b, cudaMemcpyDeviceToHost, down));
+    if (dev_alive && out_alive)
+      CK(cudaMemcpyAsync(out_alive + c0, dev_alive + c0, cn, cudaMemcpyDeviceToHost, down));
+    CK(cudaEventRecord(ctx->ev_chunk, down));
+    CK(cudaStreamWaitEvent(up, ctx->ev_chunk, 0));
+    for (int j = 0; j < 5; j++)
+      CK(cudaMemcpyAsync(dev[j] + c0, ins[j] + c0, b, cudaMemcpyHostToDevice, up));
+    if (dev_alive && in_alive)
+      CK(cudaMemcpyAsync(dev_alive + c0, in_alive + c0, cn, cudaMemcpyHostToDevice, up));
+  }
+  CK(cudaEventRecord(ctx->ev_up, up));
+  CK(cudaStreamWaitEvent(down, ctx->ev_up, 0));
+  if (sp.fp32) {
+    pdp3g_status rs = convert_staged_f32(ctx, sp, false);  // synchronises the stream
+    if (rs != PDP3G_OK) return rs;
+  } else {
+    CK(cudaStreamSynchronize(down));
+  }
+  if (!dev_alive && out_alive) memset(out_alive, 1, n);
   return PDP3G_OK;
 }
 

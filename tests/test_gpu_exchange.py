@@ -1,0 +1,93 @@
+"""pdp3g_exchange_species: the state out and the next state in, with the two
+copy directions pipelined by chunks of 2^20 particles on two streams.
+
+* out receives exactly what pdp3g_get_species returns; the species then
+  holds in (bit for bit in the FP64 form; in the FP32 form as
+  pdp3g_set_species would store it).
+* in == out (a round trip through pinned host memory, several chunks): the
+  state is unchanged and the next step equals the step of a context that
+  made no round trip (to 1e-12 in the FP64 form: its grid currents are
+  summed by atomics in a varying order).
+"""
+import numpy as np
+import pytest
+import torch
+
+from helpers import rel_inf
+from pdp3_b200 import api
+from pdp3_b200 import workloads as W
+
+pytestmark = pytest.mark.gpu
+
+KEYS = ("r", "z", "vr", "vphi", "vz")
+
+
+def pinned(a):
+    t = torch.empty(a.size, dtype=torch.from_numpy(a[:1]).dtype, pin_memory=True).numpy()
+    t[:] = a
+    return t
+
+
+@pytest.mark.parametrize("precision", ["fp64", "fp32"])
+def test_exchange_out_and_in(precision):
+    wl = W.small_config(beam=True, steps=3)
+    sim = api.from_workload(wl, precision=precision)
+    sim.step(3)
+    sim.sync()
+    for sid in range(3):
+        state = sim.species(sid)
+        n = state["r"].size
+        out = {k: np.zeros(n) for k in KEYS}
+        out["alive"] = np.zeros(n, dtype=np.uint8)
+        inp = {k: state[k].copy() for k in KEYS}
+        inp["vz"] = inp["vz"] * 0.5
+        inp["alive"] = state["alive"].copy()
+        sim.exchange_species(sid, out, inp)
+        for k in KEYS + ("alive",):
+            assert np.array_equal(out[k], state[k]), (sid, k)
+        now = sim.species(sid)
+        m = state["alive"].astype(bool)
+        if precision == "fp64":
+            for k in KEYS:
+                assert np.array_equal(now[k], inp[k]), (sid, k)
+        else:
+            assert np.abs(now["r"][m] - inp["r"][m]).max() <= 1e-6 * wl.r_size
+            assert np.abs(now["z"][m] - inp["z"][m]).max() <= 1e-6 * wl.z_size
+            for k in ("vr", "vphi", "vz"):
+                scale = max(float(np.abs(inp[k][m]).max()), 1.0)
+                assert np.abs(now[k][m] - inp[k][m]).max() <= 1e-6 * scale, (sid, k)
+    sim.close()
+
+
+@pytest.mark.parametrize("precision", ["fp64", "fp32"])
+def test_round_trip_in_place_several_chunks(precision):
+    wl = W.wake_config(ppc=3)          # 1.57M particles per plasma species: 2 chunks
+    a = api.from_workload(wl, precision=precision)
+    b = api.from_workload(wl, precision=precision)
+    for s_ in (a, b):
+        s_.step(2)
+        s_.sync()
+    before = [a.species(sid) for sid in range(2)]
+    for sid in range(2):
+        buf = {k: pinned(before[sid][k]) for k in KEYS}
+        buf["alive"] = pinned(before[sid]["alive"])
+        a.exchange_species(sid, buf, buf)
+        for k in KEYS:
+            assert np.array_equal(buf[k], before[sid][k]), (sid, k)
+        after = a.species(sid)
+        for k in KEYS:
+            if precision == "fp64":
+                assert np.array_equal(after[k], before[sid][k]), (sid, k)
+            else:
+                scale = max(float(np.abs(before[sid][k]).max()), 1e-300)
+                assert np.abs(after[k] - before[sid][k]).max() <= 1e-6 * scale, (sid, k)
+    a.step(1)
+    b.step(1)
+    a.sync()
+    b.sync()
+    # the FP64 grid currents sum by atomics, whose order varies run to run
+    tol = 1e-12 if precision == "fp64" else 1e-5
+    for c in ("E_r", "E_z", "H_phi", "J_r", "J_z"):
+        assert rel_inf(a.field(c), b.field(c)) <= tol, c
+    a.close()
+    b.close()
