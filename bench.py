@@ -388,6 +388,12 @@ def main():
     e2e = None
     if args.e2e_steps > 0 and wl.device_plasma is None:
         e2e = run_e2e(sim, wl, torch, stream, args.e2e_steps)
+        # whole job: the particle-steps of all ranks over the slowest rank's time
+        e2e_ms, e2e_work = aggregate_ranks(dist, 1000.0 * e2e.pop("_secs"), e2e.pop("_work"),
+                                           "cuda")
+        e2e["value"] = e2e_work / (e2e_ms / 1000.0)
+        e2e["h2d_bytes_per_step"] *= world  # every rank copies its own replica
+        e2e["d2h_bytes_per_step"] *= world
     elif wl.device_plasma is not None:
         e2e = {"value": None, "unit": UNIT, "h2d_bytes_per_step": None,
                "d2h_bytes_per_step": None,
@@ -774,7 +780,7 @@ def run_e2e(sim, wl, torch, stream, steps):
                            for sid, a, al, _ in bufs)
     secs = time.perf_counter() - t0
     return {"value": alive_total / secs, "unit": UNIT, "h2d_bytes_per_step": h2d,
-            "d2h_bytes_per_step": d2h, "steps": steps,
+            "d2h_bytes_per_step": d2h, "steps": steps, "_secs": secs, "_work": alive_total,
             "note": "per step, through the C ABI: one step, then every species' full state "
                     "D2H into pinned host arrays and from them H2D as the next step's input "
                     "(pdp3g_exchange_species, both directions concurrently), E_z D2H"}
