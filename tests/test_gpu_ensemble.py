@@ -4,8 +4,9 @@ stepped one by one; the cancel flag and the time budget stop it with
 PDP3G_TIMEOUT without hanging, and the autotuner picks a feasible shape.
 
 Tolerance: each run's grids within 1e-4 of max|x| of the run stepped alone
-(same arithmetic; the FP32 tile sums and FP64 atomics add in a different
-order)."""
+(same arithmetic; the FP32 running sums and FP64 atomics add in a different
+order).  Runs may use different pushers: the ensemble kernel picks each
+species' pusher at run time."""
 import numpy as np
 import pytest
 
@@ -48,6 +49,26 @@ def test_ensemble_matches_runs_stepped_alone():
         for c in ("E_r", "E_z", "H_phi", "J_z", "J_r", "J_phi"):
             assert rel_inf(b.field(c), a.field(c)) <= 1e-4, c
         assert np.array_equal(a.species(2)["alive"], b.species(2)["alive"])
+    ens.close()
+
+
+def test_ensemble_of_runs_with_different_pushers():
+    wls = small_runs(3)
+    pushers = ["vay", "boris_classic", "boris"]
+    alone = [api.from_workload(wl, precision="fp32", pusher=p) for wl, p in zip(wls, pushers)]
+    batch = [api.from_workload(wl, precision="fp32", pusher=p) for wl, p in zip(wls, pushers)]
+    for s in alone:
+        s.step(6)
+        s.sync()
+    ens = api.Ensemble(batch)
+    ens.run(6)
+    assert ens.info()["last_steps_done"] == 6
+    for a, b in zip(alone, batch):
+        b.sync()
+        for c in ("E_r", "E_z", "H_phi", "J_z", "J_r", "J_phi"):
+            assert rel_inf(b.field(c), a.field(c)) <= 1e-4, c
+        sa, sb = a.species(0), b.species(0)
+        assert np.abs(sa["vz"] - sb["vz"]).max() <= 1e-5 * np.abs(sa["vz"]).max()
     ens.close()
 
 
