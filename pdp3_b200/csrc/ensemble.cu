@@ -6,8 +6,8 @@
 //   A  bunch injection, H update and J clear of every run
 //   B  push + deposition of every chunk of every species of every run
 //   C  E update of every run, t += dt
-// Work items are global index spaces (nodes of all runs, 256-particle chunks
-// of all species) dealt to CTAs round-robin, so runs of very different sizes
+// Work items are global index spaces (nodes of all runs, F32_CHUNK-particle
+// chunks of all species) dealt to CTAs round-robin, so runs of very different sizes
 // share the GPU without per-run launches.  Each run's step is the same as
 // pdp3g_step on that run alone (same device functions, fields_body.cuh and
 // particles_f32.cuh).
