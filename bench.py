@@ -42,6 +42,10 @@ if ROOT not in sys.path:
 METRIC = "particle-steps/s & cell-updates/s: FP32 vs FP64 GPU form at fixed Gauss error"
 UNIT = "particle-steps/s"
 BYTES_PER_PARTICLE = {"fp64": 88, "fp32": 52}
+# Yee E + H update per node: H reads E 3 + H 3, writes H 3 + H_half 3 (96 B);
+# E reads E 3 + H 3 + J 3 + sigma, writes E 3 (104 B); the FP32 form also
+# writes the FP32 copies of E and the half-step H (24 B)
+BYTES_PER_NODE = {"fp64": 200, "fp32": 224}
 PEAKS_FALLBACK = {"hbm_gbs": 6650.0}
 
 
@@ -566,6 +570,12 @@ def run_ensemble(args, rank, world, local_rank, dist=None):
     seq_ms_max, _ = aggregate_ranks(dist, seq_ms, float(alive), "cuda")
     value = alive_all * args.steps / (ms_max / 1000.0)
     seq_value = alive_all * args.steps / (seq_ms_max / 1000.0)
+    # roofline of the one persistent kernel: particle state and grid bytes of
+    # a step of every run over the step time
+    nodes = sum(s_.nr * s_.nz for s_ in sims)
+    step_bytes = (n_slots * BYTES_PER_PARTICLE["fp32"] + nodes * BYTES_PER_NODE["fp32"]) * world
+    peaks, peak_src = load_peaks()
+    achieved = step_bytes / (ms_max / args.steps / 1000.0) / 1e9
     if rank == 0:
         print(json.dumps({
             "metric": METRIC, "value": value, "unit": UNIT, "n_gpus": world,
@@ -588,6 +598,12 @@ def run_ensemble(args, rank, world, local_rank, dist=None):
                                    "ms_per_step spans each run's launches on its stream, "
                                    "kernel_ms_per_step sums the kernels alone"},
             "ensemble_over_sequential": value / seq_value,
+            "cell_updates_per_s": nodes * world * args.steps / (ms_max / 1000.0),
+            "roofline": {"bound": "hbm", "achieved": achieved, "peak": peaks.get("hbm_gbs"),
+                         "unit": "GB/s", "frac": achieved / peaks.get("hbm_gbs"),
+                         "traffic": None, "kernel": "k_ensemble (whole step)",
+                         "peak_source": peak_src,
+                         "algorithmic_bytes_per_step": step_bytes},
             "clocks": clk}), flush=True)
     ens.close()
     for s_ in sims:
@@ -697,10 +713,23 @@ def run_adjoint(args, rank, world, local_rank, dist=None):
     fwd_max, particles_all = aggregate_ranks(dist, t["forward_ms"], float(wl.n_particles), "cuda")
     bwd_max, _ = aggregate_ranks(dist, t["backward_ms"], 0.0, "cuda")
     value = particles_all * steps / (fwd_max / 1000.0)
+    # roofline of the forward window: particle state and grid bytes of each
+    # step over the forward device time (the window also captures its inputs)
+    nodes = wl.n_grid_r * wl.n_grid_z
+    step_bytes = (wl.n_particles * BYTES_PER_PARTICLE["fp32"] +
+                  nodes * BYTES_PER_NODE["fp32"]) * world
+    peaks, peak_src = load_peaks()
+    achieved = step_bytes / (fwd_max / steps / 1000.0) / 1e9
     if rank == 0:
         print(json.dumps({
             "metric": METRIC, "value": value, "unit": UNIT, "n_gpus": world,
             "steps": steps, "warmup": steps, "ms_per_step": fwd_max / steps,
+            "cell_updates_per_s": nodes * world * steps / (fwd_max / 1000.0),
+            "roofline": {"bound": "hbm", "achieved": achieved, "peak": peaks.get("hbm_gbs"),
+                         "unit": "GB/s", "frac": achieved / peaks.get("hbm_gbs"),
+                         "traffic": None, "kernel": "forward window (whole step)",
+                         "peak_source": peak_src,
+                         "algorithmic_bytes_per_step": step_bytes},
             "higher_is_better": True, "scaling": "weak", "vs_baseline": None,
             "dtype": "f32+f64acc", "data": "synthetic (seeded)",
             "config": {"workload": wl.name, "window_steps": steps,
