@@ -15,8 +15,7 @@ j_r(i,k+1), at i >= 1 and on the axis cell i = 0.  CPU only."""
 import mpmath as mp
 import numpy as np
 
-mp.mp.dps = 50
-PI = mp.mpf("3.1415926535897932")
+PI = mp.mpf("3.1415926535897932")  # the same constant on both sides
 
 
 def upstream(q, dr, dz, dt, i, k, ao, an, co, cn):
@@ -90,6 +89,11 @@ def cell_local(q, dr, dz, dt, i, ao, an, co, cn):
 
 
 def test_cell_local_deposition_equals_upstream_closed_forms():
+    with mp.workdps(50):  # other modules set mpmath's global precision
+        check()
+
+
+def check():
     rng = np.random.default_rng(23)
     q, dr, dz, dt = mp.mpf("-1.6e-19") * 1e6, mp.mpf("3.9e-4"), mp.mpf("3.9e-4"), \
         mp.mpf("4.6e-13")
