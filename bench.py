@@ -681,6 +681,14 @@ def run_adjoint(args, rank, world, local_rank, dist=None):
         return W.adjoint_gradient(wl, aux, [adj.species(0), adj.species(1)], adj.species(2),
                                   adj.bunch_velocity(2), mean_field=mean_field)
     g_mf = grad(True)
+    # the mean-field terms beyond the default, for the record
+    variants = {"gather_wall_cells": ("gather", "wall_cells"),
+                "gather_walls_wall_cells": ("gather", "walls", "wall_cells")}
+    g_var = {}
+    for name, terms in variants.items():
+        adj.set_jump_terms(*terms)
+        adj.backward()
+        g_var[name] = grad(True)
     adj.set_mode("pathwise")
     adj.backward()
     g_pw = grad(False)
@@ -702,12 +710,14 @@ def run_adjoint(args, rank, world, local_rank, dist=None):
         fd[j] = {"fd": slope, "fd_se": se, "mean_field": g_mf[j], "pathwise": g_pw[j],
                  "rel_err_mean_field": (g_mf[j] - slope) / slope,
                  "rel_err_pathwise": (g_pw[j] - slope) / slope}
+        for name, g in g_var.items():
+            fd[j]["rel_err_" + name] = (g[j] - slope) / slope
     dens = [j for j in params if j < W.N_BUMPS]
     summary = {}
     if dens:
         f = np.array([fd[j]["fd"] for j in dens])
-        for mode in ("mean_field", "pathwise"):
-            a = np.array([fd[j][mode] for j in dens])
+        for mode, g in [("mean_field", g_mf), ("pathwise", g_pw)] + list(g_var.items()):
+            a = np.array([g[j] for j in dens])
             summary["density_block_rel_err_" + mode] = float(np.linalg.norm(a - f) /
                                                              np.linalg.norm(f))
     fwd_max, particles_all = aggregate_ranks(dist, t["forward_ms"], float(wl.n_particles), "cuda")

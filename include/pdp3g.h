@@ -363,14 +363,27 @@ pdp3g_status pdp3g_adjoint_species(pdp3g_adjoint *a, int32_t id, double *l_r, do
 pdp3g_status pdp3g_adjoint_field(pdp3g_adjoint *a, int32_t comp, double *host_out);
 pdp3g_status pdp3g_adjoint_bunch_velocity(pdp3g_adjoint *a, int32_t id, double *l_v);
 /* The upstream radial gather weights jump at cell faces (node-centred
-   components) and cell middles (half-node components), so the loss of a
-   many-particle run moves with the particles' density at the jumps, which a
-   per-particle (pathwise) derivative does not see.  PDP3G_ADJ_MEAN_FIELD
-   (the default) adds each particle's expected share of those jump terms for
-   a particle density uniform inside each cell; PDP3G_ADJ_PATHWISE gives the
-   exact derivative of the particles' piecewise-smooth trajectories. */
+   components) and cell middles (half-node components), and a wall
+   reflection flips u_r or u_z of the particles whose end point lies beyond
+   the wall, so the loss of a many-particle run moves with the particles'
+   density at those jumps, which a per-particle (pathwise) derivative does
+   not see.  PDP3G_ADJ_MEAN_FIELD (the default) adds each particle's expected
+   share of the jump terms of PDP3G_ADJ_DEFAULT_JUMPS; PDP3G_ADJ_PATHWISE
+   gives the exact derivative of the particles' piecewise-smooth
+   trajectories. */
 enum { PDP3G_ADJ_MEAN_FIELD = 0, PDP3G_ADJ_PATHWISE = 1 };
 pdp3g_status pdp3g_adjoint_set_mode(pdp3g_adjoint *a, int32_t mode);
+/* The mean-field terms one by one (a bit mask; 0 = pathwise):
+   PDP3G_ADJ_GATHER_JUMPS  the gather weights' jumps, for a particle density
+                           uniform inside each cell;
+   PDP3G_ADJ_WALL_JUMPS    the momentum jumps of the wall reflections;
+   PDP3G_ADJ_WALL_CELLS    the walls leave the axis cell's and the last
+                           radial cell's particles in the half next to the
+                           other cells (r >= dr/2, r <= r_max - dr/2), twice
+                           as dense; without it those cells count as full. */
+enum { PDP3G_ADJ_GATHER_JUMPS = 1, PDP3G_ADJ_WALL_JUMPS = 2, PDP3G_ADJ_WALL_CELLS = 4,
+       PDP3G_ADJ_DEFAULT_JUMPS = PDP3G_ADJ_GATHER_JUMPS };
+pdp3g_status pdp3g_adjoint_set_jump_terms(pdp3g_adjoint *a, uint32_t terms);
 /* device time of the last forward and backward calls */
 pdp3g_status pdp3g_adjoint_timing(pdp3g_adjoint *a, double *forward_ms, double *backward_ms);
 int64_t pdp3g_adjoint_bytes(pdp3g_adjoint *a);

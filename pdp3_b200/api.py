@@ -138,6 +138,7 @@ EXPORTS = [
     ("pdp3g_adjoint_bunch_velocity", _I32, [_VP, _I32, _D]),
     ("pdp3g_adjoint_timing", _I32, [_VP, _D, _D]),
     ("pdp3g_adjoint_set_mode", _I32, [_VP, _I32]),
+    ("pdp3g_adjoint_set_jump_terms", _I32, [_VP, ctypes.c_uint32]),
     ("pdp3g_adjoint_bytes", ctypes.c_int64, [_VP]),
     ("pdp3g_adjoint_destroy", None, [_VP]),
 ]
@@ -533,10 +534,19 @@ class Adjoint:
         return v.value
 
     def set_mode(self, mode):
-        """"mean_field" (default: adds the expected gather-jump terms) or
+        """"mean_field" (default: adds the expected jump terms) or
         "pathwise" (the exact derivative of each particle's trajectory)."""
         self.sim._check(self.L.pdp3g_adjoint_set_mode(
             self.h, {"mean_field": 0, "pathwise": 1}[mode]), "adjoint_set_mode")
+
+    def set_jump_terms(self, *terms):
+        """The mean-field terms one by one: any of "gather" (the gather
+        weights' jumps), "walls" (the momentum jumps of wall reflections),
+        "wall_cells" (the axis and last radial cells hold their particles in
+        the half the walls leave them); none = pathwise."""
+        bits = {"gather": 1, "walls": 2, "wall_cells": 4}
+        self.sim._check(self.L.pdp3g_adjoint_set_jump_terms(
+            self.h, sum(bits[t] for t in set(terms))), "adjoint_set_jump_terms")
 
     def timing(self):
         f, b = ctypes.c_double(), ctypes.c_double()

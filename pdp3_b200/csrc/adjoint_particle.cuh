@@ -32,7 +32,11 @@ struct Consts {
   T kphi, kz, kr;  // deposition prefactors per unit weight
   int nr, nz;   // grid nodes
   int bunch;    // 1: outer walls remove the particle
-  int face;     // 1: add the expected jump terms of the radial gather weights
+  int face;     // bit 0: expected jump terms of the radial gather weights;
+                // bit 1: expected jump terms of the wall reflections;
+                // bit 2: the gather terms with the wall cells' particles in
+                //        the half of the cell that the walls leave them
+                // (PDP3G_ADJ_GATHER_JUMPS, _WALL_JUMPS, _WALL_CELLS)
 };
 
 template <typename T>
@@ -429,14 +433,21 @@ PDP3_HD void piece_outputs(const Consts<T> &C, const Tape<T> &tp, int p, T out[4
 //   half-node (E_r, H_phi, H_z), i >= 1: the jump at the cell middle,
 //     f_i (2i + 1) / (2 (i + 1)(i + 2)).
 // f_j is the node row's value interpolated in z with the particle's weights.
+// wall_cells: the walls reflect whatever ends a step at r < dr/2 or
+// r > r_max - dr/2, so the axis cell and the last cell hold their particles
+// in the half next to the other cells, twice as dense: there a particle
+// carries the whole jump of the face on that side and none of the other.
 template <typename T>
-PDP3_HD T radial_jump(const Tape<T> &tp, T f0, T f1, T f2, T f3, T wz0, T wz1, bool rh) {
+PDP3_HD T radial_jump(const Tape<T> &tp, T f0, T f1, T f2, T f3, T wz0, T wz1, bool rh,
+                      bool wall_cells, int nr) {
   const int i = tp.i;
   const T lo = wz0 * f0 + wz1 * f2, hi = wz0 * f1 + wz1 * f3;
   if (!rh) {
     // nodes i, i+1: top face jump uses f_{i+1}, bottom face (i >= 1) f_i
     const T top = hi / T(i + 2);
     const T bottom = i >= 1 ? lo / T(i + 1) : T(0);
+    if (wall_cells && i == 0) return top;
+    if (wall_cells && i == nr - 2) return bottom;
     return T(0.5) * (top + bottom);
   }
   if (i < 1) return T(0);
@@ -460,7 +471,64 @@ PDP3_HD void gather_rev(const Consts<T> &C, const Tape<T> &tp, const T f[4], boo
   l_a += lv * (wz0 * (f0 * dwr0 + f1 * dwr1) + wz1 * (f2 * dwr0 + f3 * dwr1));
   // d wz0 / db = -1, d wz1 / db = +1 for both the node and the half-node weights
   l_b += lv * (-(f0 * wr0 + f1 * wr1) + (f2 * wr0 + f3 * wr1));
-  if (C.face) l_a += lv * radial_jump(tp, f0, f1, f2, f3, wz0, wz1, rh);
+  if (C.face & 1) l_a += lv * radial_jump(tp, f0, f1, f2, f3, wz0, wz1, rh, C.face & 4, C.nr);
+}
+
+// The walls reflect a particle whose end point lies beyond them: the end
+// point is mirrored (continuous where it meets the wall) and u_r or u_z
+// changes sign, a jump of the output momentum at the start offset a* (b*)
+// whose end point lies on the wall.  The deposits are continuous there.  A
+// particle carries per unit offset S(a*+) - S(a*-) for each such a* inside
+// its cell, times the expected density there, S the adjoint-weighted output
+// momentum with the end point on the wall:
+//   radial: rr = sqrt(x^2 + dy^2), x = i + a + dr_h; the axis reflects where
+//     rr < 1/2 - dr_h (thresholds x = +-s), the outer wall where
+//     rr > nr - 3/2 - dr_h; S(refl) - S(unrefl) = -2 u_r (ct l_ur' + st l_uphi')
+//     with (ct, st) the rotation of the end point on the wall;
+//   z: b2 = b + 2 dz_h; S(refl) - S(unrefl) = -2 u_z l_uz'.
+// Density: uniform inside a cell, except that no particle stays beyond a
+// wall (r < dr/2, z < dz/2, r > r_max - dr/2, z > z_max - dz/2: the first step
+// reflects it, and injected bunch particles start at z >= dz/2), so a wall
+// cell holds its particles in its inner half at twice the density, and a
+// threshold in its outer half carries nothing.  Bunch particles that leave
+// through the outer walls are removed, which has no linear jump; those walls
+// count for plasma species only.
+template <typename T>
+PDP3_HD T wall_density(T t, bool low_wall, bool high_wall) {
+  if (!(t > T(0) && t < T(1))) return T(0);
+  if (low_wall) return t > T(0.5) ? T(2) : T(0);
+  if (high_wall) return t < T(0.5) ? T(2) : T(0);
+  return T(1);
+}
+
+template <typename T>
+PDP3_HD T radial_wall_dS(const Tape<T> &tp, const T l_uout[3], T x2w) {
+  const T r2w = sqrt(x2w * x2w + tp.dy * tp.dy);
+  return T(-2) * tp.up[0] * (x2w / r2w * l_uout[0] + tp.dy / r2w * l_uout[1]);
+}
+
+template <typename T>
+PDP3_HD void wall_jumps(const Consts<T> &C, const Tape<T> &tp, const T l_uout[3], T &l_a,
+                        T &l_b) {
+  const bool axis_cell = tp.i == 0, outer_cell = tp.i == C.nr - 2;
+  const bool left_cell = tp.k == 0, right_cell = tp.k == C.nz - 2;
+  const T off = T(tp.i) + tp.dr_h, dy2 = tp.dy * tp.dy;
+  const T Ra = T(0.5) - tp.dr_h;
+  if (Ra * Ra > dy2) {
+    const T s = sqrt(Ra * Ra - dy2), dS = radial_wall_dS(tp, l_uout, T(0.5));
+    // rr rises with a at x = s (reflected below a*), falls at x = -s
+    l_a -= dS * wall_density(s - off, axis_cell, outer_cell);
+    l_a += dS * wall_density(-s - off, axis_cell, outer_cell);
+  }
+  if (!C.bunch) {
+    const T Ro = T(C.nr) - T(1.5) - tp.dr_h;
+    const T ao = sqrt(Ro * Ro - dy2) - off;
+    l_a += radial_wall_dS(tp, l_uout, T(C.nr) - T(1.5)) * wall_density(ao, axis_cell, outer_cell);
+  }
+  const T dSz = T(-2) * tp.up[2] * l_uout[2];
+  l_b -= dSz * wall_density(T(0.5) - T(tp.k) - 2 * tp.dz_h, left_cell, right_cell);
+  if (!C.bunch)
+    l_b += dSz * wall_density(T(C.nz) - T(1.5) - T(tp.k) - 2 * tp.dz_h, left_cell, right_cell);
 }
 
 // ----------------------------------------------------------------- reverse
@@ -478,6 +546,7 @@ PDP3_HD void reverse(const Consts<T> &C, const Tape<T> &tp, T l_an, T l_bn, cons
   l_a = 0;
   l_b = 0;
   l_w = 0;
+  if (C.face & 2) wall_jumps(C, tp, l_uout, l_a, l_b);
   // ---- outputs: an = A - shift, bn = B - shift; rotation of u
   T l_A = tp.alive_now ? l_an : T(0), l_B = tp.alive_now ? l_bn : T(0);
   T l_x2 = 0, l_r2 = 0;

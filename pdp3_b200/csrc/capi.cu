@@ -1863,7 +1863,7 @@ struct pdp3g_adjoint {
                                                // recomputed interval, slot j = step j's input
   std::vector<double> cap_t;
   bool have_forward = false;
-  int face_terms = 1;
+  int face_terms = PDP3G_ADJ_DEFAULT_JUMPS;
   double loss = 0;
   float fwd_ms = 0, bwd_ms = 0;
   cudaEvent_t ev0 = nullptr, ev1 = nullptr;
@@ -2224,6 +2224,13 @@ int64_t pdp3g_adjoint_bytes(pdp3g_adjoint *a) { return a ? a->bytes : 0; }
 
 pdp3g_status pdp3g_adjoint_set_mode(pdp3g_adjoint *a, int32_t mode) {
   if (!a || (mode != PDP3G_ADJ_MEAN_FIELD && mode != PDP3G_ADJ_PATHWISE)) return PDP3G_INVALID_ARG;
-  a->face_terms = mode == PDP3G_ADJ_MEAN_FIELD;
+  a->face_terms = mode == PDP3G_ADJ_MEAN_FIELD ? PDP3G_ADJ_DEFAULT_JUMPS : 0;
+  return PDP3G_OK;
+}
+
+pdp3g_status pdp3g_adjoint_set_jump_terms(pdp3g_adjoint *a, uint32_t terms) {
+  const uint32_t all = PDP3G_ADJ_GATHER_JUMPS | PDP3G_ADJ_WALL_JUMPS | PDP3G_ADJ_WALL_CELLS;
+  if (!a || (terms & ~all)) return PDP3G_INVALID_ARG;
+  a->face_terms = (int)terms;  // the bits of adj::Consts::face
   return PDP3G_OK;
 }

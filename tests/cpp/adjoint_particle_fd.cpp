@@ -9,7 +9,10 @@
 // 2. mean field: for particles spread uniformly over whole cells, the
 //    pathwise gather derivative plus radial_jump() equals the central
 //    difference of the particles' mean gathered value under a common radial
-//    shift, which includes the weights' jumps at faces and cell middles.
+//    shift, which includes the weights' jumps at faces and cell middles
+//    (also for windows that start or end in the half of a wall cell that the
+//    walls leave to particles, with the wall-cell share);
+// 3. the same for the momentum jumps of the wall reflections (wall_jumps()).
 // Prints one line per check and exits non-zero on failure.
 #include <cmath>
 #include <cstdio>
@@ -149,7 +152,8 @@ static int pathwise() {
 }
 
 // gathered value of a component at radial coordinate x (cells), fixed z weights
-static T gather_at(T x, const T *F0, const T *F1, T b, bool rh, bool zh, T *dG, T *jump) {
+static T gather_at(T x, const T *F0, const T *F1, T b, bool rh, bool zh, bool wall_cells, int nr,
+                   T *dG, T *jump) {
   Tape<T> tp;
   tp.i = (int)std::ceil(x) - 1;
   tp.a = x - tp.i;
@@ -161,50 +165,134 @@ static T gather_at(T x, const T *F0, const T *F1, T b, bool rh, bool zh, T *dG, 
   const T *wr = rh ? tp.wrh : tp.wrn, *dwr = rh ? tp.dwrh : tp.dwrn;
   const T *wz = zh ? tp.wzh : tp.wzn;
   if (dG) *dG = wz[0] * (f[0] * dwr[0] + f[1] * dwr[1]) + wz[1] * (f[2] * dwr[0] + f[3] * dwr[1]);
-  if (jump) *jump = radial_jump(tp, f[0], f[1], f[2], f[3], wz[0], wz[1], rh);
+  if (jump)
+    *jump = radial_jump(tp, f[0], f[1], f[2], f[3], wz[0], wz[1], rh, wall_cells, nr);
   return wz[0] * (f[0] * wr[0] + f[1] * wr[1]) + wz[1] * (f[2] * wr[0] + f[3] * wr[1]);
 }
 
+// Windows of whole cells; with wall_cells, windows that start in the axis
+// cell at r = dr/2 or end in the last cell (nr - 2) at r = r_max - dr/2, the
+// parts of those cells that the walls leave to particles.
 static int mean_field() {
   double worst = 0;
   int cases = 0;
-  for (int trial = 0; trial < 24; trial++) {
+  for (int trial = 0; trial < 36; trial++) {
     T F0[64], F1[64];
     for (int j = 0; j < 64; j++) { F0[j] = U(-1, 1) + 2; F1[j] = U(-1, 1) + 2; }
     const bool rh = trial % 2, zh = (trial / 2) % 2;
-    const int i0 = 1 + (int)(rng() % 20), i1 = i0 + 1 + (int)(rng() % 8);
+    const int wall = trial < 24 ? 0 : 1 + trial % 3 % 2;  // 1: axis cell, 2: last cell
+    int i0 = 1 + (int)(rng() % 20), i1 = i0 + 1 + (int)(rng() % 8);
+    if (wall == 1) i0 = 0;
+    const int nr = wall == 2 ? i1 + 1 : 64;  // with wall == 2 the window ends in cell nr - 2
     const T b = U(0.05, 0.95);
     // midpoint rule with a whole number of points per cell and shifts of a
     // whole number of point spacings: exactly that many points cross each
     // face, so the differences resolve the jumps without quadrature error.
     // The weights also have kinks at the faces, which make the central
     // difference O(h); Richardson extrapolation over h and 2h removes that.
-    const int per_cell = 50000, n = per_cell * (i1 - i0);
+    const int per_cell = 50000;
+    const int q0 = wall == 1 ? per_cell / 2 : 0;
+    const int q1 = per_cell * (i1 - i0) - (wall == 2 ? per_cell / 2 : 0);
+    const int n = q1 - q0;
     const T h = 50.0 / per_cell;
     double mp = 0, mm = 0, mp2 = 0, mm2 = 0, est = 0;
-    for (int q = 0; q < n; q++) {
+    for (int q = q0; q < q1; q++) {
       const T x = i0 + (q + 0.5) / per_cell;
       T dG, jump;
-      gather_at(x, F0, F1, b, rh, zh, &dG, &jump);
+      gather_at(x, F0, F1, b, rh, zh, wall != 0, nr, &dG, &jump);
       est += dG + jump;
-      mp += gather_at(x + h, F0, F1, b, rh, zh, nullptr, nullptr);
-      mm += gather_at(x - h, F0, F1, b, rh, zh, nullptr, nullptr);
-      mp2 += gather_at(x + 2 * h, F0, F1, b, rh, zh, nullptr, nullptr);
-      mm2 += gather_at(x - 2 * h, F0, F1, b, rh, zh, nullptr, nullptr);
+      mp += gather_at(x + h, F0, F1, b, rh, zh, false, nr, nullptr, nullptr);
+      mm += gather_at(x - h, F0, F1, b, rh, zh, false, nr, nullptr, nullptr);
+      mp2 += gather_at(x + 2 * h, F0, F1, b, rh, zh, false, nr, nullptr, nullptr);
+      mm2 += gather_at(x - 2 * h, F0, F1, b, rh, zh, false, nr, nullptr, nullptr);
     }
     const double d1 = (mp - mm) / (2 * h) / n, d2 = (mp2 - mm2) / (4 * h) / n;
     const double fd = 2 * d1 - d2, ad = est / n;
     const double e = std::fabs(fd - ad) / std::fmax(std::fabs(fd), 1e-3);
     if (e > worst) worst = e;
-    if (getenv("ADJ_VERBOSE")) printf("  rh %d zh %d cells [%d,%d) fd %.6g est %.6g\n", rh, zh, i0, i1, fd, ad);
+    if (getenv("ADJ_VERBOSE"))
+      printf("  rh %d zh %d wall %d cells [%d,%d) fd %.6g est %.6g\n", rh, zh, wall, i0, i1, fd,
+             ad);
     cases++;
   }
   printf("mean field: %d windows, worst rel err %.3g\n", cases, worst);
   return worst < 1e-4 ? 0 : 1;
 }
 
+// 3. wall reflections: with zero fields and adjoints on the end point and the
+//    momentum only, S = sum(adjoint x output) is piecewise smooth in the start
+//    offset a (b) with jumps where the end point meets a wall, so the mean of
+//    the reverse's l_a (l_b) with the wall terms on over the part of the cell
+//    that particles occupy ([1/2, 1) next to the axis and z = 0, [0, 1/2)
+//    next to the outer walls, else [0, 1)) equals the difference quotient of S
+//    over that part (to the midpoint rule's O(1/n) at the kinks; the jumps
+//    are O(1) here).
+static int wall_mean_field() {
+  double worst = 0;
+  int cases = 0, with_jump = 0;
+  for (int trial = 0; trial < 60; trial++) {
+    Consts<T> C;
+    C.ke = 0.3; C.kb = 0.7; C.cz = 0.13; C.kphi = 1.3; C.kz = 0.9; C.kr = 1.1;
+    C.nr = 40; C.nz = 60; C.face = 2;
+    In in = {};
+    const int kind = trial % 3;  // 0: axis and z = 0, 1: outer walls, 2: cell 1 and middle
+    C.cr = trial % 6 == 3 ? 2.0 : 0.11;  // on the axis: the threshold at x < 0 too
+    C.bunch = trial % 4 == 3 && kind != 1;  // a bunch particle is removed at the outer walls
+    in.i = kind == 0 ? 0 : (kind == 1 ? C.nr - 2 : 1);
+    in.k = kind == 0 ? 0 : (kind == 1 ? C.nz - 2 : 20);
+    in.b = U(0.1, 0.9);
+    in.a = U(0.1, 0.9);
+    in.w = 1;
+    const T sgn = kind == 1 ? 1 : -1;
+    in.u[0] = sgn * U(1, 8);
+    in.u[1] = U(-1, 1);
+    in.u[2] = sgn * U(1, 8);
+    if (C.cr > 1) {
+      // velocity (-0.6, +-0.795, 0.02) c: the x < 0 threshold lies at a = 0.6
+      const T v[3] = {-0.6, 0.795 * (trial % 4 == 3 ? 1 : -1), 0.02};
+      const T g = 1 / std::sqrt(1 - v[0] * v[0] - v[1] * v[1] - v[2] * v[2]);
+      for (int c = 0; c < 3; c++) in.u[c] = g * v[c];
+    }
+    LamOut L = {};
+    L.an = U(-1, 1); L.bn = U(-1, 1);
+    for (int c = 0; c < 3; c++) L.u[c] = U(-1, 1);
+    for (int dir = 0; dir < 2; dir++) {
+      const T lo_edge = kind == 0 ? 0.5 : 0, hi_edge = kind == 1 ? 0.5 : 1;
+      const int n = 20000;
+      double mean = 0;
+      for (int q = 0; q < n; q++) {
+        In x = in;
+        (dir == 0 ? x.a : x.b) = lo_edge + (hi_edge - lo_edge) * (q + 0.5) / n;
+        Tape<T> tp;
+        objective(C, x, L, &tp);
+        T la, lb, lu[3], lw, lfe[3][4], lfh[3][4];
+        reverse(C, tp, L.an, L.bn, L.u, L.jphi, L.piece, la, lb, lu, lw, lfe, lfh);
+        mean += (dir == 0 ? la : lb);
+      }
+      mean /= n;
+      In lo = in, hi = in;
+      (dir == 0 ? lo.a : lo.b) = lo_edge + 1e-13;
+      (dir == 0 ? hi.a : hi.b) = hi_edge - 1e-13;
+      Tape<T> tlo, thi;
+      const double want =
+          (objective(C, hi, L, &thi) - objective(C, lo, L, &tlo)) / (hi_edge - lo_edge);
+      if (thi.sr != tlo.sr || thi.sz != tlo.sz) with_jump++;
+      const double e = std::fabs(mean - want) / std::fmax(std::fabs(want), 1.0);
+      if (e > worst) worst = e;
+      if (getenv("ADJ_VERBOSE"))
+        printf("  trial %d dir %d i %d k %d bunch %d: dS/d(offset) %.9g mean l %.9g\n", trial,
+               dir, in.i, in.k, C.bunch, want, mean);
+      cases++;
+    }
+  }
+  printf("wall mean field: %d cells (%d with a reflection threshold), worst rel err %.3g\n",
+         cases, with_jump, worst);
+  return (worst < 1e-4 && with_jump > 30) ? 0 : 1;
+}
+
 int main() {
   const int a = pathwise();
   const int b = mean_field();
-  return a | b;
+  const int c = wall_mean_field();
+  return a | b | c;
 }

@@ -11,6 +11,9 @@
   at this size (few particles cross a jump of the gather weights).
 * Forward + backward leaves the state the forward ended in, and the adjoint
   rejects what it does not support.
+* The mean-field terms one by one: none is the pathwise derivative, the
+  gather terms alone are the default mean field, the wall terms change the
+  gradient, unknown bits are rejected.
 """
 import numpy as np
 import pytest
@@ -128,3 +131,29 @@ def test_backward_restores_forward_end_state_and_rejects_misuse():
     with pytest.raises(api.Pdp3gError):
         api.Adjoint(s64, 10, 5, PROBE)  # the FP64 form has no adjoint
     s64.close()
+
+
+def test_jump_terms_select_the_mean_field_parts():
+    th = W.adjoint_theta()
+    wl, aux = W.AdjointFamily(th, **SMALL).workload(th)
+    sim = api.from_workload(wl, precision="fp32")
+    adj = api.Adjoint(sim, 40, 15, PROBE)
+    adj.forward()
+    grads = {}
+    for name, select in [("pathwise", lambda: adj.set_mode("pathwise")),
+                         ("none", lambda: adj.set_jump_terms()),
+                         ("default", lambda: adj.set_mode("mean_field")),
+                         ("gather", lambda: adj.set_jump_terms("gather")),
+                         ("all", lambda: adj.set_jump_terms("gather", "walls", "wall_cells"))]:
+        select()
+        adj.backward()
+        grads[name] = np.array(W.adjoint_gradient(
+            wl, aux, [adj.species(0), adj.species(1)], adj.species(2), adj.bunch_velocity(2)))
+    # the FP64 adjoint grids sum by atomics, whose order varies run to run
+    for a, b in (("none", "pathwise"), ("gather", "default")):
+        assert np.allclose(grads[a], grads[b], rtol=1e-9, atol=0), (a, b)
+    assert not np.allclose(grads["all"], grads["gather"], rtol=1e-6, atol=0)
+    with pytest.raises(api.Pdp3gError):
+        sim._check(adj.L.pdp3g_adjoint_set_jump_terms(adj.h, 8), "adjoint_set_jump_terms")
+    adj.close()
+    sim.close()
