@@ -1465,6 +1465,7 @@ struct pdp3g_ensemble {
   std::vector<EnsRun> h_runs;
   int blocks_per_sm = 0;
   int max_blocks_per_sm = 0;
+  int pusher = -1;  // the pusher every run uses (compiled into the kernel), or -1
   double budget_ms = 0;
   long long budget_host = 0;  // cycles, source of the copy to d_budget
   long long clock_khz = 0;
@@ -1595,7 +1596,10 @@ pdp3g_status pdp3g_ensemble_create(pdp3g_ctx *const *runs, int32_t n_runs, pdp3g
     if (c->cfg.sort_interval > 0 &&
         (e->sort_interval == 0 || c->cfg.sort_interval < e->sort_interval))
       e->sort_interval = c->cfg.sort_interval;
-  e->max_blocks_per_sm = ensemble_max_blocks_per_sm();
+  e->pusher = e->runs[0]->cfg.pusher;
+  for (auto *c : e->runs)
+    if (c->cfg.pusher != e->pusher) e->pusher = -1;
+  e->max_blocks_per_sm = ensemble_max_blocks_per_sm(e->pusher);
   if (e->max_blocks_per_sm <= 0) return bail(PDP3G_CUDA_ERROR, "ensemble kernel does not fit");
   e->blocks_per_sm = e->max_blocks_per_sm;
   *out = e;
@@ -1620,7 +1624,7 @@ static pdp3g_status ens_launch(pdp3g_ensemble *e, bool allow_graph) {
     }
     if (!e->exec) {
       cudaError_t c1 = cudaStreamBeginCapture(e->stream, cudaStreamCaptureModeThreadLocal);
-      cudaError_t c2 = c1 == cudaSuccess ? ensemble_launch(e->dev, blocks, e->stream) : c1;
+      cudaError_t c2 = c1 == cudaSuccess ? ensemble_launch(e->dev, blocks, e->pusher, e->stream) : c1;
       cudaGraph_t g = nullptr;
       cudaError_t c3 = c1 == cudaSuccess ? cudaStreamEndCapture(e->stream, &g) : c1;
       // the captured node must keep the cooperative attribute: the kernel's
@@ -1658,7 +1662,7 @@ static pdp3g_status ens_launch(pdp3g_ensemble *e, bool allow_graph) {
       return PDP3G_OK;
     }
   }
-  EK(ensemble_launch(e->dev, blocks, e->stream));
+  EK(ensemble_launch(e->dev, blocks, e->pusher, e->stream));
   return PDP3G_OK;
 }
 

@@ -64,7 +64,10 @@ __device__ void ens_inject(const EnsembleDev &E, const EnsSpecies &sp) {
 }
 
 // The step count is read from E.status[2] (written before each launch), so
-// one captured graph serves every segment length.
+// one captured graph serves every segment length.  PUSHER: the pusher of
+// every run when they share one (compiled in, as in k_push_deposit_f32),
+// -1 for runs with different pushers (chosen per species at run time).
+template <int PUSHER>
 __global__ void __launch_bounds__(F32_THREADS, F32_MIN_BLOCKS) k_ensemble(EnsembleDev E) {
   const int nsteps = *(volatile int *)&E.status[2];
   const long long budget = *(volatile const long long *)E.budget_cycles;
@@ -126,7 +129,7 @@ __global__ void __launch_bounds__(F32_THREADS, F32_MIN_BLOCKS) k_ensemble(Ensemb
       }
       __syncthreads();
       for (long long c = first; c < ce; c += gridDim.x)
-        f32_chunk<false>(desc.g, desc.s, SpeciesOut{}, desc.pusher, c - cb, sm);
+        f32_chunk<false, PUSHER>(desc.g, desc.s, SpeciesOut{}, desc.pusher, c - cb, sm);
     }
     grid.sync();
     // ---- phase C: E update, t += dt
@@ -146,17 +149,26 @@ __global__ void __launch_bounds__(F32_THREADS, F32_MIN_BLOCKS) k_ensemble(Ensemb
   }
 }
 
-int ensemble_max_blocks_per_sm() {
+static void (*ensemble_kernel(int pusher))(EnsembleDev) {
+  switch (pusher) {
+    case 0: return k_ensemble<0>;
+    case 1: return k_ensemble<1>;
+    case 2: return k_ensemble<2>;
+    default: return k_ensemble<-1>;
+  }
+}
+
+int ensemble_max_blocks_per_sm(int pusher) {
   int nb = 0;
-  if (cudaOccupancyMaxActiveBlocksPerMultiprocessor(&nb, k_ensemble, F32_THREADS, 0) !=
-      cudaSuccess)
+  if (cudaOccupancyMaxActiveBlocksPerMultiprocessor(&nb, ensemble_kernel(pusher), F32_THREADS,
+                                                    0) != cudaSuccess)
     return 0;
   return nb;
 }
 
 // One cooperative launch of E.status[2] steps (graph capture of this call is
-// done by the caller).
-cudaError_t ensemble_launch(const EnsembleDev &E, int blocks, cudaStream_t st) {
+// done by the caller); pusher: the runs' common pusher, or -1.
+cudaError_t ensemble_launch(const EnsembleDev &E, int blocks, int pusher, cudaStream_t st) {
   cudaLaunchConfig_t cfg = {};
   cfg.gridDim = dim3(blocks);
   cfg.blockDim = dim3(F32_THREADS);
@@ -167,7 +179,7 @@ cudaError_t ensemble_launch(const EnsembleDev &E, int blocks, cudaStream_t st) {
   attr[0].val.cooperative = 1;
   cfg.attrs = attr;
   cfg.numAttrs = 1;
-  return cudaLaunchKernelEx(&cfg, k_ensemble, E);
+  return cudaLaunchKernelEx(&cfg, ensemble_kernel(pusher), E);
 }
 
 }  // namespace pdp3g

@@ -168,8 +168,9 @@ struct EnsembleDev {
   const long long *budget_cycles;  // device: 0 = none (read at launch, so graphs see updates)
 };
 
-int ensemble_max_blocks_per_sm();
-cudaError_t ensemble_launch(const EnsembleDev &E, int blocks, cudaStream_t st);
+// pusher: the pusher every run uses, or -1 when they differ
+int ensemble_max_blocks_per_sm(int pusher);
+cudaError_t ensemble_launch(const EnsembleDev &E, int blocks, int pusher, cudaStream_t st);
 
 // byte offsets of the radix sort's scratch (sort.cu)
 struct SortLayout {
