@@ -520,8 +520,8 @@ PDP3_HD void wall_jumps(const Consts<T> &C, const Tape<T> &tp, const T l_uout[3]
     l_a -= dS * wall_density(s - off, axis_cell, outer_cell);
     l_a += dS * wall_density(-s - off, axis_cell, outer_cell);
   }
-  if (!C.bunch) {
-    const T Ro = T(C.nr) - T(1.5) - tp.dr_h;
+  const T Ro = T(C.nr) - T(1.5) - tp.dr_h;
+  if (!C.bunch && Ro * Ro > dy2) {
     const T ao = sqrt(Ro * Ro - dy2) - off;
     l_a += radial_wall_dS(tp, l_uout, T(C.nr) - T(1.5)) * wall_density(ao, axis_cell, outer_cell);
   }
