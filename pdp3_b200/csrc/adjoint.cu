@@ -159,7 +159,9 @@ __device__ __forceinline__ bool warp_seg_sum(int key, float (&v)[N]) {
 // consecutive grids each).  Each thread takes one particle; the 24
 // field-node adjoints of a warp's particles are summed over runs of lanes
 // that share their gather nodes (particles sorted by cell) and each run adds
-// its totals to the FP64 grids.  Warps are independent.
+// its totals to the FP64 grids.  Warps are independent.  WALLS: whether the
+// wall-reflection jump terms (face bit 1) are compiled in.
+template <bool WALLS>
 __global__ void __launch_bounds__(ADJ_THREADS, ADJ_MIN_BLOCKS) k_adj_particles(
     GridDev g, const float *E3, const float *Hh3, AdjSpeciesDev S, AdjGrids A, int face) {
   const int ncz = g.nz - 1;
@@ -241,8 +243,8 @@ __global__ void __launch_bounds__(ADJ_THREADS, ADJ_MIN_BLOCKS) k_adj_particles(
       }
       const float l_uout[3] = {S.lur[p], S.luphi[p], S.luz[p]};
       float l_a, l_b, l_u[3], l_w, l_fe[3][4], l_fh[3][4];
-      adj::reverse(C, tp, S.la[p], S.lb[p], l_uout, l_jphi, l_piece, l_a, l_b, l_u, l_w, l_fe,
-                   l_fh);
+      adj::reverse<float, WALLS>(C, tp, S.la[p], S.lb[p], l_uout, l_jphi, l_piece, l_a, l_b,
+                                 l_u, l_w, l_fe, l_fh);
       S.la[p] = l_a;
       S.lb[p] = l_b;
       S.lur[p] = l_u[0];
@@ -354,16 +356,16 @@ void adj_launch_particles(const GridDev &g, const float *E3, const float *Hh3,
                           const AdjSpeciesDev &S, const AdjGrids &A, int face, cudaStream_t st) {
   if (S.st.n <= 0) return;
   const long long nchunks = (S.st.n + ADJ_THREADS - 1) / ADJ_THREADS;
+  auto kernel = (face & 2) ? k_adj_particles<true> : k_adj_particles<false>;
   int bpsm = 0;
-  if (cudaOccupancyMaxActiveBlocksPerMultiprocessor(&bpsm, k_adj_particles, ADJ_THREADS, 0) !=
+  if (cudaOccupancyMaxActiveBlocksPerMultiprocessor(&bpsm, kernel, ADJ_THREADS, 0) !=
           cudaSuccess || bpsm < 1)
     bpsm = 1;
   int dev = 0, nsm = 148;
   cudaGetDevice(&dev);
   cudaDeviceGetAttribute(&nsm, cudaDevAttrMultiProcessorCount, dev);
   const long long blocks = std::min<long long>(nchunks, (long long)bpsm * nsm);
-  k_adj_particles<<<(int)std::max<long long>(blocks, 1), ADJ_THREADS, 0, st>>>(g, E3, Hh3, S, A,
-                                                                               face);
+  kernel<<<(int)std::max<long long>(blocks, 1), ADJ_THREADS, 0, st>>>(g, E3, Hh3, S, A, face);
 }
 
 void adj_launch_inject(const AdjSpeciesDev &S, long long start, long long count, double dt,

@@ -537,7 +537,9 @@ PDP3_HD void wall_jumps(const Consts<T> &C, const Tape<T> &tp, const T l_uout[3]
 // (adjoint of J_phi at (i1,k1),(i1+1,k1),(i1,k1+1),(i1+1,k1+1)), l_piece[p][4]
 // (adjoint of J_z(ci,ck), J_z(ci+1,ck), J_r(ci,ck), J_r(ci,ck+1) per piece).
 // Outputs: l_a, l_b, l_u[3], l_w, l_fe[3][4], l_fh[3][4].
-template <typename T>
+// WALLS = false compiles the wall terms out (C.face bit 1 is then ignored),
+// which keeps them from costing registers where they are off.
+template <typename T, bool WALLS = true>
 PDP3_HD void reverse(const Consts<T> &C, const Tape<T> &tp, T l_an, T l_bn, const T l_uout[3],
                      const T l_jphi[4], const T l_piece[3][4], T &l_a, T &l_b, T l_u[3], T &l_w,
                      T l_fe[3][4], T l_fh[3][4]) {
@@ -546,7 +548,7 @@ PDP3_HD void reverse(const Consts<T> &C, const Tape<T> &tp, T l_an, T l_bn, cons
   l_a = 0;
   l_b = 0;
   l_w = 0;
-  if (C.face & 2) wall_jumps(C, tp, l_uout, l_a, l_b);
+  if (WALLS && (C.face & 2)) wall_jumps(C, tp, l_uout, l_a, l_b);
   // ---- outputs: an = A - shift, bn = B - shift; rotation of u
   T l_A = tp.alive_now ? l_an : T(0), l_B = tp.alive_now ? l_bn : T(0);
   T l_x2 = 0, l_r2 = 0;
