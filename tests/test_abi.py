@@ -45,6 +45,8 @@ def test_status_strings_and_null_arguments():
     assert L.pdp3g_step(None, 1) == 1
     assert L.pdp3g_sync(None) == 1
     assert L.pdp3g_species_size(None, 0) == -1
+    assert L.pdp3g_adjoint_set_mode(None, 0) == 1
+    assert L.pdp3g_adjoint_set_jump_terms(None, 1) == 1
 
 
 def test_invalid_config_rejected_before_device_use():
