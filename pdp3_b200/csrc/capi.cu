@@ -40,6 +40,10 @@ struct pdp3g_ctx {
   int n_sm = 148;
   cudaStream_t stream = nullptr;
   cudaStream_t stream_up = nullptr;  // pdp3g_exchange_species' host->device copies
+  // the particle phase steps species 1, 3, ... on stream_side beside the
+  // others on stream (fork and join events on stream)
+  cudaStream_t stream_side = nullptr;
+  cudaEvent_t ev_fork = nullptr, ev_join = nullptr;
   cudaEvent_t ev_chunk = nullptr, ev_up = nullptr;
   double dr = 0, dz = 0, t = 0;
   double *grid_mem = nullptr;
@@ -247,7 +251,10 @@ pdp3g_status pdp3g_create(const pdp3g_config *cfg, pdp3g_ctx **out) {
     pdp3g_destroy(ctx);
     return s;
   };
-  if ((e = cudaStreamCreateWithFlags(&ctx->stream, cudaStreamNonBlocking)) != cudaSuccess)
+  if ((e = cudaStreamCreateWithFlags(&ctx->stream, cudaStreamNonBlocking)) != cudaSuccess ||
+      (e = cudaStreamCreateWithFlags(&ctx->stream_side, cudaStreamNonBlocking)) != cudaSuccess ||
+      (e = cudaEventCreateWithFlags(&ctx->ev_fork, cudaEventDisableTiming)) != cudaSuccess ||
+      (e = cudaEventCreateWithFlags(&ctx->ev_join, cudaEventDisableTiming)) != cudaSuccess)
     return bail(PDP3G_CUDA_ERROR);
   if ((e = dalloc(ctx, &ctx->grid_mem, ng * PDP3G_NCOMP)) != cudaSuccess)
     return bail(e == cudaErrorMemoryAllocation ? PDP3G_NO_MEMORY : PDP3G_CUDA_ERROR);
@@ -340,6 +347,9 @@ void pdp3g_destroy(pdp3g_ctx *ctx) {
   cudaFree(ctx->d_stage);
   if (ctx->stream) cudaStreamDestroy(ctx->stream);
   if (ctx->stream_up) cudaStreamDestroy(ctx->stream_up);
+  if (ctx->stream_side) cudaStreamDestroy(ctx->stream_side);
+  if (ctx->ev_fork) cudaEventDestroy(ctx->ev_fork);
+  if (ctx->ev_join) cudaEventDestroy(ctx->ev_join);
   if (ctx->ev_chunk) cudaEventDestroy(ctx->ev_chunk);
   if (ctx->ev_up) cudaEventDestroy(ctx->ev_up);
   delete ctx;
@@ -750,16 +760,30 @@ static cudaError_t phase_reset_j(pdp3g_ctx *ctx) {
   return cudaMemsetAsync(ctx->g.jr, 0, sizeof(double) * ng * 3, ctx->stream);
 }
 
-// ParticlesList::step_v + full_current_distribution (src/particlesList.cpp:20-54)
+// ParticlesList::step_v + full_current_distribution (src/particlesList.cpp:20-54).
+// Species are independent apart from their sums into J (atomics), so with
+// two or more species every second one runs on the side stream: the last,
+// partial round of CTAs of one species' kernel overlaps the next kernel.
 static void phase_particles(pdp3g_ctx *ctx) {
-  for (auto &sp : ctx->species) {
+  const bool fork = ctx->species.size() >= 2;
+  if (fork) {
+    cudaEventRecord(ctx->ev_fork, ctx->stream);
+    cudaStreamWaitEvent(ctx->stream_side, ctx->ev_fork, 0);
+  }
+  for (size_t j = 0; j < ctx->species.size(); j++) {
+    Species &sp = ctx->species[j];
+    cudaStream_t st = fork && (j & 1) ? ctx->stream_side : ctx->stream;
     if (sp.fp32)
       launch_push_deposit_f32(ctx->g, sp.f32, ctx->cfg.pusher, ctx->n_sm, ctx->f32_blocks_per_sm,
-                              ctx->stream);
+                              st);
     else
-      launch_push_deposit_f64(ctx->g, sp.dev, ctx->cfg.pusher, ctx->n_sm, ctx->stream);
+      launch_push_deposit_f64(ctx->g, sp.dev, ctx->cfg.pusher, ctx->n_sm, st);
     ctx->launches++;
     ctx->particle_launches++;
+  }
+  if (fork) {
+    cudaEventRecord(ctx->ev_join, ctx->stream_side);
+    cudaStreamWaitEvent(ctx->stream, ctx->ev_join, 0);
   }
 }
 
