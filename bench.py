@@ -219,6 +219,20 @@ def cpu_sample_run(wl, steps, warmup, fraction, threads):
     return rate, kind, threads, sample, secs
 
 
+def cpu_baseline(wl, steps, fraction, one_thread_fraction):
+    """The upstream CPU step on all host cores, plus a 1-thread figure on a
+    smaller sample of the same workload (the upstream sets its OpenMP thread
+    count to all cores itself, src/loadInitParam.cpp:25-29)."""
+    threads = os.cpu_count() or 1
+    rate, kind, cores, sample, _ = cpu_sample_run(wl, steps, 1, fraction, threads)
+    out = {"value": rate, "unit": UNIT, "cores": cores, "kind": kind, "sample": sample}
+    if threads > 1 and one_thread_fraction > 0:
+        r1, _, _, s1, _ = cpu_sample_run(wl, max(1, min(steps, 2)), 1, one_thread_fraction, 1)
+        out["one_thread"] = {"value": r1, "unit": UNIT, "cores": 1, "sample": s1}
+        out["threads_speedup"] = rate / r1
+    return out
+
+
 def run_reference(args, rank, world):
     if rank != 0:
         return 0
@@ -227,6 +241,10 @@ def run_reference(args, rank, world):
     fraction = args.cpu_fraction
     steps = max(1, args.steps)
     rate, kind, cores, sample, secs = cpu_sample_run(wl, steps, args.warmup, fraction, threads)
+    one = None
+    if threads > 1 and args.cpu_one_thread_fraction > 0:
+        r1, _, _, s1, _ = cpu_sample_run(wl, 2, 1, args.cpu_one_thread_fraction, 1)
+        one = {"value": r1, "unit": UNIT, "cores": 1, "sample": s1}
     line = {
         "metric": METRIC, "value": rate, "unit": UNIT, "impl": "reference", "n_gpus": 0,
         "steps": steps, "warmup": args.warmup, "ms_per_step": 1000.0 * secs / steps,
@@ -235,7 +253,7 @@ def run_reference(args, rank, world):
         "config": {"workload": wl.name, "n_grid_r": wl.n_grid_r, "n_grid_z": wl.n_grid_z,
                    "particles": wl.n_particles, "pusher": wl.pusher, "sample": sample},
         "cpu_baseline": {"value": rate, "unit": UNIT, "cores": cores, "kind": kind,
-                         "sample": sample},
+                         "sample": sample, "one_thread": one},
         "e2e": {"value": rate, "unit": UNIT, "h2d_bytes_per_step": 0, "d2h_bytes_per_step": 0},
     }
     print(json.dumps(line), flush=True)
@@ -269,12 +287,14 @@ def main():
                     help="divide every ensemble run's grid by this (smaller runs)")
     ap.add_argument("--ppc", type=int, default=None,
                     help="macroparticles per cell (profiling runs on a smaller case)")
-    ap.add_argument("--e2e-steps", type=int, default=3)
+    ap.add_argument("--e2e-steps", type=int, default=10)
     ap.add_argument("--accuracy-steps", type=int, default=1000,
                     help="untimed FP32-vs-FP64 run of this many steps after the timing "
                          "(0: skip)")
     ap.add_argument("--cpu-fraction", type=float, default=1.0 / 32)
     ap.add_argument("--cpu-steps", type=int, default=3)
+    ap.add_argument("--cpu-one-thread-fraction", type=float, default=1.0 / 256,
+                    help="plasma fraction of the 1-thread CPU figure (0: skip it)")
     ap.add_argument("--no-cpu-baseline", action="store_true")
     args = ap.parse_args()
 
@@ -407,9 +427,14 @@ def main():
     cpu = None
     if rank == 0 and world == 1 and not args.no_cpu_baseline:
         try:
-            rate, kind, cores, sample, _ = cpu_sample_run(
-                wl, args.cpu_steps, 1, args.cpu_fraction, os.cpu_count() or 1)
-            cpu = {"value": rate, "unit": UNIT, "cores": cores, "kind": kind, "sample": sample}
+            cpu = cpu_baseline(wl, args.cpu_steps, args.cpu_fraction,
+                               args.cpu_one_thread_fraction)
+            if wl.device_plasma is not None:
+                cpu["full_size"] = (
+                    "not run: memory and time (the upstream double** layout holds ~62 GB of "
+                    "host memory for the %d particles, and one step takes ~%.0f s at the "
+                    "rate above); the sample is the same grid, density ramp, bunch and "
+                    "pusher at a reduced ppc" % (wl.n_particles, wl.n_particles / cpu["value"]))
         except Exception as exc:  # reported, not fatal
             cpu = {"value": None, "unit": UNIT, "cores": None, "kind": None,
                    "sample": "failed: %s" % exc}
@@ -429,6 +454,7 @@ def main():
             "steps": args.steps, "warmup": args.warmup, "ms_per_step": ms_max / args.steps,
             "higher_is_better": True, "scaling": "weak", "vs_baseline": None,
             "dtype": "f64" if head_prec == "fp64" else "f32+f64acc",
+            "fp64_plain_value": v64, "fp32_over_fp64": v32 / v64,
             "data": "synthetic (seeded)",
             "config": {"workload": wl.name, "n_grid_r": wl.n_grid_r, "n_grid_z": wl.n_grid_z,
                        "particles": wl.n_particles, "pusher": wl.pusher,
@@ -436,10 +462,10 @@ def main():
                        "l2": "inputs larger than L2 (particle state %.2f GB)"
                              % (bytes_particle_phase / 1e9)},
             "forms": forms,
-            "accuracy": accuracy,
             "cell_updates_per_s": n_nodes / (ms_fields / 1000.0) if ms_fields > 0 else None,
             "cell_updates_per_s_step": n_nodes * args.steps * world / (ms_max / 1000.0),
             "kernel_ms": {"particles": ms_part, "fields": ms_fields,
+                          "sort": tm["ms_sort"] / max(tm["steps"], 1),
                           "other": tm["ms_other"] / max(tm["steps"], 1)},
             "roofline": {"bound": "hbm", "achieved": achieved, "peak": peaks.get("hbm_gbs"),
                          "unit": "GB/s", "frac": achieved / peaks.get("hbm_gbs"),
@@ -451,6 +477,7 @@ def main():
             "cpu_baseline": cpu,
             "gpu_launches": tm["launches"],
             "clocks": clk,
+            "accuracy": accuracy,
         }
         print(json.dumps(line), flush=True)
     if accuracy is None:
@@ -505,8 +532,9 @@ def run_accuracy(api, wl, device, steps, every):
         s_.close()
     return {"steps": steps, "every": every, "status_events": first_status,
             "max_gauss_rel_fp32": max(r["gauss_rel_fp32"] for r in rows),
+            "max_gauss_rel_fp64": max(r["gauss_rel_fp64"] for r in rows),
             "max_field_energy_rel_diff": max(r["field_energy_rel_diff"] for r in rows),
-            "final": rows[-1], "trace": rows}
+            "max_kinetic_energy_rel_diff": max(r["kinetic_energy_rel_diff"] for r in rows)}
 
 
 def run_ensemble(args, rank, world, local_rank, dist=None):
@@ -576,6 +604,13 @@ def run_ensemble(args, rank, world, local_rank, dist=None):
     step_bytes = (n_slots * BYTES_PER_PARTICLE["fp32"] + nodes * BYTES_PER_NODE["fp32"]) * world
     peaks, peak_src = load_peaks()
     achieved = step_bytes / (ms_max / args.steps / 1000.0) / 1e9
+    cpu = None
+    if rank == 0 and world == 1 and not args.no_cpu_baseline:
+        try:
+            cpu = ensemble_cpu_baseline(params, alive, args.steps, args.cpu_fraction / 2)
+        except Exception as exc:  # reported, not fatal
+            cpu = {"value": None, "unit": UNIT, "cores": None, "kind": None,
+                   "sample": "failed: %s" % exc}
     if rank == 0:
         print(json.dumps({
             "metric": METRIC, "value": value, "unit": UNIT, "n_gpus": world,
@@ -604,11 +639,38 @@ def run_ensemble(args, rank, world, local_rank, dist=None):
                          "traffic": None, "kernel": "k_ensemble (whole step)",
                          "peak_source": peak_src,
                          "algorithmic_bytes_per_step": step_bytes},
+            "cpu_baseline": cpu,
             "clocks": clk}), flush=True)
     ens.close()
     for s_ in sims:
         s_.close()
     return 0
+
+
+def ensemble_cpu_baseline(params, alive, steps, fraction, n_sample=4):
+    """The upstream CPU step on a sample of the ensemble's runs (n_sample runs
+    spread over the list, `fraction` of each one's plasma, 2 steps each, all
+    host cores), extrapolated to every run for `steps` steps: the runs are
+    independent, so the CPU would step them one after another at the sampled
+    particle-steps rate."""
+    from pdp3_b200 import workloads as W
+    threads = os.cpu_count() or 1
+    picks = sorted(set(int(round(x)) for x in np.linspace(0, len(params) - 1, n_sample)))
+    work = secs = 0.0
+    kind = None
+    for j in picks:
+        wl = W.ensemble_run_workload(params[j], steps=500)
+        rate, kind, _, _, sec = cpu_sample_run(wl, 2, 1, fraction, threads)
+        work += rate * sec
+        secs += sec
+    rate = work / secs
+    return {"value": rate, "unit": UNIT, "cores": threads, "kind": kind,
+            "sample": "runs %s of %d, %.4g of each run's plasma particles + bunch, 2 steps "
+                      "after 1 warm-up each, %d OpenMP threads" % (picks, len(params), fraction,
+                                                                    threads),
+            "extrapolated_seconds": alive * steps / rate,
+            "extrapolation": "%d runs x %d steps (%d alive particles) one after another at "
+                             "the sampled rate" % (len(params), steps, alive)}
 
 
 def fitted_fd_slope(api, W, fam, theta, j, steps, probe, hmax=0.02, npts=4):
@@ -805,7 +867,9 @@ def run_e2e(sim, wl, torch, stream, steps):
     t0 = time.perf_counter()
     alive_total = 0
     P = ctypes.POINTER(ctypes.c_double)
+    step_rates = []
     for _ in range(steps):
+        ts = time.perf_counter()
         sim.step(1)
         # this step's state out and, from the same host arrays, the next
         # step's input in: both PCIe directions at once (pdp3g_exchange_species)
@@ -815,11 +879,16 @@ def run_e2e(sim, wl, torch, stream, steps):
             sim._check(sim.L.pdp3g_exchange_species(sim.h, sid, *ptrs, al, *ptrs, al),
                        "exchange_species")
         sim._check(sim.L.pdp3g_get_field(sim.h, 2, ez.ctypes.data_as(P)), "get_field")
-        alive_total += sum(len(a["r"]) if sid < len(wl.species) else int(al.sum())
-                           for sid, a, al, _ in bufs)
+        te = time.perf_counter()
+        n_step = sum(len(a["r"]) if sid < len(wl.species) else int(al.sum())
+                     for sid, a, al, _ in bufs)
+        alive_total += n_step
+        step_rates.append(n_step / (te - ts))
     secs = time.perf_counter() - t0
     return {"value": alive_total / secs, "unit": UNIT, "h2d_bytes_per_step": h2d,
             "d2h_bytes_per_step": d2h, "steps": steps, "_secs": secs, "_work": alive_total,
+            "per_step": {"median": statistics.median(step_rates), "min": min(step_rates),
+                         "max": max(step_rates)},
             "note": "per step, through the C ABI: one step, then every species' full state "
                     "D2H into pinned host arrays and from them H2D as the next step's input "
                     "(pdp3g_exchange_species, both directions concurrently), E_z D2H"}

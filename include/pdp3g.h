@@ -289,8 +289,11 @@ pdp3g_status pdp3g_reset_timing(pdp3g_ctx *ctx);
    rejected with PDP3G_INVALID_ARG.  Every call shares that array and no
    entry needs clearing (each call overwrites the slots it reads), but calls
    that overlap on the GPU race on it: serialise them.  The first call on a
-   device looks up the array's device address; make that first call before
-   any stream capture.  Calls no cudaMalloc/cudaFree. */
+   device (and the first after the current context changes, e.g. after a
+   cudaDeviceReset) looks up the array's device address; make that first
+   call before any stream capture.  A CUDA error already pending on the
+   calling thread is reported as PDP3G_CUDA_ERROR and left in place, and
+   nothing is launched.  Calls no cudaMalloc/cudaFree. */
 pdp3g_status pdp3g_field_diagnostics_noalloc(
     const double *e_r, const double *e_phi, const double *e_z, const double *h_r,
     const double *h_phi, const double *h_z, const double *rho, const double *rho0,

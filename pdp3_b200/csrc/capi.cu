@@ -764,11 +764,14 @@ static cudaError_t phase_reset_j(pdp3g_ctx *ctx) {
 // Species are independent apart from their sums into J (atomics), so with
 // two or more species every second one runs on the side stream: the last,
 // partial round of CTAs of one species' kernel overlaps the next kernel.
-static void phase_particles(pdp3g_ctx *ctx) {
+// The fork and join are checked: if the join's wait failed, the phases
+// after this one would no longer be ordered after the side stream's J sums.
+static cudaError_t phase_particles(pdp3g_ctx *ctx) {
   const bool fork = ctx->species.size() >= 2;
+  cudaError_t e;
   if (fork) {
-    cudaEventRecord(ctx->ev_fork, ctx->stream);
-    cudaStreamWaitEvent(ctx->stream_side, ctx->ev_fork, 0);
+    if ((e = cudaEventRecord(ctx->ev_fork, ctx->stream)) != cudaSuccess) return e;
+    if ((e = cudaStreamWaitEvent(ctx->stream_side, ctx->ev_fork, 0)) != cudaSuccess) return e;
   }
   for (size_t j = 0; j < ctx->species.size(); j++) {
     Species &sp = ctx->species[j];
@@ -782,9 +785,10 @@ static void phase_particles(pdp3g_ctx *ctx) {
     ctx->particle_launches++;
   }
   if (fork) {
-    cudaEventRecord(ctx->ev_join, ctx->stream_side);
-    cudaStreamWaitEvent(ctx->stream, ctx->ev_join, 0);
+    if ((e = cudaEventRecord(ctx->ev_join, ctx->stream_side)) != cudaSuccess) return e;
+    if ((e = cudaStreamWaitEvent(ctx->stream, ctx->ev_join, 0)) != cudaSuccess) return e;
   }
+  return cudaGetLastError();
 }
 
 // EField::calc_field (src/eField.cpp:85-170)
@@ -817,7 +821,7 @@ pdp3g_status pdp3g_step(pdp3g_ctx *ctx, int32_t nsteps) {
       if (ss != PDP3G_OK) return ss;
     }
     if (ev) cudaEventRecord(ev->ev[4], st);
-    phase_particles(ctx);
+    CK(phase_particles(ctx));
     if (ev) cudaEventRecord(ev->ev[5], st);
     phase_calc_e(ctx);
     if (ev) cudaEventRecord(ev->ev[6], st);
@@ -857,8 +861,7 @@ pdp3g_status pdp3g_reset_j(pdp3g_ctx *ctx) {
 pdp3g_status pdp3g_push_deposit(pdp3g_ctx *ctx) {
   if (!ctx) return PDP3G_INVALID_ARG;
   CK(cudaSetDevice(ctx->device));
-  phase_particles(ctx);
-  CK(cudaGetLastError());
+  CK(phase_particles(ctx));
   return PDP3G_OK;
 }
 
@@ -1991,7 +1994,7 @@ pdp3g_status adj_forward_step(pdp3g_adjoint *a, int cap) {
     phase_inject(ctx);
     phase_calc_h(ctx);
     CK(phase_reset_j(ctx));
-    phase_particles(ctx);
+    CK(phase_particles(ctx));
     phase_calc_e(ctx);
     phase_advance(ctx);
     return PDP3G_OK;

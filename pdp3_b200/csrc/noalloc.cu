@@ -9,6 +9,7 @@
 // Its scratch (one partial sum triple per chunk of the grid) lives in a
 // file-scope __device__ array of fixed size, which every GPU that loads
 // this library keeps until the process exits.  All calls share it.
+#include <cuda.h>
 #include <cuda_runtime.h>
 
 #include <cmath>
@@ -30,7 +31,13 @@ constexpr int NA_MAX_DEVICES = 64;
 static __device__ __align__(256) double g_noalloc_scratch[NA_MAX_CHUNKS * 3];
 
 std::mutex g_setup_mutex;
+// The array's address is looked up per device and per context: after a
+// cudaDeviceReset, or with a non-primary context current, the module is
+// loaded again and the array may sit elsewhere.
 double *g_scratch_addr[NA_MAX_DEVICES] = {nullptr};
+CUcontext g_scratch_ctx[NA_MAX_DEVICES] = {nullptr};
+typedef CUresult (*ctx_get_current_fn)(CUcontext *);
+ctx_get_current_fn g_ctx_get_current = nullptr;
 
 // Block b sums nodes [b*NA_CHUNK, (b+1)*NA_CHUNK) and writes its three
 // partial sums to scratch[3b .. 3b+2].  The per-node terms are those of
@@ -99,15 +106,30 @@ __global__ void k_field_diag_finish(const double *scratch, int chunks, double *o
 }
 
 // Device address of the scratch array on the current device, looked up once
-// per device (the array's name is only a host-side stand-in in host code).
+// per device and context (the array's name is only a host-side stand-in in
+// host code).  The driver's cuCtxGetCurrent is reached through the runtime's
+// entry-point query, so the library keeps no link-time dependency on libcuda.
 cudaError_t scratch_address(int device, double **ptr) {
   if (device < 0 || device >= NA_MAX_DEVICES) return cudaErrorInvalidDevice;
   std::lock_guard<std::mutex> lock(g_setup_mutex);
-  if (g_scratch_addr[device] == nullptr) {
+  if (g_ctx_get_current == nullptr) {
+    void *fn = nullptr;
+    cudaDriverEntryPointQueryResult q;
+    cudaError_t e = cudaGetDriverEntryPoint("cuCtxGetCurrent", &fn, cudaEnableDefault, &q);
+    if (e != cudaSuccess) return e;
+    if (q != cudaDriverEntryPointSuccess || fn == nullptr) return cudaErrorSymbolNotFound;
+    g_ctx_get_current = (ctx_get_current_fn)fn;
+  }
+  CUcontext cur = nullptr;
+  if (g_ctx_get_current(&cur) != CUDA_SUCCESS) return cudaErrorContextIsDestroyed;
+  if (g_scratch_addr[device] == nullptr || cur == nullptr || g_scratch_ctx[device] != cur) {
     void *p = nullptr;
     cudaError_t e = cudaGetSymbolAddress(&p, g_noalloc_scratch);
     if (e != cudaSuccess) return e;
+    // the runtime makes the primary context current if none was
+    if (cur == nullptr && g_ctx_get_current(&cur) != CUDA_SUCCESS) return cudaErrorContextIsDestroyed;
     g_scratch_addr[device] = (double *)p;
+    g_scratch_ctx[device] = cur;
   }
   *ptr = g_scratch_addr[device];
   return cudaSuccess;
@@ -140,6 +162,14 @@ extern "C" pdp3g_status pdp3g_field_diagnostics_noalloc(
             nodes, (long long)NA_MAX_CHUNKS * NA_CHUNK, NA_MAX_CHUNKS, NA_CHUNK);
     return PDP3G_INVALID_ARG;
   }
+  // an error left pending by the caller's own earlier work is reported and
+  // left in place for the caller's check; nothing is launched
+  const cudaError_t pending = cudaPeekAtLastError();
+  if (pending != cudaSuccess) {
+    fprintf(stderr, "pdp3g_field_diagnostics_noalloc: a CUDA error was pending before the "
+                    "call (%s); nothing launched\n", cudaGetErrorString(pending));
+    return PDP3G_CUDA_ERROR;
+  }
   int device = 0;
   if (cudaGetDevice(&device) != cudaSuccess) return PDP3G_CUDA_ERROR;
   double *scratch = nullptr;
@@ -150,6 +180,7 @@ extern "C" pdp3g_status pdp3g_field_diagnostics_noalloc(
   k_field_diag_chunks<<<(int)chunks, NA_THREADS, 0, st>>>(e_r, e_phi, e_z, h_r, h_phi, h_z, rho,
                                                           rho0, sigma, n_grid_r, n_grid_z, dr,
                                                           dz, scratch);
+  if (cudaGetLastError() != cudaSuccess) return PDP3G_CUDA_ERROR;
   k_field_diag_finish<<<1, NA_THREADS, 0, st>>>(scratch, (int)chunks, out);
   return cudaGetLastError() == cudaSuccess ? PDP3G_OK : PDP3G_CUDA_ERROR;
 }

@@ -492,20 +492,28 @@ class DevicePlasma:
 def large_config(seed=1003, n_grid_r=513, n_grid_z=4097, r_size=0.1, z_size=0.8, ppc=64,
                  density=1e17, ramp_fraction=0.2, steps=2000, beam_gamma=10.0,
                  beam_radius=5e-3, beam_length=0.02, beam_density=5e16, pusher="vay",
-                 sort_interval=20):
+                 sort_interval=20, host_plasma=False):
     """Large FP32 case: 512x4096 cells, electrons and protons at 64 ppc
     (268,435,456 particles, generated on the GPU), density ramped linearly
     from 0 to 1e17 m^-3 over the first 20% of z, gamma = 10 electron bunch
     (r 5 mm, length 2 cm, 5e16 m^-3) with the Vay pusher, particles re-sorted
-    by cell every 20 steps."""
+    by cell every 20 steps.  host_plasma=True builds the plasma as host
+    arrays instead (same conventions, numpy generator; for reduced ppc,
+    where the same particles must also reach the oracle)."""
     dr = r_size / (n_grid_r - 1)
     dz = z_size / (n_grid_z - 1)
-    plasma = DevicePlasma(seed, r_size, z_size, n_grid_r, n_grid_z, ppc, density,
-                          ramp_fraction * z_size)
+    z_ramp = ramp_fraction * z_size
+    species, plasma = [], None
+    if host_plasma:
+        rng = np.random.default_rng(seed)
+        species = thermal_plasma(rng, r_size, z_size, n_grid_r, n_grid_z, ppc,
+                                 lambda zc: density * np.minimum(zc / z_ramp, 1.0), 1.0)
+    else:
+        plasma = DevicePlasma(seed, r_size, z_size, n_grid_r, n_grid_z, ppc, density, z_ramp)
     bunch_cells = (beam_radius / dr) * (beam_length / dz)
     beam = BeamInit(-1.0, 1.0, int(round(64 * bunch_cells)), beam_length, beam_radius,
                     beam_density, gamma_velocity(beam_gamma), 1, 0.0, "reverse", seed)
     return Workload("large_%dx%d_ppc%d" % (n_grid_r - 1, n_grid_z - 1, ppc), r_size, z_size,
                     n_grid_r, n_grid_z, courant_dt(dr, dz), steps,
-                    absorbing_layer(n_grid_r, n_grid_z, 10), pusher, [], beam, sort_interval,
-                    plasma)
+                    absorbing_layer(n_grid_r, n_grid_z, 10), pusher, species, beam,
+                    sort_interval, plasma)

@@ -8,7 +8,8 @@ Those files hold values printed with 6 significant digits, which float32
 stores without loss, so they are kept here as float32 arrays, one per probe,
 shaped (r_end - r_start, z_end - z_start).
 
-Usage: python tests/golden/make_golden.py [upstream root, default /root/reference]
+Usage: python tests/golden/make_golden.py <upstream source root>
+       (or set PDP3_REFERENCE to the upstream source root)
 """
 import gzip
 import os
@@ -41,7 +42,9 @@ def frame_box(name):
 
 
 def main():
-    root = sys.argv[1] if len(sys.argv) > 1 else "/root/reference"
+    root = sys.argv[1] if len(sys.argv) > 1 else os.environ.get("PDP3_REFERENCE")
+    if not root:
+        sys.exit("usage: make_golden.py <upstream source root> (or set PDP3_REFERENCE)")
     out = {}
     for comp, frame in FRAMES.items():
         path = os.path.join(root, "test", "functional", "true_data", comp, frame, "4.dat.gz")
