@@ -526,7 +526,10 @@ __device__ __forceinline__ void deposit_rz(const GridDev &g, double q, double r_
 // The fused particle phase for one species.
 // 4 CTAs of 256 threads per SM (64 registers): the kernel is latency-bound
 // and gains more from residency than it loses to the few spilled registers.
-__global__ void __launch_bounds__(256, 4) k_push_deposit_f64(GridDev g, SpeciesDev s, int pusher) {
+// PUSHER: 0 relativistic Boris, 1 Vay, 2 classic Boris (one kernel per
+// pusher, as the FP32 form has).
+template <int PUSHER>
+__global__ void __launch_bounds__(256, 4) k_push_deposit_f64(GridDev g, SpeciesDev s) {
   const double half_dt = g.dt / 2.;
   const double dr = g.dr, dz = g.dz;
   const double radius_wall = g.r_size - dr / 2.;
@@ -545,17 +548,38 @@ __global__ void __launch_bounds__(256, 4) k_push_deposit_f64(GridDev g, SpeciesD
     const double w = s.w[p];
     const double q = s.charge * w, m = s.mass * w;
     // gather (E at time n, H at n+1/2 from the half-time arrays)
+    // The six components in one rolled loop: every component's arithmetic
+    // is the same as six inlined calls, but the kernel holds one copy of it
+    // (instruction-cache misses were the kernel's top stall).
     double e[3], b[3];
-    e[0] = gather_one(g, g.er, r, z, true, false);
-    e[2] = gather_one(g, g.ez, r, z, false, true);
-    e[1] = gather_one(g, g.ephi, r, z, false, false);
-    b[2] = gather_one(g, g.hzh, r, z, true, false);
-    b[0] = gather_one(g, g.hrh, r, z, false, true);
-    b[1] = gather_one(g, g.hphih, r, z, true, true);
-    if (pusher == 1)
+    {
+      double g0 = 0, g1 = 0, g2 = 0, g3 = 0, g4 = 0, g5 = 0;
+#pragma unroll 1
+      for (int c = 0; c < 6; c++) {
+        const double *f =
+            c == 0 ? g.er
+                   : (c == 1 ? g.ez : (c == 2 ? g.ephi : (c == 3 ? g.hzh : (c == 4 ? g.hrh : g.hphih))));
+        const bool rh = (c == 0) || (c == 3) || (c == 5);
+        const bool zh = (c == 1) || (c == 4) || (c == 5);
+        const double val = gather_one(g, f, r, z, rh, zh);
+        g0 = c == 0 ? val : g0;
+        g1 = c == 1 ? val : g1;
+        g2 = c == 2 ? val : g2;
+        g3 = c == 3 ? val : g3;
+        g4 = c == 4 ? val : g4;
+        g5 = c == 5 ? val : g5;
+      }
+      e[0] = g0;
+      e[2] = g1;
+      e[1] = g2;
+      b[2] = g3;
+      b[0] = g4;
+      b[1] = g5;
+    }
+    if (PUSHER == 1)
       vay(g, q, m, e, b, v);
     else
-      boris(g, q, m, e, b, v, pusher == 0);
+      boris(g, q, m, e, b, v, PUSHER == 0);
     // dump_position_to_old + half_step_pos + back_position_to_rz
     // (src/particles.cpp:1256-1294); y is 0 on entry
     const double r_old = r, z_old = z;
@@ -683,7 +707,12 @@ void launch_push_deposit_f64(const GridDev &g, const SpeciesDev &s, int pusher, 
   long long blocks = (s.n + 255) / 256;
   const long long cap = (long long)n_sm * 8;
   if (blocks > cap) blocks = cap;
-  k_push_deposit_f64<<<(int)blocks, 256, 0, st>>>(g, s, pusher);
+  if (pusher == 1)
+    k_push_deposit_f64<1><<<(int)blocks, 256, 0, st>>>(g, s);
+  else if (pusher == 2)
+    k_push_deposit_f64<2><<<(int)blocks, 256, 0, st>>>(g, s);
+  else
+    k_push_deposit_f64<0><<<(int)blocks, 256, 0, st>>>(g, s);
 }
 
 void launch_charge_density_f64(const GridDev &g, const SpeciesDev &s, double *rho,
