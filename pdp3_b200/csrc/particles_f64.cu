@@ -11,9 +11,9 @@
 //
 // Compiled with --fmad=false and written in the upstream evaluation order so
 // that every per-particle result is the CPU step's, bit for bit, except for
-// log() and pow() whose CUDA implementations may differ from glibc by an ulp
-// or two; J is accumulated with FP64 atomics, so its summation order (not
-// its terms) differs from the serial CPU loop.
+// log(), whose CUDA implementation may differ from glibc's by an ulp or two,
+// and get_gamma_inv (see there); J is accumulated with FP64 atomics, so its
+// summation order (not its terms) differs from the serial CPU loop.
 //
 // Algorithmic bytes per particle-step: reads r, z, v_r, v_phi, v_z, w
 // (48 B), writes r, z, v_r, v_phi, v_z (40 B), plus 1 B alive flag read and
@@ -112,9 +112,23 @@ __device__ __forceinline__ double get_gamma(const GridDev &g, double sq_velocity
   return gamma;
 }
 
-// lib::get_gamma_inv, src/lib.cpp:72-80
+// lib::get_gamma_inv, src/lib.cpp:72-80: pow(x, -0.5) there.  Here y =
+// 1/sqrt(x) refined by one Newton step whose residual 1 - x y^2 is formed
+// exactly with fused multiply-adds (y^2 = t + h split by fma, Markstein's
+// method).  On the host it equals glibc's pow(x, -0.5) for all but 0.05% of
+// 2e7 random x in [1, 100] (plain 1/sqrt(x): 40%); on the device it is closer
+// to the CPU step than CUDA's pow (one-step deviation of the wake and large
+// grids from the oracle 1e-16 instead of 1e-14), at a fraction of pow's
+// cost on the FP64 pipe.  The fma calls are explicit: they are not
+// contractions, which --fmad=false disables.
 __device__ __forceinline__ double get_gamma_inv(double sq_velocity) {
-  return pow(1.0 + sq_velocity / LIGHT_SPEED_POW_2, -0.5);
+  const double x = 1.0 + sq_velocity / LIGHT_SPEED_POW_2;
+  const double y = 1.0 / sqrt(x);
+  const double t = y * y;
+  const double h = fma(y, y, -t);  // y * y = t + h exactly
+  double r = fma(-x, t, 1.0);
+  r = fma(-x, h, r);               // 1 - x y^2
+  return fma(0.5 * y, r, y);
 }
 
 // Particles::boris_pusher_single, src/particles.cpp:1025-1150
