@@ -575,17 +575,26 @@ def run_ensemble(args, rank, world, local_rank, dist=None):
         s_.set_timing(False)
     ens = api.Ensemble(sims)
     bpsm = ens.autotune(2)
-    ens.run(args.warmup)
+    chosen = "step_graph" if ens.info()["mode"] == 1 else "persistent"
+    # both modes timed (every rank takes the same steps in the same order);
+    # the autotuner's choice is the value
+    modes = {}
     clocks = ClockSampler(local_rank)
     clocks.start()
     time.sleep(0.3)
-    if dist is not None:
-        dist.barrier()
-    torch.cuda.synchronize()
-    ens.run(args.steps)
-    torch.cuda.synchronize()
-    if dist is not None:
-        dist.barrier()
+    for m in ([x for x in ("persistent", "step_graph") if x != chosen] + [chosen]):
+        ens.set_mode(m)
+        ens.run(args.warmup)
+        if dist is not None:
+            dist.barrier()
+        torch.cuda.synchronize()
+        ens.run(args.steps)
+        torch.cuda.synchronize()
+        if dist is not None:
+            dist.barrier()
+        inf = ens.info()
+        modes[m] = {"ms_per_step": inf["last_ms"] / args.steps,
+                    "cuda_graph": bool(inf["used_graph"])}
     clk = clocks.stop()
     info = ens.info()
     ms = info["last_ms"]
@@ -625,8 +634,17 @@ def run_ensemble(args, rank, world, local_rank, dist=None):
                        "grids": "r in {64,128,256} x z in {256,512,1024} cells / %d"
                                 % args.ensemble_scale,
                        "parallelism": "replicas x%d" % world},
-            "ensemble": {"blocks_per_sm": bpsm, "blocks": info["blocks"],
-                         "cuda_graph": bool(info["used_graph"]), "ms_per_step": ms / args.steps},
+            "ensemble": {"mode": chosen, "blocks_per_sm": info["blocks_per_sm"],
+                         "blocks": info["blocks"], "cuda_graph": bool(info["used_graph"]),
+                         "ms_per_step": ms / args.steps,
+                         "modes": {m: dict(v, value=alive_all * args.steps /
+                                           (v["ms_per_step"] * args.steps / 1000.0),
+                                           over_sequential=(seq_ms_max / args.steps) /
+                                           v["ms_per_step"])
+                                   for m, v in modes.items()},
+                         "autotuner": "persistent kernel at every feasible CTAs-per-SM "
+                                      "count and the step graph, 2 steps each; the fastest "
+                                      "is kept"},
             "sequential": {"value": seq_value, "ms_per_step": seq_ms_max / args.steps,
                            "kernel_ms_per_step": seq_kernel_ms / args.steps,
                            "note": "same runs, each stepped alone with per-run launches; "

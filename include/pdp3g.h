@@ -68,7 +68,7 @@ typedef struct {
   double pml_l1, pml_l2, pml_l3, pml_sigma1, pml_sigma2;
   int32_t pusher;       /* pdp3g_pusher */
   int32_t precision;    /* pdp3g_precision */
-  int32_t device;       /* CUDA device ordinal */
+  int32_t device;       /* CUDA device ordinal (PDP3G_INVALID_ARG past the last one) */
   int32_t sort_interval;/* particles re-sorted by cell every N steps (0: never) */
 } pdp3g_config;
 
@@ -309,20 +309,32 @@ pdp3g_status pdp3g_field_diagnostics_noalloc(
    state stays in its context (pdp3g_get_field etc. work as usual).  The
    kernel checks a host-mapped cancel flag and a time budget once per step
    and returns PDP3G_TIMEOUT when either stops it; the steps done are
-   reported by pdp3g_ensemble_info and added to every run's time. */
+   reported by pdp3g_ensemble_info and added to every run's time.
+   A second mode (PDP3G_ENS_STEP_GRAPH) replays one captured CUDA graph per
+   step in which every run's own step kernels (those of pdp3g_step) sit on
+   parallel branches, with the bunch injection and the time advance done on
+   the device; its cancel flag and budget are checked between steps (at most
+   eight steps in flight).  pdp3g_ensemble_autotune times both modes. */
 typedef struct pdp3g_ensemble pdp3g_ensemble;
+enum { PDP3G_ENS_PERSISTENT = 0, PDP3G_ENS_STEP_GRAPH = 1 };
 typedef struct {
   int32_t runs, blocks_per_sm, blocks, used_graph;
   double last_ms;            /* device time of the last run call */
   int64_t last_steps_done;
   int64_t particles;         /* macroparticle slots over all runs */
+  int32_t mode;              /* PDP3G_ENS_PERSISTENT or PDP3G_ENS_STEP_GRAPH */
+  int32_t reserved;
 } pdp3g_ensemble_stats;
 pdp3g_status pdp3g_ensemble_create(pdp3g_ctx *const *runs, int32_t n_runs, pdp3g_ensemble **out);
 pdp3g_status pdp3g_ensemble_run(pdp3g_ensemble *e, int32_t nsteps);
-/* tries every feasible CTAs-per-SM count for steps_per_trial steps each (the
-   trial steps advance the runs) and keeps the fastest */
+/* times the persistent kernel at every feasible CTAs-per-SM count and the
+   step-graph mode, steps_per_trial steps each (the trial steps advance the
+   runs), and keeps the fastest; *blocks_per_sm receives the persistent
+   kernel's count, or 0 when the step graph won */
 pdp3g_status pdp3g_ensemble_autotune(pdp3g_ensemble *e, int32_t steps_per_trial,
                                      int32_t *blocks_per_sm);
+/* PDP3G_ENS_PERSISTENT (the default) or PDP3G_ENS_STEP_GRAPH */
+pdp3g_status pdp3g_ensemble_set_mode(pdp3g_ensemble *e, int32_t mode);
 pdp3g_status pdp3g_ensemble_set_budget(pdp3g_ensemble *e, double max_ms);  /* 0: none */
 /* re-sort every run's plasma species by cell every `steps` steps (between
    persistent launches); default: the smallest positive sort_interval of the

@@ -53,7 +53,8 @@ class EnsembleInfo(ctypes.Structure):
     _fields_ = [("runs", ctypes.c_int32), ("blocks_per_sm", ctypes.c_int32),
                 ("blocks", ctypes.c_int32), ("used_graph", ctypes.c_int32),
                 ("last_ms", ctypes.c_double), ("last_steps_done", ctypes.c_int64),
-                ("particles", ctypes.c_int64)]
+                ("particles", ctypes.c_int64), ("mode", ctypes.c_int32),
+                ("reserved", ctypes.c_int32)]
 
 
 class Timing(ctypes.Structure):
@@ -110,6 +111,7 @@ EXPORTS = [
     ("pdp3g_ensemble_create", _I32, [ctypes.POINTER(_VP), _I32, ctypes.POINTER(_VP)]),
     ("pdp3g_ensemble_run", _I32, [_VP, _I32]),
     ("pdp3g_ensemble_autotune", _I32, [_VP, _I32, ctypes.POINTER(_I32)]),
+    ("pdp3g_ensemble_set_mode", _I32, [_VP, _I32]),
     ("pdp3g_ensemble_set_budget", _I32, [_VP, ctypes.c_double]),
     ("pdp3g_ensemble_set_sort_interval", _I32, [_VP, _I32]),
     ("pdp3g_ensemble_cancel", _I32, [_VP, _I32]),
@@ -458,6 +460,13 @@ class Ensemble:
         self._check(self.L.pdp3g_ensemble_autotune(self.h, int(steps_per_trial), ctypes.byref(b)),
                     "ensemble_autotune")
         return b.value
+
+    MODES = {"persistent": 0, "step_graph": 1}
+
+    def set_mode(self, mode):
+        """"persistent" (one cooperative kernel per call) or "step_graph" (one
+        captured graph per step with every run's own kernels)."""
+        self._check(self.L.pdp3g_ensemble_set_mode(self.h, self.MODES[mode]), "set_mode")
 
     def set_budget(self, max_ms):
         self._check(self.L.pdp3g_ensemble_set_budget(self.h, float(max_ms)), "set_budget")

@@ -233,11 +233,20 @@ pdp3g_status pdp3g_create(const pdp3g_config *cfg, pdp3g_ctx **out) {
       !(cfg->dt > 0) || cfg->pusher < 0 || cfg->pusher > 2 ||
       (cfg->precision != PDP3G_FP64 && cfg->precision != PDP3G_FP32_CELL))
     return PDP3G_INVALID_ARG;
+  // an ordinal past the last device is the caller's error; checked first so
+  // that no CUDA error is left pending on the calling thread
+  int ndev = 0;
+  if (cudaGetDeviceCount(&ndev) != cudaSuccess) {
+    cudaGetLastError();
+    return PDP3G_CUDA_ERROR;
+  }
+  if (cfg->device < 0 || cfg->device >= ndev) return PDP3G_INVALID_ARG;
   pdp3g_ctx *ctx = new pdp3g_ctx();
   ctx->cfg = *cfg;
   ctx->device = cfg->device;
   cudaError_t e = cudaSetDevice(cfg->device);
   if (e != cudaSuccess) {
+    cudaGetLastError();  // this call's own error: not left for the caller's next check
     delete ctx;
     return PDP3G_CUDA_ERROR;
   }
@@ -1507,6 +1516,12 @@ struct pdp3g_ensemble {
   int64_t last_steps_done = 0;
   int64_t total_particles = 0;
   std::string last_error;
+  // step-graph mode: one captured graph of one step of every run
+  int mode = PDP3G_ENS_PERSISTENT;
+  cudaGraph_t step_graph = nullptr;
+  cudaGraphExec_t step_exec = nullptr;
+  cudaEvent_t ev_fork = nullptr;
+  std::vector<cudaEvent_t> ev_join;
 };
 
 static pdp3g_status ens_fail(pdp3g_ensemble *e, pdp3g_status st, const std::string &m) {
@@ -1528,6 +1543,10 @@ void pdp3g_ensemble_destroy(pdp3g_ensemble *e) {
   if (e->stream) cudaStreamSynchronize(e->stream);
   if (e->exec) cudaGraphExecDestroy(e->exec);
   if (e->graph) cudaGraphDestroy(e->graph);
+  if (e->step_exec) cudaGraphExecDestroy(e->step_exec);
+  if (e->step_graph) cudaGraphDestroy(e->step_graph);
+  if (e->ev_fork) cudaEventDestroy(e->ev_fork);
+  for (auto ev : e->ev_join) cudaEventDestroy(ev);
   cudaFree(e->d_runs);
   cudaFree(e->d_species);
   cudaFree(e->d_status);
@@ -1693,6 +1712,106 @@ static pdp3g_status ens_launch(pdp3g_ensemble *e, bool allow_graph) {
   return PDP3G_OK;
 }
 
+// Step-graph mode: captures one step of every run as one graph.  The
+// injection of every bunch runs first (device time of each run), then each
+// run's own phases on its own streams (HField::calc_field, reset_j, the
+// particle phase with its two-stream fork, EField::calc_field; the same
+// launches as pdp3g_step), and after the runs' branches join, t += dt of
+// every run on the device.  Nothing in the graph depends on the step, so one
+// graph serves every step.
+static pdp3g_status ens_capture_step(pdp3g_ensemble *e) {
+  if (e->step_exec) return PDP3G_OK;
+  if (!e->ev_fork) EK(cudaEventCreateWithFlags(&e->ev_fork, cudaEventDisableTiming));
+  while (e->ev_join.size() < e->runs.size()) {
+    cudaEvent_t ev;
+    EK(cudaEventCreateWithFlags(&ev, cudaEventDisableTiming));
+    e->ev_join.push_back(ev);
+  }
+  EK(cudaStreamBeginCapture(e->stream, cudaStreamCaptureModeThreadLocal));
+  cudaError_t ce = ensemble_inject_all(e->dev, e->stream);
+  if (ce == cudaSuccess) ce = cudaEventRecord(e->ev_fork, e->stream);
+  for (size_t r = 0; r < e->runs.size() && ce == cudaSuccess; r++) {
+    pdp3g_ctx *ctx = e->runs[r];
+    ce = cudaStreamWaitEvent(ctx->stream, e->ev_fork, 0);
+    if (ce != cudaSuccess) break;
+    phase_calc_h(ctx);
+    ce = phase_reset_j(ctx);
+    if (ce == cudaSuccess) ce = phase_particles(ctx);
+    if (ce != cudaSuccess) break;
+    phase_calc_e(ctx);
+    ce = cudaEventRecord(e->ev_join[r], ctx->stream);
+    if (ce == cudaSuccess) ce = cudaStreamWaitEvent(e->stream, e->ev_join[r], 0);
+  }
+  if (ce == cudaSuccess) ce = ensemble_advance(e->dev, e->stream);
+  cudaGraph_t g = nullptr;
+  cudaError_t ce2 = cudaStreamEndCapture(e->stream, &g);
+  if (ce == cudaSuccess) ce = ce2;
+  if (ce == cudaSuccess) ce = cudaGraphInstantiate(&e->step_exec, g, 0);
+  if (ce != cudaSuccess) {
+    if (g) cudaGraphDestroy(g);
+    e->step_exec = nullptr;
+    cudaGetLastError();
+    return ens_fail(e, PDP3G_CUDA_ERROR,
+                    std::string("step graph capture: ") + cudaGetErrorString(ce));
+  }
+  e->step_graph = g;
+  return PDP3G_OK;
+}
+
+// nsteps replays of the step graph; the cancel flag and the budget are
+// checked between steps, with at most kInFlight steps queued ahead
+static pdp3g_status ens_segment_graph(pdp3g_ensemble *e, int nsteps, float *ms_out, int *done,
+                                      int *stop) {
+  pdp3g_status cs = ens_capture_step(e);
+  if (cs != PDP3G_OK) return cs;
+  for (size_t r = 0; r < e->runs.size(); r++) e->h_runs[r].t = e->runs[r]->t;
+  EK(cudaMemcpyAsync(e->d_runs, e->h_runs.data(), sizeof(EnsRun) * e->h_runs.size(),
+                     cudaMemcpyHostToDevice, e->stream));
+  const int init[4] = {0, 0, nsteps, 0};
+  EK(cudaMemcpyAsync(e->d_status, init, sizeof(init), cudaMemcpyHostToDevice, e->stream));
+  constexpr int kInFlight = 8;
+  cudaEvent_t start, mark[kInFlight];
+  EK(cudaEventCreate(&start));
+  for (int i = 0; i < kInFlight; i++) cudaEventCreate(&mark[i]);
+  cudaEventRecord(start, e->stream);
+  int launched = 0, st_code = 0;
+  cudaError_t err = cudaSuccess;
+  e->last_used_graph = true;
+  for (; launched < nsteps; launched++) {
+    if (*(volatile int *)e->h_cancel) { st_code = 1; break; }
+    if (launched >= kInFlight) {
+      // the step launched kInFlight steps ago has ended: its time against the budget
+      cudaEvent_t old = mark[launched % kInFlight];
+      if ((err = cudaEventSynchronize(old)) != cudaSuccess) break;
+      float el = 0;
+      cudaEventElapsedTime(&el, start, old);
+      if (e->budget_ms > 0 && el > e->budget_ms) { st_code = 2; break; }
+    }
+    if ((err = cudaGraphLaunch(e->step_exec, e->stream)) != cudaSuccess) break;
+    cudaEventRecord(mark[launched % kInFlight], e->stream);
+  }
+  cudaEvent_t end;
+  cudaEventCreate(&end);
+  cudaEventRecord(end, e->stream);
+  cudaError_t sync = cudaStreamSynchronize(e->stream);
+  float ms = 0;
+  cudaEventElapsedTime(&ms, start, end);
+  cudaEventDestroy(start);
+  cudaEventDestroy(end);
+  for (int i = 0; i < kInFlight; i++) cudaEventDestroy(mark[i]);
+  if (err != cudaSuccess) return ens_fail(e, PDP3G_CUDA_ERROR, cudaGetErrorString(err));
+  if (sync != cudaSuccess) return ens_fail(e, PDP3G_CUDA_ERROR, cudaGetErrorString(sync));
+  for (auto *c : e->runs) {
+    for (int i = 0; i < launched; i++) c->t = c->t + c->cfg.dt;
+    c->steps += launched;
+  }
+  e->steps_total += launched;
+  *ms_out = ms;
+  *done = launched;
+  *stop = st_code;
+  return PDP3G_OK;
+}
+
 // one persistent launch of nsteps steps; *done receives the steps done
 static pdp3g_status ens_segment(pdp3g_ensemble *e, int nsteps, bool allow_graph, float *ms_out,
                                 int *done, int *stop) {
@@ -1780,7 +1899,9 @@ static pdp3g_status ens_run(pdp3g_ensemble *e, int nsteps, bool allow_graph, flo
     }
     float ms = 0;
     int done = 0;
-    pdp3g_status st = ens_segment(e, seg, allow_graph, &ms, &done, &stop);
+    pdp3g_status st = e->mode == PDP3G_ENS_STEP_GRAPH
+                          ? ens_segment_graph(e, seg, &ms, &done, &stop)
+                          : ens_segment(e, seg, allow_graph, &ms, &done, &stop);
     e->budget_ms = saved_budget;
     if (st != PDP3G_OK) return st;
     total += ms;
@@ -1805,6 +1926,7 @@ pdp3g_status pdp3g_ensemble_autotune(pdp3g_ensemble *e, int32_t steps_per_trial,
   if (!e || steps_per_trial <= 0) return PDP3G_INVALID_ARG;
   float best = 0;
   int best_b = e->blocks_per_sm;
+  e->mode = PDP3G_ENS_PERSISTENT;
   for (int b = 1; b <= e->max_blocks_per_sm; b++) {
     e->blocks_per_sm = b;
     float ms = 0;
@@ -1816,7 +1938,21 @@ pdp3g_status pdp3g_ensemble_autotune(pdp3g_ensemble *e, int32_t steps_per_trial,
     }
   }
   e->blocks_per_sm = best_b;
-  if (blocks_per_sm) *blocks_per_sm = best_b;
+  // the step graph (its capture and first replay are untimed: one warm-up step)
+  e->mode = PDP3G_ENS_STEP_GRAPH;
+  float ms_graph = 0;
+  pdp3g_status st = ens_run(e, 1, false, nullptr);
+  if (st == PDP3G_OK) st = ens_run(e, steps_per_trial, false, &ms_graph);
+  if (st != PDP3G_OK) return st;
+  e->mode = ms_graph < best ? PDP3G_ENS_STEP_GRAPH : PDP3G_ENS_PERSISTENT;
+  if (blocks_per_sm) *blocks_per_sm = e->mode == PDP3G_ENS_STEP_GRAPH ? 0 : best_b;
+  return PDP3G_OK;
+}
+
+pdp3g_status pdp3g_ensemble_set_mode(pdp3g_ensemble *e, int32_t mode) {
+  if (!e || (mode != PDP3G_ENS_PERSISTENT && mode != PDP3G_ENS_STEP_GRAPH))
+    return PDP3G_INVALID_ARG;
+  e->mode = mode;
   return PDP3G_OK;
 }
 
@@ -1847,6 +1983,8 @@ pdp3g_status pdp3g_ensemble_info(pdp3g_ensemble *e, pdp3g_ensemble_stats *out) {
   out->last_ms = e->last_ms;
   out->last_steps_done = e->last_steps_done;
   out->particles = e->total_particles;
+  out->mode = e->mode;
+  out->reserved = 0;
   return PDP3G_OK;
 }
 

@@ -149,6 +149,37 @@ __global__ void __launch_bounds__(F32_THREADS, F32_MIN_BLOCKS) k_ensemble(Ensemb
   }
 }
 
+// ---- graph mode: every run's own step kernels on parallel branches of one
+// captured graph per ensemble step.  Two small kernels make that graph the
+// same for every step: the injection reads each run's time from device
+// memory (as the persistent kernel's phase A does), and the time advance
+// runs on the device after the runs' branches join.
+
+// Bunch::bunch_inject for every bunch species of every run: CTA j handles
+// species j (grid = number of species)
+__global__ void k_ens_inject_all(EnsembleDev E) {
+  if (blockIdx.x < (unsigned)E.nspecies && E.species[blockIdx.x].is_bunch)
+    ens_inject(E, E.species[blockIdx.x]);
+}
+
+// t += dt of every run (src/loadInitParam.cpp:586), the same FP64 accumulation
+__global__ void k_ens_advance(EnsembleDev E) {
+  const int r = blockIdx.x * blockDim.x + threadIdx.x;
+  if (r < E.nruns) E.runs[r].t = E.runs[r].t + E.runs[r].g.dt;
+  if (r == 0) E.status[0] = E.status[0] + 1;
+}
+
+cudaError_t ensemble_inject_all(const EnsembleDev &E, cudaStream_t st) {
+  if (E.nspecies <= 0) return cudaSuccess;
+  k_ens_inject_all<<<E.nspecies, F32_THREADS, 0, st>>>(E);
+  return cudaGetLastError();
+}
+
+cudaError_t ensemble_advance(const EnsembleDev &E, cudaStream_t st) {
+  k_ens_advance<<<(E.nruns + 127) / 128, 128, 0, st>>>(E);
+  return cudaGetLastError();
+}
+
 static void (*ensemble_kernel(int pusher))(EnsembleDev) {
   switch (pusher) {
     case 0: return k_ensemble<0>;

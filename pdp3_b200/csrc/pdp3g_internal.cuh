@@ -171,6 +171,10 @@ struct EnsembleDev {
 // pusher: the pusher every run uses, or -1 when they differ
 int ensemble_max_blocks_per_sm(int pusher);
 cudaError_t ensemble_launch(const EnsembleDev &E, int blocks, int pusher, cudaStream_t st);
+// graph mode: injection of every bunch, and t += dt of every run (both from
+// and into device memory)
+cudaError_t ensemble_inject_all(const EnsembleDev &E, cudaStream_t st);
+cudaError_t ensemble_advance(const EnsembleDev &E, cudaStream_t st);
 
 // byte offsets of the radix sort's scratch (sort.cu)
 struct SortLayout {
