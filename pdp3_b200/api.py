@@ -141,6 +141,7 @@ EXPORTS = [
     ("pdp3g_adjoint_timing", _I32, [_VP, _D, _D]),
     ("pdp3g_adjoint_set_mode", _I32, [_VP, _I32]),
     ("pdp3g_adjoint_set_jump_terms", _I32, [_VP, ctypes.c_uint32]),
+    ("pdp3g_adjoint_set_face_width", _I32, [_VP, ctypes.c_double]),
     ("pdp3g_adjoint_bytes", ctypes.c_int64, [_VP]),
     ("pdp3g_adjoint_destroy", None, [_VP]),
 ]
@@ -556,6 +557,12 @@ class Adjoint:
         bits = {"gather": 1, "walls": 2, "wall_cells": 4}
         self.sim._check(self.L.pdp3g_adjoint_set_jump_terms(
             self.h, sum(bits[t] for t in set(terms))), "adjoint_set_jump_terms")
+
+    def set_face_width(self, half_width):
+        """0: gather jump terms for a density uniform in each cell; h in
+        (0, 0.5]: a box-kernel density estimate of half-width h cells."""
+        self._check(self.L.pdp3g_adjoint_set_face_width(self.h, float(half_width)),
+                    "adjoint_set_face_width")
 
     def timing(self):
         f, b = ctypes.c_double(), ctypes.c_double()

@@ -163,7 +163,8 @@ __device__ __forceinline__ bool warp_seg_sum(int key, float (&v)[N]) {
 // wall-reflection jump terms (face bit 1) are compiled in.
 template <bool WALLS>
 __global__ void __launch_bounds__(ADJ_THREADS, ADJ_MIN_BLOCKS) k_adj_particles(
-    GridDev g, const float *E3, const float *Hh3, AdjSpeciesDev S, AdjGrids A, int face) {
+    GridDev g, const float *E3, const float *Hh3, AdjSpeciesDev S, AdjGrids A, int face,
+    float face_h) {
   const int ncz = g.nz - 1;
   const size_t ng = (size_t)g.nr * g.nz;
   adj::Consts<float> C;
@@ -178,6 +179,7 @@ __global__ void __launch_bounds__(ADJ_THREADS, ADJ_MIN_BLOCKS) k_adj_particles(
   C.nz = g.nz;
   C.bunch = S.st.kind == KIND_BUNCH;
   C.face = face;
+  C.face_h = face_h;
   const long long nchunks = (S.st.n + ADJ_THREADS - 1) / ADJ_THREADS;
   for (long long chunk = blockIdx.x; chunk < nchunks; chunk += gridDim.x) {
     const long long p = chunk * ADJ_THREADS + threadIdx.x;
@@ -353,7 +355,8 @@ void adj_launch_h(const GridDev &g, const AdjGrids &A, cudaStream_t st) {
 }
 
 void adj_launch_particles(const GridDev &g, const float *E3, const float *Hh3,
-                          const AdjSpeciesDev &S, const AdjGrids &A, int face, cudaStream_t st) {
+                          const AdjSpeciesDev &S, const AdjGrids &A, int face, float face_h,
+                          cudaStream_t st) {
   if (S.st.n <= 0) return;
   const long long nchunks = (S.st.n + ADJ_THREADS - 1) / ADJ_THREADS;
   auto kernel = (face & 2) ? k_adj_particles<true> : k_adj_particles<false>;
@@ -365,7 +368,8 @@ void adj_launch_particles(const GridDev &g, const float *E3, const float *Hh3,
   cudaGetDevice(&dev);
   cudaDeviceGetAttribute(&nsm, cudaDevAttrMultiProcessorCount, dev);
   const long long blocks = std::min<long long>(nchunks, (long long)bpsm * nsm);
-  kernel<<<(int)std::max<long long>(blocks, 1), ADJ_THREADS, 0, st>>>(g, E3, Hh3, S, A, face);
+  kernel<<<(int)std::max<long long>(blocks, 1), ADJ_THREADS, 0, st>>>(g, E3, Hh3, S, A, face,
+                                                                         face_h);
 }
 
 void adj_launch_inject(const AdjSpeciesDev &S, long long start, long long count, double dt,

@@ -32,6 +32,9 @@ struct Consts {
   T kphi, kz, kr;  // deposition prefactors per unit weight
   int nr, nz;   // grid nodes
   int bunch;    // 1: outer walls remove the particle
+  T face_h = T(0);  // > 0: the gather jump terms from the particles within
+                   // face_h (cells) of each jump, a box-kernel estimate of
+                   // the density there; 0: density uniform inside each cell
   int face;     // bit 0: expected jump terms of the radial gather weights;
                 // bit 1: expected jump terms of the wall reflections;
                 // bit 2: the gather terms with the wall cells' particles in
@@ -437,22 +440,39 @@ PDP3_HD void piece_outputs(const Consts<T> &C, const Tape<T> &tp, int p, T out[4
 // r > r_max - dr/2, so the axis cell and the last cell hold their particles
 // in the half next to the other cells, twice as dense: there a particle
 // carries the whole jump of the face on that side and none of the other.
+// face_h > 0 replaces the uniform-density shares by a box-kernel estimate
+// of the density at each jump: a particle within face_h (in cells) of a jump
+// carries that jump / (2 face_h), others none of it.  In expectation this
+// equals the uniform shares where the density is linear inside the cell,
+// and it follows the density where it is not (a wake's compressed electrons,
+// half-filled wall cells).
 template <typename T>
 PDP3_HD T radial_jump(const Tape<T> &tp, T f0, T f1, T f2, T f3, T wz0, T wz1, bool rh,
-                      bool wall_cells, int nr) {
+                      bool wall_cells, int nr, T face_h) {
   const int i = tp.i;
   const T lo = wz0 * f0 + wz1 * f2, hi = wz0 * f1 + wz1 * f3;
   if (!rh) {
     // nodes i, i+1: top face jump uses f_{i+1}, bottom face (i >= 1) f_i
     const T top = hi / T(i + 2);
     const T bottom = i >= 1 ? lo / T(i + 1) : T(0);
+    if (face_h > T(0)) {
+      T s = T(0);
+      if (tp.a > T(1) - face_h) s += top / (T(2) * face_h);
+      if (tp.a < face_h) s += bottom / (T(2) * face_h);
+      return s;
+    }
     if (wall_cells && i == 0) return top;
     if (wall_cells && i == nr - 2) return bottom;
     return T(0.5) * (top + bottom);
   }
   if (i < 1) return T(0);
   const T fi = tp.ir_h == i ? lo : hi;  // node i is the inner node when ir = i
-  return fi * T(2 * i + 1) / (T(2) * T(i + 1) * T(i + 2));
+  const T jump = fi * T(2 * i + 1) / (T(2) * T(i + 1) * T(i + 2));
+  if (face_h > T(0)) {
+    const T d = tp.a - T(0.5);  // the jump sits at the cell middle
+    return (d < face_h && d > -face_h) ? jump / (T(2) * face_h) : T(0);
+  }
+  return jump;
 }
 
 // adjoint of one gathered component: lv = adjoint of the gathered value;
@@ -471,7 +491,8 @@ PDP3_HD void gather_rev(const Consts<T> &C, const Tape<T> &tp, const T f[4], boo
   l_a += lv * (wz0 * (f0 * dwr0 + f1 * dwr1) + wz1 * (f2 * dwr0 + f3 * dwr1));
   // d wz0 / db = -1, d wz1 / db = +1 for both the node and the half-node weights
   l_b += lv * (-(f0 * wr0 + f1 * wr1) + (f2 * wr0 + f3 * wr1));
-  if (C.face & 1) l_a += lv * radial_jump(tp, f0, f1, f2, f3, wz0, wz1, rh, C.face & 4, C.nr);
+  if (C.face & 1)
+    l_a += lv * radial_jump(tp, f0, f1, f2, f3, wz0, wz1, rh, C.face & 4, C.nr, C.face_h);
 }
 
 // The walls reflect a particle whose end point lies beyond them: the end

@@ -2033,6 +2033,7 @@ struct pdp3g_adjoint {
   std::vector<double> cap_t;
   bool have_forward = false;
   int face_terms = PDP3G_ADJ_DEFAULT_JUMPS;
+  float face_h = PDP3G_ADJ_DEFAULT_FACE_WIDTH;  // adj::Consts::face_h
   double loss = 0;
   float fwd_ms = 0, bwd_ms = 0;
   cudaEvent_t ev0 = nullptr, ev1 = nullptr;
@@ -2169,7 +2170,7 @@ void adj_reverse_step(pdp3g_adjoint *a, int cap) {
     AdjSpeciesDev S = a->ls[j];
     S.st = sp.f32;
     S.st = slot_view(a, j, cap);
-    adj_launch_particles(ctx->g, E3, E3 + 3 * ng, S, a->A, a->face_terms, st);
+    adj_launch_particles(ctx->g, E3, E3 + 3 * ng, S, a->A, a->face_terms, a->face_h, st);
     if (sp.is_bunch) {
       long long start, count;
       inject_range(ctx, sp, a->cap_t[cap], start, count);
@@ -2401,5 +2402,11 @@ pdp3g_status pdp3g_adjoint_set_jump_terms(pdp3g_adjoint *a, uint32_t terms) {
   const uint32_t all = PDP3G_ADJ_GATHER_JUMPS | PDP3G_ADJ_WALL_JUMPS | PDP3G_ADJ_WALL_CELLS;
   if (!a || (terms & ~all)) return PDP3G_INVALID_ARG;
   a->face_terms = (int)terms;  // the bits of adj::Consts::face
+  return PDP3G_OK;
+}
+
+pdp3g_status pdp3g_adjoint_set_face_width(pdp3g_adjoint *a, double half_width) {
+  if (!a || !(half_width >= 0.0 && half_width <= 0.5)) return PDP3G_INVALID_ARG;
+  a->face_h = (float)half_width;
   return PDP3G_OK;
 }

@@ -153,7 +153,7 @@ static int pathwise() {
 
 // gathered value of a component at radial coordinate x (cells), fixed z weights
 static T gather_at(T x, const T *F0, const T *F1, T b, bool rh, bool zh, bool wall_cells, int nr,
-                   T *dG, T *jump) {
+                   T face_h, T *dG, T *jump) {
   Tape<T> tp;
   tp.i = (int)std::ceil(x) - 1;
   tp.a = x - tp.i;
@@ -166,21 +166,25 @@ static T gather_at(T x, const T *F0, const T *F1, T b, bool rh, bool zh, bool wa
   const T *wz = zh ? tp.wzh : tp.wzn;
   if (dG) *dG = wz[0] * (f[0] * dwr[0] + f[1] * dwr[1]) + wz[1] * (f[2] * dwr[0] + f[3] * dwr[1]);
   if (jump)
-    *jump = radial_jump(tp, f[0], f[1], f[2], f[3], wz[0], wz[1], rh, wall_cells, nr);
+    *jump = radial_jump(tp, f[0], f[1], f[2], f[3], wz[0], wz[1], rh, wall_cells, nr, face_h);
   return wz[0] * (f[0] * wr[0] + f[1] * wr[1]) + wz[1] * (f[2] * wr[0] + f[3] * wr[1]);
 }
 
 // Windows of whole cells; with wall_cells, windows that start in the axis
 // cell at r = dr/2 or end in the last cell (nr - 2) at r = r_max - dr/2, the
-// parts of those cells that the walls leave to particles.
+// parts of those cells that the walls leave to particles.  Each window is
+// checked with the uniform-density shares (face_h = 0) and with box-kernel
+// shares of half-width 1/4 and 1/8 cell, which count the particles actually
+// near each jump (the wall-cell flag then has no role).
 static int mean_field() {
   double worst = 0;
   int cases = 0;
-  for (int trial = 0; trial < 36; trial++) {
+  for (int trial = 0; trial < 108; trial++) {
+    const T face_h = trial < 36 ? 0.0 : (trial < 72 ? 0.25 : 0.125);
     T F0[64], F1[64];
     for (int j = 0; j < 64; j++) { F0[j] = U(-1, 1) + 2; F1[j] = U(-1, 1) + 2; }
     const bool rh = trial % 2, zh = (trial / 2) % 2;
-    const int wall = trial < 24 ? 0 : 1 + trial % 3 % 2;  // 1: axis cell, 2: last cell
+    const int wall = trial % 36 < 24 ? 0 : 1 + trial % 3 % 2;  // 1: axis cell, 2: last cell
     int i0 = 1 + (int)(rng() % 20), i1 = i0 + 1 + (int)(rng() % 8);
     if (wall == 1) i0 = 0;
     const int nr = wall == 2 ? i1 + 1 : 64;  // with wall == 2 the window ends in cell nr - 2
@@ -199,20 +203,23 @@ static int mean_field() {
     for (int q = q0; q < q1; q++) {
       const T x = i0 + (q + 0.5) / per_cell;
       T dG, jump;
-      gather_at(x, F0, F1, b, rh, zh, wall != 0, nr, &dG, &jump);
+      gather_at(x, F0, F1, b, rh, zh, wall != 0, nr, face_h, &dG, &jump);
       est += dG + jump;
-      mp += gather_at(x + h, F0, F1, b, rh, zh, false, nr, nullptr, nullptr);
-      mm += gather_at(x - h, F0, F1, b, rh, zh, false, nr, nullptr, nullptr);
-      mp2 += gather_at(x + 2 * h, F0, F1, b, rh, zh, false, nr, nullptr, nullptr);
-      mm2 += gather_at(x - 2 * h, F0, F1, b, rh, zh, false, nr, nullptr, nullptr);
+      mp += gather_at(x + h, F0, F1, b, rh, zh, false, nr, 0, nullptr, nullptr);
+      mm += gather_at(x - h, F0, F1, b, rh, zh, false, nr, 0, nullptr, nullptr);
+      mp2 += gather_at(x + 2 * h, F0, F1, b, rh, zh, false, nr, 0, nullptr, nullptr);
+      mm2 += gather_at(x - 2 * h, F0, F1, b, rh, zh, false, nr, 0, nullptr, nullptr);
     }
     const double d1 = (mp - mm) / (2 * h) / n, d2 = (mp2 - mm2) / (4 * h) / n;
     const double fd = 2 * d1 - d2, ad = est / n;
-    const double e = std::fabs(fd - ad) / std::fmax(std::fabs(fd), 1e-3);
+    // relative to |fd|, floored at 1e-2 (the field values are in [1, 3]): a
+    // window whose jumps nearly cancel has an fd near 0, and the midpoint
+    // rule's absolute error there (~5e-7) says nothing about the shares
+    const double e = std::fabs(fd - ad) / std::fmax(std::fabs(fd), 1e-2);
     if (e > worst) worst = e;
     if (getenv("ADJ_VERBOSE"))
-      printf("  rh %d zh %d wall %d cells [%d,%d) fd %.6g est %.6g\n", rh, zh, wall, i0, i1, fd,
-             ad);
+      printf("  rh %d zh %d wall %d face_h %.3f cells [%d,%d) fd %.6g est %.6g\n", rh, zh, wall,
+             face_h, i0, i1, fd, ad);
     cases++;
   }
   printf("mean field: %d windows, worst rel err %.3g\n", cases, worst);
