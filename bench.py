@@ -769,6 +769,14 @@ def run_adjoint(args, rank, world, local_rank, dist=None):
         adj.set_jump_terms(*terms)
         adj.backward()
         g_var[name] = grad(True)
+    # the jump densities: uniform inside each cell (face width 0) and a
+    # narrower box kernel than the default 1/8 cell
+    adj.set_mode("mean_field")
+    for hw in (0.0, 0.0625):
+        adj.set_face_width(hw)
+        adj.backward()
+        g_var["face_width_%g" % hw] = grad(True)
+    adj.set_face_width(0.125)
     adj.set_mode("pathwise")
     adj.backward()
     g_pw = grad(False)
@@ -792,6 +800,16 @@ def run_adjoint(args, rank, world, local_rank, dist=None):
                  "rel_err_pathwise": (g_pw[j] - slope) / slope}
         for name, g in g_var.items():
             fd[j]["rel_err_" + name] = (g[j] - slope) / slope
+        if j == W.N_BUMPS:
+            # gamma: a second fit over +-1% with 16 points (the loss is a
+            # staircase of small jumps; past about +-2% the injection's
+            # ceil(duration / dt) changes the particles injected per step)
+            s1, se1 = fitted_fd_slope(api, W, fam, theta, j, steps, probe, hmax=0.01, npts=8)
+            fd[j]["fd_pm1pct_16pts"] = s1
+            fd[j]["fd_pm1pct_16pts_se"] = se1
+            fd[j]["rel_err_mean_field_vs_pm1pct"] = (g_mf[j] - s1) / s1
+            for name, g in g_var.items():
+                fd[j]["rel_err_%s_vs_pm1pct" % name] = (g[j] - s1) / s1
     dens = [j for j in params if j < W.N_BUMPS]
     summary = {}
     if dens:

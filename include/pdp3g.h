@@ -399,11 +399,11 @@ pdp3g_status pdp3g_adjoint_set_mode(pdp3g_adjoint *a, int32_t mode);
 enum { PDP3G_ADJ_GATHER_JUMPS = 1, PDP3G_ADJ_WALL_JUMPS = 2, PDP3G_ADJ_WALL_CELLS = 4,
        PDP3G_ADJ_DEFAULT_JUMPS = PDP3G_ADJ_GATHER_JUMPS };
 pdp3g_status pdp3g_adjoint_set_jump_terms(pdp3g_adjoint *a, uint32_t terms);
-/* The density the gather jump terms use: 0 (PDP3G_ADJ_DEFAULT_FACE_WIDTH)
-   takes it uniform inside each cell; half_width in (0, 0.5] (cells) estimates
-   it at each jump from the particles within half_width of it (a box
-   kernel), which follows densities that are not uniform inside a cell. */
-#define PDP3G_ADJ_DEFAULT_FACE_WIDTH 0.0
+/* The density the gather jump terms use: 0 takes it uniform inside each
+   cell; half_width in (0, 0.5] (cells) estimates it at each jump from the
+   particles within half_width of it (a box kernel), which follows densities
+   that are not uniform inside a cell.  Default 1/8 cell. */
+#define PDP3G_ADJ_DEFAULT_FACE_WIDTH 0.125
 pdp3g_status pdp3g_adjoint_set_face_width(pdp3g_adjoint *a, double half_width);
 /* device time of the last forward and backward calls */
 pdp3g_status pdp3g_adjoint_timing(pdp3g_adjoint *a, double *forward_ms, double *backward_ms);
