@@ -395,7 +395,10 @@ pdp3g_status pdp3g_adjoint_set_mode(pdp3g_adjoint *a, int32_t mode);
    PDP3G_ADJ_WALL_CELLS    the walls leave the axis cell's and the last
                            radial cell's particles in the half next to the
                            other cells (r >= dr/2, r <= r_max - dr/2), twice
-                           as dense; without it those cells count as full. */
+                           as dense; without it those cells count as full.
+                           Applies to the uniform jump density (face width
+                           0): the box kernel counts the particles that are
+                           there. */
 enum { PDP3G_ADJ_GATHER_JUMPS = 1, PDP3G_ADJ_WALL_JUMPS = 2, PDP3G_ADJ_WALL_CELLS = 4,
        PDP3G_ADJ_DEFAULT_JUMPS = PDP3G_ADJ_GATHER_JUMPS };
 pdp3g_status pdp3g_adjoint_set_jump_terms(pdp3g_adjoint *a, uint32_t terms);

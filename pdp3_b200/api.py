@@ -553,7 +553,8 @@ class Adjoint:
         """The mean-field terms one by one: any of "gather" (the gather
         weights' jumps), "walls" (the momentum jumps of wall reflections),
         "wall_cells" (the axis and last radial cells hold their particles in
-        the half the walls leave them); none = pathwise."""
+        the half the walls leave them; with the uniform jump density only,
+        face width 0); none = pathwise."""
         bits = {"gather": 1, "walls": 2, "wall_cells": 4}
         self.sim._check(self.L.pdp3g_adjoint_set_jump_terms(
             self.h, sum(bits[t] for t in set(terms))), "adjoint_set_jump_terms")
@@ -561,8 +562,8 @@ class Adjoint:
     def set_face_width(self, half_width):
         """0: gather jump terms for a density uniform in each cell; h in
         (0, 0.5]: a box-kernel density estimate of half-width h cells."""
-        self._check(self.L.pdp3g_adjoint_set_face_width(self.h, float(half_width)),
-                    "adjoint_set_face_width")
+        self.sim._check(self.L.pdp3g_adjoint_set_face_width(self.h, float(half_width)),
+                        "adjoint_set_face_width")
 
     def timing(self):
         f, b = ctypes.c_double(), ctypes.c_double()

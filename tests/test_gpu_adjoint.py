@@ -134,10 +134,13 @@ def test_backward_restores_forward_end_state_and_rejects_misuse():
 
 
 def test_jump_terms_select_the_mean_field_parts():
+    """With the uniform jump density (face width 0), where the wall-cell
+    term applies; the box-kernel default is exercised by the config-4 test."""
     th = W.adjoint_theta()
     wl, aux = W.AdjointFamily(th, **SMALL).workload(th)
     sim = api.from_workload(wl, precision="fp32")
     adj = api.Adjoint(sim, 40, 15, PROBE)
+    adj.set_face_width(0.0)
     adj.forward()
     grads = {}
     for name, select in [("pathwise", lambda: adj.set_mode("pathwise")),
@@ -155,5 +158,15 @@ def test_jump_terms_select_the_mean_field_parts():
     assert not np.allclose(grads["all"], grads["gather"], rtol=1e-6, atol=0)
     with pytest.raises(api.Pdp3gError):
         sim._check(adj.L.pdp3g_adjoint_set_jump_terms(adj.h, 8), "adjoint_set_jump_terms")
+    for bad in (-0.1, 0.6):
+        with pytest.raises(api.Pdp3gError):
+            adj.set_face_width(bad)
+    # the box kernel moves the gradient away from the uniform shares
+    adj.set_mode("mean_field")
+    adj.set_face_width(0.125)
+    adj.backward()
+    g_box = np.array(W.adjoint_gradient(
+        wl, aux, [adj.species(0), adj.species(1)], adj.species(2), adj.bunch_velocity(2)))
+    assert not np.allclose(g_box, grads["default"], rtol=1e-6, atol=0)
     adj.close()
     sim.close()

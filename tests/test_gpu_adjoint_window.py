@@ -39,6 +39,13 @@ def test_config4_window_gradient_and_cost():
     fam = W.AdjointFamily(theta)
     wl, aux = fam.workload(theta)
     probe = W.ADJOINT_PROBE
+    # warm-up window on a context of its own (first launches of every kernel)
+    warm = api.from_workload(wl, precision="fp32")
+    wa = api.Adjoint(warm, 2 * INTERVAL, INTERVAL, probe)
+    wa.forward()
+    wa.backward()
+    wa.close()
+    warm.close()
     sim = api.from_workload(wl, precision="fp32")
     adj = api.Adjoint(sim, STEPS, INTERVAL, probe)
     adj.forward()
