@@ -769,6 +769,23 @@ static cudaError_t phase_reset_j(pdp3g_ctx *ctx) {
   return cudaMemsetAsync(ctx->g.jr, 0, sizeof(double) * ng * 3, ctx->stream);
 }
 
+// Species fork/join: with two or more species, every second species runs on
+// the context's side stream between these two (the species only share
+// atomic sums into the grids).
+static cudaError_t species_fork(pdp3g_ctx *ctx) {
+  if (ctx->species.size() < 2) return cudaSuccess;
+  cudaError_t e = cudaEventRecord(ctx->ev_fork, ctx->stream);
+  return e != cudaSuccess ? e : cudaStreamWaitEvent(ctx->stream_side, ctx->ev_fork, 0);
+}
+static cudaError_t species_join(pdp3g_ctx *ctx) {
+  if (ctx->species.size() < 2) return cudaSuccess;
+  cudaError_t e = cudaEventRecord(ctx->ev_join, ctx->stream_side);
+  return e != cudaSuccess ? e : cudaStreamWaitEvent(ctx->stream, ctx->ev_join, 0);
+}
+static cudaStream_t species_stream(const pdp3g_ctx *ctx, size_t j) {
+  return ctx->species.size() >= 2 && (j & 1) ? ctx->stream_side : ctx->stream;
+}
+
 // ParticlesList::step_v + full_current_distribution (src/particlesList.cpp:20-54).
 // Species are independent apart from their sums into J (atomics), so with
 // two or more species every second one runs on the side stream: the last,
@@ -2146,29 +2163,33 @@ pdp3g_status adj_forward_step(pdp3g_adjoint *a, int cap) {
   CK(cudaMemcpyAsync(a->cap_fields + (size_t)cap * 6 * ng, ctx->mirror, sizeof(float) * 6 * ng,
                      cudaMemcpyDeviceToDevice, ctx->stream));
   CK(phase_reset_j(ctx));
+  CK(species_fork(ctx));
   for (size_t j = 0; j < ctx->species.size(); j++) {
     const SpeciesF32 in = slot_view(a, j, cap), nx = slot_view(a, j, cap + 1);
     launch_push_deposit_f32_to(ctx->g, in, in_place(nx), ctx->cfg.pusher, ctx->n_sm,
-                               ctx->f32_blocks_per_sm, ctx->stream);
+                               ctx->f32_blocks_per_sm, species_stream(ctx, j));
     ctx->launches++;
     ctx->particle_launches++;
   }
+  CK(species_join(ctx));
   phase_calc_e(ctx);
   phase_advance(ctx);
   return PDP3G_OK;
 }
 
-// reverse of the step stored in capture slot cap
-void adj_reverse_step(pdp3g_adjoint *a, int cap) {
+// reverse of the step stored in capture slot cap; the species' reverses on
+// two streams as in the forward step
+cudaError_t adj_reverse_step(pdp3g_adjoint *a, int cap) {
   pdp3g_ctx *ctx = a->ctx;
   const size_t ng = (size_t)ctx->cfg.n_grid_r * ctx->cfg.n_grid_z;
-  cudaStream_t st = ctx->stream;
-  adj_launch_e(ctx->g, a->A, st);
+  adj_launch_e(ctx->g, a->A, ctx->stream);
   const float *E3 = a->cap_fields + (size_t)cap * 6 * ng;
+  cudaError_t e = species_fork(ctx);
+  if (e != cudaSuccess) return e;
   for (size_t j = 0; j < ctx->species.size(); j++) {
     const Species &sp = ctx->species[j];
+    const cudaStream_t st = species_stream(ctx, j);
     AdjSpeciesDev S = a->ls[j];
-    S.st = sp.f32;
     S.st = slot_view(a, j, cap);
     adj_launch_particles(ctx->g, E3, E3 + 3 * ng, S, a->A, a->face_terms, a->face_h, st);
     if (sp.is_bunch) {
@@ -2178,7 +2199,9 @@ void adj_reverse_step(pdp3g_adjoint *a, int cap) {
                         a->d_lv + j, st);
     }
   }
-  adj_launch_h(ctx->g, a->A, st);
+  if ((e = species_join(ctx)) != cudaSuccess) return e;
+  adj_launch_h(ctx->g, a->A, ctx->stream);
+  return cudaGetLastError();
 }
 
 pdp3g_status adj_fail(pdp3g_adjoint *a, pdp3g_status st, const std::string &m) {
@@ -2332,7 +2355,7 @@ pdp3g_status pdp3g_backward_window(pdp3g_adjoint *a) {
       pdp3g_status fs = adj_forward_step(a, s - s0);
       if (fs != PDP3G_OK) return fs;
     }
-    for (int s = s1 - 1; s >= s0; s--) adj_reverse_step(a, s - s0);
+    for (int s = s1 - 1; s >= s0; s--) CK(adj_reverse_step(a, s - s0));
   }
   rs = adj_restore_checkpoint(a, a->nwin);
   if (rs != PDP3G_OK) return rs;
