@@ -233,6 +233,10 @@ pdp3g_status pdp3g_create(const pdp3g_config *cfg, pdp3g_ctx **out) {
       !(cfg->dt > 0) || cfg->pusher < 0 || cfg->pusher > 2 ||
       (cfg->precision != PDP3G_FP64 && cfg->precision != PDP3G_FP32_CELL))
     return PDP3G_INVALID_ARG;
+  // the FP32 form's int32 cell index and 32-bit node offsets
+  if (cfg->precision == PDP3G_FP32_CELL &&
+      (long long)cfg->n_grid_r * cfg->n_grid_z >= (1LL << 31))
+    return PDP3G_INVALID_ARG;
   // an ordinal past the last device is the caller's error; checked first so
   // that no CUDA error is left pending on the calling thread
   int ndev = 0;

@@ -5,7 +5,10 @@
 
 namespace pdp3g {
 
-#define GIDX(i, k) ((size_t)(i) * (size_t)g.nz + (size_t)(k))
+// node offset i * n_grid_z + k in 32-bit arithmetic (FP32 contexts hold
+// fewer than 2^31 nodes, checked at creation): one multiply-add instead of
+// a 64-bit one per address
+#define GIDX(i, k) ((unsigned)(i) * (unsigned)g.nz + (unsigned)(k))
 
 constexpr int F32_THREADS = 256;
 constexpr int F32_MIN_BLOCKS = 4;                     // CTAs per SM (64 registers)
@@ -17,21 +20,14 @@ static_assert(F32_CHUNK == F32_WARPS * F32_WARP_CHUNK, "CTA chunk = its warps' c
 __device__ __forceinline__ void flag32(const GridDev &g, unsigned bit) { atomicOr(g.err, bit); }
 
 // moves (i, f) so that f is in (0, 1] (CELL_NUMBER semantics); cells below
-// 0 clamp to 0 like the upstream "sometimes it gives -1" workaround.
+// 0 clamp to 0 like the upstream "sometimes it gives -1" workaround.  c =
+// ceil(f) - 1 cells in one step, branch-free; for a move of at most one cell
+// (all that a step at Courant 0.5 makes) f - c is the same subtraction of 1
+// as a cell-by-cell loop would make.
 __device__ __forceinline__ void renorm(int &i, float &f) {
-  // one cell is the usual move; up to 4 in each direction
-  if (f > 1.0f) {
-    f -= 1.0f;
-    i += 1;
-#pragma unroll 1
-    for (int it = 1; it < 4 && f > 1.0f; it++) { f -= 1.0f; i += 1; }
-  }
-  if (f <= 0.0f) {
-    f += 1.0f;
-    i -= 1;
-#pragma unroll 1
-    for (int it = 1; it < 4 && f <= 0.0f; it++) { f += 1.0f; i -= 1; }
-  }
+  const float c = ceilf(f) - 1.0f;
+  i += (int)c;
+  f -= c;
   if (i < 0) { f = f + (float)i; i = 0; }
 }
 
