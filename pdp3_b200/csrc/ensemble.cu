@@ -70,7 +70,6 @@ __device__ void ens_inject(const EnsembleDev &E, const EnsSpecies &sp) {
 template <int PUSHER>
 __global__ void __launch_bounds__(F32_THREADS, F32_MIN_BLOCKS) k_ensemble(EnsembleDev E) {
   const int nsteps = *(volatile int *)&E.status[2];
-  const long long budget = *(volatile const long long *)E.budget_cycles;
   cg::grid_group grid = cg::this_grid();
   __shared__ F32Shared sm;
   __shared__ struct {
@@ -78,14 +77,18 @@ __global__ void __launch_bounds__(F32_THREADS, F32_MIN_BLOCKS) k_ensemble(Ensemb
     SpeciesF32 s;
     int pusher;
   } desc;
-  const long long gtid = (long long)blockIdx.x * blockDim.x + threadIdx.x;
-  const long long gstride = (long long)gridDim.x * blockDim.x;
-  const long long t_start = clock64();
+  // thread 0 alone tests the cancel flag and the budget: its start clock
+  // lives in shared memory, not in every thread's registers
+  __shared__ long long t_start_sh;
+  if (threadIdx.x == 0) t_start_sh = clock64();
   for (int step = 0; step < nsteps; step++) {
+    const long long gtid = (long long)blockIdx.x * blockDim.x + threadIdx.x;
+    const long long gstride = (long long)gridDim.x * blockDim.x;
     if (gtid == 0) {
       int stop = 0;
+      const long long budget = *(volatile const long long *)E.budget_cycles;
       if (*E.cancel) stop = 1;
-      else if (budget > 0 && clock64() - t_start > budget) stop = 2;
+      else if (budget > 0 && clock64() - t_start_sh > budget) stop = 2;
       E.status[1] = stop;
       __threadfence();
     }
@@ -117,9 +120,10 @@ __global__ void __launch_bounds__(F32_THREADS, F32_MIN_BLOCKS) k_ensemble(Ensemb
     // and species descriptors in shared memory, where they cannot alias the
     // grids and particle arrays that the chunk loop writes.
     for (int sp = 0; sp < E.nspecies; sp++) {
-      const long long cb = E.species[sp].chunk_begin;
-      const long long ce = sp + 1 < E.nspecies ? E.species[sp + 1].chunk_begin : E.total_chunks;
-      long long first = cb + (((long long)blockIdx.x - cb) % gridDim.x + gridDim.x) % gridDim.x;
+      const int cb = (int)E.species[sp].chunk_begin;
+      const int ce = (int)(sp + 1 < E.nspecies ? E.species[sp + 1].chunk_begin : E.total_chunks);
+      const int G = (int)gridDim.x;
+      int first = cb + (((int)blockIdx.x - cb) % G + G) % G;
       if (first >= ce) continue;
       __syncthreads();
       if (threadIdx.x == 0) {
@@ -128,7 +132,7 @@ __global__ void __launch_bounds__(F32_THREADS, F32_MIN_BLOCKS) k_ensemble(Ensemb
         desc.pusher = E.runs[E.species[sp].run].pusher;
       }
       __syncthreads();
-      for (long long c = first; c < ce; c += gridDim.x)
+      for (int c = first; c < ce; c += G)
         f32_chunk<false, PUSHER>(desc.g, desc.s, SpeciesOut{}, desc.pusher, c - cb, sm);
     }
     grid.sync();
