@@ -635,6 +635,7 @@ def run_ensemble(args, rank, world, local_rank, dist=None):
                                 % args.ensemble_scale,
                        "parallelism": "replicas x%d" % world},
             "ensemble": {"mode": chosen, "blocks_per_sm": info["blocks_per_sm"],
+                         "graph_blocks_per_sm": info["graph_blocks_per_sm"],
                          "blocks": info["blocks"], "cuda_graph": bool(info["used_graph"]),
                          "ms_per_step": ms / args.steps,
                          "modes": {m: dict(v, value=alive_all * args.steps /
@@ -643,8 +644,9 @@ def run_ensemble(args, rank, world, local_rank, dist=None):
                                            v["ms_per_step"])
                                    for m, v in modes.items()},
                          "autotuner": "persistent kernel at every feasible CTAs-per-SM "
-                                      "count and the step graph, 2 steps each; the fastest "
-                                      "is kept"},
+                                      "count and the step graph with the runs' particle "
+                                      "kernels at 2, 4 and 8 CTAs per SM, 2 steps each; "
+                                      "the fastest is kept"},
             "sequential": {"value": seq_value, "ms_per_step": seq_ms_max / args.steps,
                            "kernel_ms_per_step": seq_kernel_ms / args.steps,
                            "note": "same runs, each stepped alone with per-run launches; "

@@ -323,14 +323,16 @@ typedef struct {
   int64_t last_steps_done;
   int64_t particles;         /* macroparticle slots over all runs */
   int32_t mode;              /* PDP3G_ENS_PERSISTENT or PDP3G_ENS_STEP_GRAPH */
-  int32_t reserved;
+  int32_t graph_blocks_per_sm; /* CTAs per SM of the runs' particle kernels in the
+                                  step graph (0: each context's own) */
 } pdp3g_ensemble_stats;
 pdp3g_status pdp3g_ensemble_create(pdp3g_ctx *const *runs, int32_t n_runs, pdp3g_ensemble **out);
 pdp3g_status pdp3g_ensemble_run(pdp3g_ensemble *e, int32_t nsteps);
 /* times the persistent kernel at every feasible CTAs-per-SM count and the
-   step-graph mode, steps_per_trial steps each (the trial steps advance the
-   runs), and keeps the fastest; *blocks_per_sm receives the persistent
-   kernel's count, or 0 when the step graph won */
+   step graph with the runs' particle kernels at 2, 4 and 8 CTAs per SM,
+   steps_per_trial steps each (the trial steps advance the runs), and keeps
+   the fastest; *blocks_per_sm receives the persistent kernel's count, or 0
+   when the step graph won (its count: pdp3g_ensemble_info) */
 pdp3g_status pdp3g_ensemble_autotune(pdp3g_ensemble *e, int32_t steps_per_trial,
                                      int32_t *blocks_per_sm);
 /* PDP3G_ENS_PERSISTENT (the default) or PDP3G_ENS_STEP_GRAPH */

@@ -54,7 +54,7 @@ class EnsembleInfo(ctypes.Structure):
                 ("blocks", ctypes.c_int32), ("used_graph", ctypes.c_int32),
                 ("last_ms", ctypes.c_double), ("last_steps_done", ctypes.c_int64),
                 ("particles", ctypes.c_int64), ("mode", ctypes.c_int32),
-                ("reserved", ctypes.c_int32)]
+                ("graph_blocks_per_sm", ctypes.c_int32)]
 
 
 class Timing(ctypes.Structure):

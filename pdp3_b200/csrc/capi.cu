@@ -1539,6 +1539,7 @@ struct pdp3g_ensemble {
   std::string last_error;
   // step-graph mode: one captured graph of one step of every run
   int mode = PDP3G_ENS_PERSISTENT;
+  int graph_bpsm = 0;  // CTAs per SM of the runs' particle kernels in the step graph (0: theirs)
   cudaGraph_t step_graph = nullptr;
   cudaGraphExec_t step_exec = nullptr;
   cudaEvent_t ev_fork = nullptr;
@@ -1748,8 +1749,19 @@ static pdp3g_status ens_capture_step(pdp3g_ensemble *e) {
     EK(cudaEventCreateWithFlags(&ev, cudaEventDisableTiming));
     e->ev_join.push_back(ev);
   }
-  EK(cudaStreamBeginCapture(e->stream, cudaStreamCaptureModeThreadLocal));
-  cudaError_t ce = ensemble_inject_all(e->dev, e->stream);
+  // the runs' particle kernels take the step graph's CTAs-per-SM count while
+  // it is captured; each context keeps its own for its own steps
+  std::vector<int> own_bpsm;
+  for (auto *c : e->runs) {
+    own_bpsm.push_back(c->f32_blocks_per_sm);
+    if (e->graph_bpsm > 0) c->f32_blocks_per_sm = e->graph_bpsm;
+  }
+  cudaError_t ce = cudaStreamBeginCapture(e->stream, cudaStreamCaptureModeThreadLocal);
+  if (ce != cudaSuccess) {
+    for (size_t r = 0; r < e->runs.size(); r++) e->runs[r]->f32_blocks_per_sm = own_bpsm[r];
+    return ens_fail(e, PDP3G_CUDA_ERROR, cudaGetErrorString(ce));
+  }
+  ce = ensemble_inject_all(e->dev, e->stream);
   if (ce == cudaSuccess) ce = cudaEventRecord(e->ev_fork, e->stream);
   for (size_t r = 0; r < e->runs.size() && ce == cudaSuccess; r++) {
     pdp3g_ctx *ctx = e->runs[r];
@@ -1766,6 +1778,7 @@ static pdp3g_status ens_capture_step(pdp3g_ensemble *e) {
   if (ce == cudaSuccess) ce = ensemble_advance(e->dev, e->stream);
   cudaGraph_t g = nullptr;
   cudaError_t ce2 = cudaStreamEndCapture(e->stream, &g);
+  for (size_t r = 0; r < e->runs.size(); r++) e->runs[r]->f32_blocks_per_sm = own_bpsm[r];
   if (ce == cudaSuccess) ce = ce2;
   if (ce == cudaSuccess) ce = cudaGraphInstantiate(&e->step_exec, g, 0);
   if (ce != cudaSuccess) {
@@ -1959,12 +1972,33 @@ pdp3g_status pdp3g_ensemble_autotune(pdp3g_ensemble *e, int32_t steps_per_trial,
     }
   }
   e->blocks_per_sm = best_b;
-  // the step graph (its capture and first replay are untimed: one warm-up step)
+  // the step graph at 2, 4 and 8 CTAs per SM for the runs' particle kernels
+  // (each capture and its first replay untimed: one warm-up step)
   e->mode = PDP3G_ENS_STEP_GRAPH;
   float ms_graph = 0;
-  pdp3g_status st = ens_run(e, 1, false, nullptr);
-  if (st == PDP3G_OK) st = ens_run(e, steps_per_trial, false, &ms_graph);
-  if (st != PDP3G_OK) return st;
+  int best_g = 0;
+  for (int gb : {2, 4, 8}) {
+    if (e->step_exec) cudaGraphExecDestroy(e->step_exec);
+    if (e->step_graph) cudaGraphDestroy(e->step_graph);
+    e->step_exec = nullptr;
+    e->step_graph = nullptr;
+    e->graph_bpsm = gb;
+    float ms = 0;
+    pdp3g_status st = ens_run(e, 1, false, nullptr);
+    if (st == PDP3G_OK) st = ens_run(e, steps_per_trial, false, &ms);
+    if (st != PDP3G_OK) return st;
+    if (best_g == 0 || ms < ms_graph) {
+      ms_graph = ms;
+      best_g = gb;
+    }
+  }
+  if (best_g != e->graph_bpsm) {
+    cudaGraphExecDestroy(e->step_exec);
+    cudaGraphDestroy(e->step_graph);
+    e->step_exec = nullptr;
+    e->step_graph = nullptr;
+    e->graph_bpsm = best_g;
+  }
   e->mode = ms_graph < best ? PDP3G_ENS_STEP_GRAPH : PDP3G_ENS_PERSISTENT;
   if (blocks_per_sm) *blocks_per_sm = e->mode == PDP3G_ENS_STEP_GRAPH ? 0 : best_b;
   return PDP3G_OK;
@@ -2005,7 +2039,7 @@ pdp3g_status pdp3g_ensemble_info(pdp3g_ensemble *e, pdp3g_ensemble_stats *out) {
   out->last_steps_done = e->last_steps_done;
   out->particles = e->total_particles;
   out->mode = e->mode;
-  out->reserved = 0;
+  out->graph_blocks_per_sm = e->graph_bpsm;
   return PDP3G_OK;
 }
 
