@@ -1,5 +1,6 @@
-"""GPU parity of the FP64 plain form against the oracle on the benchmarked
-grids, through the C ABI.
+"""GPU parity of the FP64 plain form (and, within FP32 rounding, of the FP32
+cell-local form) against the oracle on the benchmarked grids, through the
+C ABI.
 
 The wake grid (257 x 2049 nodes over 0.1 x 0.8 m, gamma = 5 bunch injected
 at z = 0, 10-cell absorbing layer) and the large grid (513 x 4097 nodes,
@@ -15,6 +16,8 @@ Tolerances (FP64):
   * 20 steps with injection: alive flags identical (integer outcome of the
     injection schedule), time bit-identical, grids and particle arrays
     within 1e-9 (rounding differences grow through the coupled update).
+Tolerances (FP32 form, one step): grids within 1e-4 of max|x|, positions
+within 1e-6 of a cell, alive flags identical.
 """
 import numpy as np
 import pytest
@@ -152,3 +155,34 @@ def test_species_on_two_streams_sum_like_species_alone():
         assert np.abs(total[c]).max() > 0, c
         assert rel_inf(together.field(c), total[c]) <= 1e-12, c
     together.close()
+
+
+@pytest.mark.parametrize("case", ["wake", "large"])
+def test_fp32_form_one_step_against_the_oracle(case):
+    """The FP32 cell-local form on the same grids, particles and seeded
+    fields as the FP64 tests above: one step within FP32 rounding of the
+    oracle's FP64 step.  Tolerance 1e-4 of max|x| per grid (an FP32 offset
+    resolves ~6e-8 of a cell; the deposits are summed in FP32 per warp before
+    the FP64 grid add), and positions within 1e-6 of a cell."""
+    if case == "wake":
+        wl = W.wake_config(ppc=PPC, steps=1)
+        seed = 35
+    else:
+        wl = W.large_config(ppc=PPC, steps=1, host_plasma=True, sort_interval=0)
+        seed = 36
+    orc = oracle_from_workload(wl)
+    g32 = api.from_workload(wl, precision="fp32")
+    seed_fields([orc, g32], (wl.n_grid_r, wl.n_grid_z), seed=seed)
+    orc.step()
+    g32.step()
+    g32.sync()
+    for c in ("E_r", "E_phi", "E_z", "H_r", "H_phi", "H_z", "J_r", "J_phi", "J_z"):
+        err = rel_inf(g32.field(c), orc.field(c))
+        assert err <= 1e-4, (case, c, err)
+    for sid in range(3):
+        a, b = g32.species(sid), orc.species(sid)
+        assert np.array_equal(a["alive"], b["alive"]), (case, sid)
+        m = b["alive"].astype(bool)
+        assert float(np.abs(a["r"][m] - b["r"][m]).max()) <= 1e-6 * wl.dr, (case, sid)
+        assert float(np.abs(a["z"][m] - b["z"][m]).max()) <= 1e-6 * wl.dz, (case, sid)
+    g32.close()
