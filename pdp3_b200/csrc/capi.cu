@@ -1804,10 +1804,20 @@ static pdp3g_status ens_segment_graph(pdp3g_ensemble *e, int nsteps, float *ms_o
   const int init[4] = {0, 0, nsteps, 0};
   EK(cudaMemcpyAsync(e->d_status, init, sizeof(init), cudaMemcpyHostToDevice, e->stream));
   constexpr int kInFlight = 8;
-  cudaEvent_t start, mark[kInFlight];
-  EK(cudaEventCreate(&start));
-  for (int i = 0; i < kInFlight; i++) cudaEventCreate(&mark[i]);
-  cudaEventRecord(start, e->stream);
+  cudaEvent_t start = nullptr, end = nullptr, mark[kInFlight] = {};
+  auto free_events = [&]() {
+    if (start) cudaEventDestroy(start);
+    if (end) cudaEventDestroy(end);
+    for (int i = 0; i < kInFlight; i++)
+      if (mark[i]) cudaEventDestroy(mark[i]);
+  };
+  bool made = cudaEventCreate(&start) == cudaSuccess && cudaEventCreate(&end) == cudaSuccess;
+  for (int i = 0; i < kInFlight && made; i++) made = cudaEventCreate(&mark[i]) == cudaSuccess;
+  if (!made || cudaEventRecord(start, e->stream) != cudaSuccess) {
+    free_events();
+    cudaGetLastError();
+    return ens_fail(e, PDP3G_CUDA_ERROR, "step graph: timing events");
+  }
   int launched = 0, st_code = 0;
   cudaError_t err = cudaSuccess;
   e->last_used_graph = true;
@@ -1824,15 +1834,11 @@ static pdp3g_status ens_segment_graph(pdp3g_ensemble *e, int nsteps, float *ms_o
     if ((err = cudaGraphLaunch(e->step_exec, e->stream)) != cudaSuccess) break;
     cudaEventRecord(mark[launched % kInFlight], e->stream);
   }
-  cudaEvent_t end;
-  cudaEventCreate(&end);
   cudaEventRecord(end, e->stream);
   cudaError_t sync = cudaStreamSynchronize(e->stream);
   float ms = 0;
   cudaEventElapsedTime(&ms, start, end);
-  cudaEventDestroy(start);
-  cudaEventDestroy(end);
-  for (int i = 0; i < kInFlight; i++) cudaEventDestroy(mark[i]);
+  free_events();
   if (err != cudaSuccess) return ens_fail(e, PDP3G_CUDA_ERROR, cudaGetErrorString(err));
   if (sync != cudaSuccess) return ens_fail(e, PDP3G_CUDA_ERROR, cudaGetErrorString(sync));
   for (auto *c : e->runs) {
