@@ -1,7 +1,8 @@
 """Benchmark of the PDP3 per-timestep PIC loop on B200.
 
     python bench.py [--gpus N] [--steps K] [--warmup W] [--impl ours|reference]
-                    [--precision fp64|fp32] [--workload wake|thermal]
+                    [--precision fp64|fp32]
+                    [--workload wake|thermal|large|ensemble|adjoint]
 
 Workload (default): the beam-plasma wake case, 256 x 2048 cells over
 r in [0, 0.1] m, z in [0, 0.8] m, electrons and protons at 64 macroparticles
