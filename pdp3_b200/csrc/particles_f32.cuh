@@ -532,8 +532,16 @@ __device__ __forceinline__ void f32_warp_chunk(const GridDev &g, const SpeciesF3
       if (alive_now) {
         int rz_i, rz_k;
         float vrz4[4];
-        if (deposit_path(g, i, a, k, b, in, an, kn, bn, s.kz * w, s.kr * w, rz_i, rz_k, vrz4))
+        if (in == i && kn == k) {
+          // the step stays in its cell (all but about one particle-step in
+          // a thousand at thermal speeds): the one piece deposit_path would
+          // make, without its face-crossing logic
+          piece_values(i, a, b, an, bn, s.kz * w, s.kr * w, vrz4);
+          acc_add<1>(g, acc_rz, i * g.nz + k, vrz4);
+        } else if (deposit_path(g, i, a, k, b, in, an, kn, bn, s.kz * w, s.kr * w, rz_i, rz_k,
+                                vrz4)) {
           acc_add<1>(g, acc_rz, rz_i * g.nz + rz_k, vrz4);
+        }
         // back_velocity_to_rz (src/particles.cpp:1005-1015): cos = x/r, sin = y/r
         const float inv_r2 = 1.0f / r2;
         const float st = dy * inv_r2, ct = x2 * inv_r2;
