@@ -585,7 +585,19 @@ PDP3_HD void reverse(const Consts<T> &C, const Tape<T> &tp, T l_an, T l_bn, cons
     l_r2 += -l_ct * tp.ct / tp.r2 - l_st * tp.st / tp.r2;
     l_dy += l_st / tp.r2;
     // ---- r-z path adjoint
-    if (tp.path_ok) {
+    if (tp.path_ok && tp.np == 0) {
+      // the step stays in its cell (almost every step): one piece from
+      // (a, b) to (A, B), the general loop's single iteration
+      const T lo[4] = {l_piece[0][0], l_piece[0][1], l_piece[0][2], l_piece[0][3]};
+      T la0 = 0, lc0 = 0, la1 = 0, lc1 = 0, lkz = 0, lkr = 0;
+      piece_rev(tp.i, tp.qa0, tp.qb0, tp.qa1, tp.qb1, C.kz * tp.w, C.kr * tp.w, lo, la0, lc0,
+                la1, lc1, lkz, lkr);
+      l_w += lkz * C.kz + lkr * C.kr;
+      l_a += la0;
+      l_b += lc0;
+      l_A += la1;
+      l_B += lc1;
+    } else if (tp.path_ok) {
       // adjoints of the path points Q0..Q3, kept in scalars: the piece loop is
       // not unrolled (one copy of piece_rev) and reads the tape through
       // selects, so nothing is indexed at run time
