@@ -361,7 +361,10 @@ void pdp3g_ensemble_destroy(pdp3g_ensemble *e);
    pdp3g_backward_window recomputes each interval from its checkpoint
    (storing every step's particle-phase input) and runs the hand-written
    reverse of each step, last to first; it leaves the context in the state
-   that the forward ended in.  Results, all with respect to the state at the
+   that the forward ended in.  The forward stores the particle-phase inputs
+   of its last interval as it runs them, so the first backward after a
+   forward recomputes every interval but the last (a second backward after
+   the same forward recomputes them all).  Results, all with respect to the state at the
    start of the forward window: per particle dL/dr and dL/dz (per metre),
    dL/du for u = gamma v / c (r, phi, z) and dL/dw (weight); per grid node
    dL/dE and dL/dH; per bunch dL/dv for the beam velocity through the

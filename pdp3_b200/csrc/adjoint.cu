@@ -119,14 +119,16 @@ __device__ __forceinline__ void ladd(const GridDev &g, double *f, int i, int k, 
 }
 
 #ifndef ADJ_THREADS_PER_CTA
-#define ADJ_THREADS_PER_CTA 256
+#define ADJ_THREADS_PER_CTA 128
 #endif
 #ifndef ADJ_MIN_BLOCKS
-#define ADJ_MIN_BLOCKS 2  // CTAs per SM the register budget is sized for (128 registers)
+#define ADJ_MIN_BLOCKS 4  // CTAs per SM the register budget is sized for (128 registers)
 #endif
 // the particle reverse keeps its tape in registers: with the warp-level
-// reduction of the field-node adjoints (no shared tile, no barrier), 2 CTAs
-// of 128 registers per thread beat 4 CTAs of 64 with the tape spilled
+// reduction of the field-node adjoints (no shared tile, no barrier), 512
+// resident threads of 128 registers beat 1024 of 64 with the tape spilled;
+// 128-thread CTAs (4 per SM) end the grid-stride loop with a shorter tail
+// than 256-thread ones (2 per SM)
 constexpr int ADJ_THREADS = ADJ_THREADS_PER_CTA;
 // Warp-level segmented sum over runs of consecutive lanes with the same key
 // (particles sorted by cell, with the same half-cell quadrant, share their

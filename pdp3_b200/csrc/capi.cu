@@ -2093,6 +2093,7 @@ struct pdp3g_adjoint {
                                                // recomputed interval, slot j = step j's input
   std::vector<double> cap_t;
   bool have_forward = false;
+  bool tail_captured = false;  // the capture slots hold the last interval as the forward ran it
   int face_terms = PDP3G_ADJ_DEFAULT_JUMPS;
   float face_h = PDP3G_ADJ_DEFAULT_FACE_WIDTH;  // adj::Consts::face_h
   double loss = 0;
@@ -2152,13 +2153,15 @@ pdp3g_status adj_save_checkpoint(pdp3g_adjoint *a, int idx) {
   return PDP3G_OK;
 }
 
-pdp3g_status adj_restore_checkpoint(pdp3g_adjoint *a, int idx) {
+// particles: also copy the checkpoint's particles into the context's species
+// (the backward's recompute reads them from capture slot 0 instead)
+pdp3g_status adj_restore_checkpoint(pdp3g_adjoint *a, int idx, bool particles = true) {
   pdp3g_ctx *ctx = a->ctx;
   const size_t ng = (size_t)ctx->cfg.n_grid_r * ctx->cfg.n_grid_z;
   CK(cudaMemcpyAsync(comp_ptr(ctx, PDP3G_E_R), a->ck_fields + (size_t)idx * 6 * ng,
                      sizeof(double) * 6 * ng, cudaMemcpyDeviceToDevice, ctx->stream));
   for (int c = PDP3G_E_R; c <= PDP3G_E_Z; c++) refresh_mirror(ctx, c);
-  for (size_t j = 0; j < ctx->species.size(); j++)
+  for (size_t j = 0; particles && j < ctx->species.size(); j++)
     CK(snap_copy(ctx->species[j].f32, a->ck_parts[idx][j], 1, ctx->stream));
   ctx->t = a->ck_t[idx];
   ctx->steps = a->ck_steps[idx];
@@ -2342,15 +2345,24 @@ pdp3g_status pdp3g_forward_window(pdp3g_adjoint *a, double *loss) {
   CK(cudaSetDevice(ctx->device));
   cudaStream_t st = ctx->stream;
   const size_t ng = (size_t)ctx->cfg.n_grid_r * ctx->cfg.n_grid_z;
+  // The last interval runs through the capture slots, as the backward's
+  // recompute would run it, so the first backward reverses it directly.
+  const int tail0 = (a->nwin - 1) * a->interval;
+  a->tail_captured = false;
   CK(cudaEventRecord(a->ev0, st));
   for (int s = 0; s < a->window; s++) {
     if (s % a->interval == 0) {
       pdp3g_status cs = adj_save_checkpoint(a, s / a->interval);
       if (cs != PDP3G_OK) return cs;
     }
-    pdp3g_status fs = adj_forward_step(a, -1);
+    if (s == tail0)
+      for (size_t j = 0; j < ctx->species.size(); j++)
+        CK(snap_copy(ctx->species[j].f32, a->cap_parts[0][j], 0, st));
+    pdp3g_status fs = adj_forward_step(a, s >= tail0 ? s - tail0 : -1);
     if (fs != PDP3G_OK) return fs;
   }
+  for (size_t j = 0; j < ctx->species.size(); j++)
+    CK(snap_copy(ctx->species[j].f32, a->cap_parts[a->window - tail0][j], 1, st));
   pdp3g_status cs = adj_save_checkpoint(a, a->nwin);
   if (cs != PDP3G_OK) return cs;
   CK(cudaMemsetAsync(a->d_loss, 0, sizeof(double), st));
@@ -2362,6 +2374,7 @@ pdp3g_status pdp3g_forward_window(pdp3g_adjoint *a, double *loss) {
   if (ss != PDP3G_OK) return ss;
   CK(cudaEventElapsedTime(&a->fwd_ms, a->ev0, a->ev1));
   a->have_forward = true;
+  a->tail_captured = true;
   if (loss) *loss = a->loss;
   return PDP3G_OK;
 }
@@ -2391,14 +2404,17 @@ pdp3g_status pdp3g_backward_window(pdp3g_adjoint *a) {
   adj_launch_seed(ctx->g, a->A, a->r0, a->r1, a->z0, a->z1, a->d_loss, st);
   for (int w = a->nwin - 1; w >= 0; w--) {
     const int s0 = w * a->interval, s1 = std::min(a->window, s0 + a->interval);
-    rs = adj_restore_checkpoint(a, w);
-    if (rs != PDP3G_OK) return rs;
-    for (size_t j = 0; j < ctx->species.size(); j++)
-      CK(snap_copy(slot_view(a, j, 0), a->ck_parts[w][j], 1, st));
-    for (int s = s0; s < s1; s++) {
-      pdp3g_status fs = adj_forward_step(a, s - s0);
-      if (fs != PDP3G_OK) return fs;
+    if (!(w == a->nwin - 1 && a->tail_captured)) {
+      rs = adj_restore_checkpoint(a, w, false);
+      if (rs != PDP3G_OK) return rs;
+      for (size_t j = 0; j < ctx->species.size(); j++)
+        CK(snap_copy(slot_view(a, j, 0), a->ck_parts[w][j], 1, st));
+      for (int s = s0; s < s1; s++) {
+        pdp3g_status fs = adj_forward_step(a, s - s0);
+        if (fs != PDP3G_OK) return fs;
+      }
     }
+    a->tail_captured = false;  // the slots now hold interval w
     for (int s = s1 - 1; s >= s0; s--) CK(adj_reverse_step(a, s - s0));
   }
   rs = adj_restore_checkpoint(a, a->nwin);

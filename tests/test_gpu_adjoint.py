@@ -11,6 +11,10 @@
   at this size (few particles cross a jump of the gather weights).
 * Forward + backward leaves the state the forward ended in, and the adjoint
   rejects what it does not support.
+* The forward stores its last interval's particle-phase inputs, which the
+  first backward reverses without recomputing; a second backward recomputes
+  every interval and must give the same gradient (1e-9: the recompute's
+  atomic summation order differs from the forward's).
 * The mean-field terms one by one: none is the pathwise derivative, the
   gather terms alone are the default mean field, the wall terms change the
   gradient, unknown bits are rejected.
@@ -131,6 +135,24 @@ def test_backward_restores_forward_end_state_and_rejects_misuse():
     with pytest.raises(api.Pdp3gError):
         api.Adjoint(s64, 10, 5, PROBE)  # the FP64 form has no adjoint
     s64.close()
+
+
+def test_first_backward_reuses_the_last_interval():
+    th = W.adjoint_theta()
+    wl, aux = W.AdjointFamily(th, **SMALL).workload(th)
+    sim = api.from_workload(wl, precision="fp32")
+    # 45 steps at 20 per checkpoint: a last interval of 5 steps
+    adj = api.Adjoint(sim, 45, 20, PROBE)
+    adj.forward()
+    grads = []
+    for _ in range(2):
+        adj.backward()
+        grads.append(np.array(W.adjoint_gradient(
+            wl, aux, [adj.species(0), adj.species(1)], adj.species(2), adj.bunch_velocity(2))))
+    assert np.abs(grads[0]).max() > 0
+    assert np.allclose(grads[0], grads[1], rtol=1e-9, atol=0), (grads[0], grads[1])
+    adj.close()
+    sim.close()
 
 
 def test_jump_terms_select_the_mean_field_parts():
