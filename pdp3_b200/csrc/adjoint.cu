@@ -130,9 +130,43 @@ __device__ __forceinline__ void ladd(const GridDev &g, double *f, int i, int k, 
 // 128-thread CTAs (4 per SM) end the grid-stride loop with a shorter tail
 // than 256-thread ones (2 per SM)
 constexpr int ADJ_THREADS = ADJ_THREADS_PER_CTA;
+static_assert(ADJ_THREADS % 16 == 0, "prefetch sizes are multiples of 16 bytes");
+#ifndef ADJ_PREFETCH_AHEAD
+#define ADJ_PREFETCH_AHEAD 1  // CTA iterations between a chunk's prefetch and its use
+#endif
 // Warp-level segmented sum over runs of consecutive lanes with the same key
 // (particles sorted by cell, with the same half-cell quadrant, share their
 // 24 gather nodes); the last lane of each run holds the run's totals.
+// L2 prefetch of [ptr, ptr + bytes) by the bulk-copy unit (bytes a multiple
+// of 16; skipped unless ptr is 16-byte aligned).  A hint: nothing waits on it.
+__device__ __forceinline__ void prefetch_l2(const void *ptr, unsigned bytes) {
+  if ((reinterpret_cast<unsigned long long>(ptr) & 15ull) != 0) return;
+  asm volatile("cp.async.bulk.prefetch.L2.global [%0], %1;" ::"l"(ptr), "r"(bytes) : "memory");
+}
+
+// One lane asks L2 for the particle chunk that this CTA steps after the
+// current one (the reverse is latency-bound: 16 warps per SM), when that
+// chunk is a full one: every prefetched byte lies inside the arrays.
+__device__ __forceinline__ void prefetch_chunk(const AdjSpeciesDev &S, long long next) {
+  if ((next + 1) * ADJ_THREADS > S.st.n) return;
+  const long long q = next * ADJ_THREADS;
+  constexpr unsigned B4 = 4u * ADJ_THREADS;
+  prefetch_l2(S.st.cell + q, B4);
+  prefetch_l2(S.st.fr + q, B4);
+  prefetch_l2(S.st.fz + q, B4);
+  prefetch_l2(S.st.ur + q, B4);
+  prefetch_l2(S.st.uphi + q, B4);
+  prefetch_l2(S.st.uz + q, B4);
+  prefetch_l2(S.st.w + q, B4);
+  if (S.st.alive) prefetch_l2(S.st.alive + q, ADJ_THREADS);
+  prefetch_l2(S.la + q, B4);
+  prefetch_l2(S.lb + q, B4);
+  prefetch_l2(S.lur + q, B4);
+  prefetch_l2(S.luphi + q, B4);
+  prefetch_l2(S.luz + q, B4);
+  prefetch_l2(S.lw + q, 2 * B4);
+}
+
 template <int N>
 __device__ __forceinline__ bool warp_seg_sum(int key, float (&v)[N]) {
   const unsigned FULL = 0xffffffffu;
@@ -184,6 +218,7 @@ __global__ void __launch_bounds__(ADJ_THREADS, ADJ_MIN_BLOCKS) k_adj_particles(
   C.face_h = face_h;
   const long long nchunks = (S.st.n + ADJ_THREADS - 1) / ADJ_THREADS;
   for (long long chunk = blockIdx.x; chunk < nchunks; chunk += gridDim.x) {
+    if (threadIdx.x == 0) prefetch_chunk(S, chunk + ADJ_PREFETCH_AHEAD * (long long)gridDim.x);
     const long long p = chunk * ADJ_THREADS + threadIdx.x;
     bool live = p < S.st.n && (S.st.alive == nullptr || S.st.alive[p]);
     const int c = live ? S.st.cell[p] : 0;
