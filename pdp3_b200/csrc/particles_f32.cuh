@@ -31,21 +31,47 @@ __device__ __forceinline__ void renorm(int &i, float &f) {
   if (i < 0) { f = f + (float)i; i = 0; }
 }
 
-// adds v into the FP64 grid current comp (0 j_r, 1 j_phi, 2 j_z) at node (i, k)
-__device__ __forceinline__ void dep(const GridDev &g, int comp, int i, int k, float v) {
-  if ((unsigned)i >= (unsigned)g.nr || (unsigned)k >= (unsigned)g.nz) {
-    flag32(g, ERR_OUT_OF_GRID);
+// adds v into the FP64 grid current `base` at node (i, k), flagging nodes
+// outside the grid.  Arguments by value: the out-of-line callers below take
+// no pointer to the kernel's parameters or locals.
+__device__ __forceinline__ void dep_node(unsigned *err, double *base, int nr, int nz, int i, int k,
+                                         float v) {
+  if ((unsigned)i >= (unsigned)nr || (unsigned)k >= (unsigned)nz) {
+    atomicOr(err, ERR_OUT_OF_GRID);
     return;
   }
-  double *base = comp == 0 ? g.jr : (comp == 1 ? g.jphi : g.jz);
-  atomicAdd(base + GIDX(i, k), (double)v);
+  atomicAdd(base + (unsigned)i * (unsigned)nz + (unsigned)k, (double)v);
 }
+
+// the per-node tested deposits of a 2x2 block at the grid edge (dep_block's
+// rare path, kept out of line so that the inlined copies of dep_block stay
+// small); mode as MODE in dep_block
+static __device__ __noinline__ void dep_block_edge(double *jr, double *jphi, double *jz,
+                                                   unsigned *err, int nr, int nz, int mode, int i,
+                                                   int k, float v0, float v1, float v2, float v3) {
+  if (mode == 0) {
+    dep_node(err, jphi, nr, nz, i, k, v0);
+    dep_node(err, jphi, nr, nz, i + 1, k, v1);
+    dep_node(err, jphi, nr, nz, i, k + 1, v2);
+    dep_node(err, jphi, nr, nz, i + 1, k + 1, v3);
+  } else {
+    dep_node(err, jz, nr, nz, i, k, v0);
+    dep_node(err, jz, nr, nz, i + 1, k, v1);
+    dep_node(err, jr, nr, nz, i, k, v2);
+    dep_node(err, jr, nr, nz, i, k + 1, v3);
+  }
+}
+
+// atanh(s)/s - 1 away from 0: rare in a step (|s| >= 0.1 is a radial move of
+// a fifth of the radius), and out of line, so the hot loop keeps no copy of
+// atanhf's code
+static __device__ __noinline__ float atanh_ratio_m1_far(float s) { return atanhf(s) / s - 1.0f; }
 
 // eps(s) = atanh(s)/s - 1
 __device__ __forceinline__ float atanh_ratio_m1(float s) {
   const float s2 = s * s;
   if (s2 < 0.01f) return s2 * (1.0f / 3.0f + s2 * (0.2f + s2 * (1.0f / 7.0f + s2 * (1.0f / 9.0f))));
-  return atanhf(s) / s - 1.0f;
+  return atanh_ratio_m1_far(s);
 }
 
 // One straight piece of the step inside cell (ci, ck), endpoints given as
@@ -59,10 +85,10 @@ __device__ __forceinline__ void piece_values(int ci, float ao, float co, float a
   const float rho_m = fi + fm;
   const float beta = 1.0f - co;  // ((k+1) dz - z_o)/dz
   if (ci >= 1) {
-    const float s = 0.5f * drho / rho_m;
+    const float inv_rm = 1.0f / rho_m;
+    const float s = 0.5f * drho * inv_rm;
     const float eps = atanh_ratio_m1(s);
     const float ii1 = fi * (fi + 1.0f);
-    const float inv_rm = 1.0f / rho_m;
     out[0] = kz * dzeta * ((1.0f - fm) * (2.0f * fi + fm) + ii1 * eps) * inv_rm / fi;
     out[1] = kz * dzeta * (fm * (2.0f * fi + 1.0f + fm) - ii1 * eps) * inv_rm / (fi + 1.0f);
     const float rho_o = fi + ao, rho_n = fi + an;
@@ -72,7 +98,8 @@ __device__ __forceinline__ void piece_values(int ci, float ao, float co, float a
     const float h = 0.5f * ii1;
     const float inv_r0 = kr / (fi + 0.5f);
     out[2] = inv_r0 * (0.5f * drho * beta - 0.25f * dzeta * drho + h * (q1 * beta - q2 - q3));
-    out[3] = inv_r0 * (0.5f * drho * co + 0.25f * dzeta * drho + h * (q1 * co + q2 + q3));
+    // beta + co = 1, so out[2] + out[3] = inv_r0 (drho / 2 + h q1)
+    out[3] = inv_r0 * (0.5f * drho + h * q1) - out[2];
   } else {
     // i = 0: src/particles.cpp:415-473 (no log terms; i(i+1) = 0)
     out[0] = 8.0f * kz * dzeta * (1.0f - fm);
@@ -103,33 +130,21 @@ __device__ __forceinline__ void dep_block(const GridDev &g, int i, int k, const 
     }
     return;
   }
-  if (MODE == 0) {
-    dep(g, 1, i, k, v[0]);
-    dep(g, 1, i + 1, k, v[1]);
-    dep(g, 1, i, k + 1, v[2]);
-    dep(g, 1, i + 1, k + 1, v[3]);
-  } else {
-    dep(g, 2, i, k, v[0]);
-    dep(g, 2, i + 1, k, v[1]);
-    dep(g, 0, i, k, v[2]);
-    dep(g, 0, i, k + 1, v[3]);
-  }
-}
-
-__device__ __forceinline__ void dep_rz(const GridDev &g, int ci, int ck, const float v[4]) {
-  dep_block<1>(g, ci, ck, v);
+  dep_block_edge(g.jr, g.jphi, g.jz, g.err, g.nr, g.nz, MODE, i, k, v[0], v[1], v[2], v[3]);
 }
 
 // The step's straight path from (i, a, k, b) to (in, an, kn, bn) split at the
-// cell faces it crosses (at most one r face and one z face).  The first
-// piece's cell and values are returned (the caller accumulates them); further
-// pieces are deposited directly.  Returns false when the path spans more than
-// one cell in r or z (nothing is deposited, as upstream).
-__device__ __forceinline__ bool deposit_path(const GridDev &g, int i, float a, int k, float b,
-                                             int in, float an, int kn, float bn, float kz,
-                                             float kr, int &c0i, int &c0k, float first[4]) {
+// cell faces it crosses (at most one r face and one z face), each piece
+// deposited into j_z and j_r.  Nothing is deposited when the path spans more
+// than one cell in r or z (as upstream).  Only steps that leave their cell
+// come here (about one in a thousand at thermal speeds): out of line, with
+// its arguments by value and no results, so that the hot loop keeps neither
+// its code nor a local array for it.
+static __device__ __noinline__ void deposit_path(double *jr, double *jz, unsigned *err, int nr,
+                                                 int nz, int i, float a, int k, float b, int in,
+                                                 float an, int kn, float bn, float kz, float kr) {
   const int di = in - i, dk = kn - k;
-  if (di < -1 || di > 1 || dk < -1 || dk > 1) return false;
+  if (di < -1 || di > 1 || dk < -1 || dk > 1) return;
   // end point relative to the start cell
   const float A = (float)di + an, B = (float)dk + bn;
   float tr = 2.0f, tz = 2.0f;
@@ -143,8 +158,6 @@ __device__ __forceinline__ bool deposit_path(const GridDev &g, int i, float a, i
   const int kind0 = r_first ? 0 : 1;
   int ci = i, ck = k;
   float pa = a, pb = b;  // current point relative to (i, k)
-  c0i = i;
-  c0k = k;
 #pragma unroll 1
   for (int p = 0; p <= np; p++) {
     float qa, qb;
@@ -164,20 +177,18 @@ __device__ __forceinline__ bool deposit_path(const GridDev &g, int i, float a, i
       qb = B;
     }
     const float oi = (float)(ci - i), ok = (float)(ck - k);
-    if (p == 0) {
-      piece_values(ci, pa - oi, pb - ok, qa - oi, qb - ok, kz, kr, first);
-    } else {
-      float v[4];
-      piece_values(ci, pa - oi, pb - ok, qa - oi, qb - ok, kz, kr, v);
-      dep_rz(g, ci, ck, v);
-    }
+    float v[4];
+    piece_values(ci, pa - oi, pb - ok, qa - oi, qb - ok, kz, kr, v);
+    dep_node(err, jz, nr, nz, ci, ck, v[0]);
+    dep_node(err, jz, nr, nz, ci + 1, ck, v[1]);
+    dep_node(err, jr, nr, nz, ci, ck, v[2]);
+    dep_node(err, jr, nr, nz, ci, ck + 1, v[3]);
     if (p < np) {
       if (kind == 0) ci += di; else ck += dk;
     }
     pa = qa;
     pb = qb;
   }
-  return true;
 }
 
 // A lane's running sum of the 4 deposits of consecutive particles with the
@@ -530,17 +541,16 @@ __device__ __forceinline__ void f32_warp_chunk(const GridDev &g, const SpeciesF3
       renorm(in, an);
       renorm(kn, bn);
       if (alive_now) {
-        int rz_i, rz_k;
-        float vrz4[4];
         if (in == i && kn == k) {
           // the step stays in its cell (all but about one particle-step in
           // a thousand at thermal speeds): the one piece deposit_path would
-          // make, without its face-crossing logic
+          // make, without its face-crossing logic, into the running sums
+          float vrz4[4];
           piece_values(i, a, b, an, bn, s.kz * w, s.kr * w, vrz4);
           acc_add<1>(g, acc_rz, i * g.nz + k, vrz4);
-        } else if (deposit_path(g, i, a, k, b, in, an, kn, bn, s.kz * w, s.kr * w, rz_i, rz_k,
-                                vrz4)) {
-          acc_add<1>(g, acc_rz, rz_i * g.nz + rz_k, vrz4);
+        } else {
+          deposit_path(g.jr, g.jz, g.err, g.nr, g.nz, i, a, k, b, in, an, kn, bn, s.kz * w,
+                       s.kr * w);
         }
         // back_velocity_to_rz (src/particles.cpp:1005-1015): cos = x/r, sin = y/r
         const float inv_r2 = 1.0f / r2;
