@@ -28,11 +28,22 @@ __device__ __forceinline__ int cell_number(double x, double dx) {  // include/ge
   return (int)ceil(x / dx) - 1;
 }
 
-__device__ __forceinline__ void flag(const GridDev &g, unsigned bit) { atomicOr(g.err, bit); }
+template <typename G>
+__device__ __forceinline__ void flag(const G &g, unsigned bit) { atomicOr(g.err, bit); }
+
+// what the r-z deposition reads of the grid, passed by value to its
+// out-of-line parts (no pointer to the kernel's parameters)
+struct DepGrid64 {
+  double *jr, *jz;
+  unsigned *err;
+  int nr, nz;
+  double dr, dz, dt;
+};
 
 // J accumulation with a bounds check: a node outside the grid is never
 // written; it raises ERR_OUT_OF_GRID instead.
-__device__ __forceinline__ void add(const GridDev &g, double *base, int i, int k, double v) {
+template <typename G>
+__device__ __forceinline__ void add(const G &g, double *base, int i, int k, double v) {
   if ((unsigned)i >= (unsigned)g.nr || (unsigned)k >= (unsigned)g.nz) {
     flag(g, ERR_OUT_OF_GRID);
     return;
@@ -253,7 +264,8 @@ __device__ __forceinline__ void deposit_jphi(const GridDev &g, double q, double 
 #define DENS_STRICT(q, r, dr, dz, dt) ((q) / (PI * 4. * (r) * (dz) * (dz) * (dr) * (dt)))
 
 // Particles::simple_current_distribution, src/particles.cpp:333-474
-__device__ __forceinline__ void simple_current(const GridDev &g, double q, double radius_new,
+template <typename G>
+__device__ __forceinline__ void simple_current(const G &g, double q, double radius_new,
                                             double longitude_new, double radius_old,
                                             double longitude_old, int i_n, int k_n) {
   const double dr = g.dr, dz = g.dz, delta_t = g.dt;
@@ -302,10 +314,11 @@ __device__ __forceinline__ void simple_current(const GridDev &g, double q, doubl
   add(g, g.jr, i_n, k_n + 1, wj);
 }
 
-// Particles::strict_motion_weighting, src/particles.cpp:786-988
-__device__ __forceinline__ void strict_motion(const GridDev &g, double q, double radius_new,
-                                           double longitude_new, double radius_old,
-                                           double longitude_old) {
+// Particles::strict_motion_weighting, src/particles.cpp:786-988 (a step with
+// no radial or no axial motion), out of line
+static __device__ __noinline__ void strict_motion(DepGrid64 g, double q, double radius_new,
+                                                  double longitude_new, double radius_old,
+                                                  double longitude_old) {
   const double dr = g.dr, dz = g.dz, delta_t = g.dt;
   int i_n = cell_number(radius_new, dr), k_n = cell_number(longitude_new, dz);
   int i_o = cell_number(radius_old, dr), k_o = cell_number(longitude_old, dz);
@@ -404,29 +417,16 @@ __device__ __forceinline__ void strict_motion(const GridDev &g, double q, double
   }
 }
 
-// Particles::current_distribution, src/particles.cpp:476-686: the segment
-// (r_o, z_o) -> (r_n, z_n) is split at cell faces into 1, 2 or 3 pieces.
-__device__ __forceinline__ void deposit_rz(const GridDev &g, double q, double r_n, double z_n,
-                                           double r_o, double z_o) {
+// Particles::current_distribution (src/particles.cpp:476-686), the cases of a
+// step that crosses one or two cell faces (2 or 3 pieces).  Out of line, as
+// strict_motion is: few steps cross a face (about one in a thousand at
+// thermal speeds), and the hot loop then keeps none of their code (64-ppc
+// wake case: 9.57 -> 9.36 ms per particle phase, the results unchanged).
+static __device__ __noinline__ void deposit_rz_cross(DepGrid64 g, double q, double r_n,
+                                                     double z_n, double r_o, double z_o, int i_n,
+                                                     int k_n, int i_o, int k_o, int res_cell) {
   const double dr = g.dr, dz = g.dz;
-  int i_n = cell_number(r_n, dr), k_n = cell_number(z_n, dz);
-  int i_o = cell_number(r_o, dr), k_o = cell_number(z_o, dz);
-  if (i_n < 0) i_n = 0;
-  if (k_n < 0) k_n = 0;
-  if (i_o < 0) i_o = 0;
-  if (k_o < 0) k_o = 0;
-  if (r_o == (i_o + 1) * dr) i_o = i_n;
-  if (z_o == (k_o + 1) * dz) k_o = k_n;
-  if (r_n == (i_n + 1) * dr) i_n = i_o;
-  if (z_n == (k_n + 1) * dz) k_n = k_o;
-  const int res_cell = abs(i_n - i_o) + abs(k_n - k_o);
-  if ((fabs(r_n - r_o) < MNZL) || (fabs(z_n - z_o) < MNZL)) {
-    strict_motion(g, q, r_n, z_n, r_o, z_o);
-    return;
-  }
-  if (res_cell == 0) {
-    simple_current(g, q, r_n, z_n, r_o, z_o, i_n, k_n);
-  } else if (res_cell == 1) {
+  if (res_cell == 1) {
     if ((i_n != i_o) && (k_n == k_o)) {
       if (r_o > (i_n + 1) * dr) {
         const double a = (r_o - r_n) / (z_o - z_n);
@@ -534,6 +534,35 @@ __device__ __forceinline__ void deposit_rz(const GridDev &g, double q, double r_
         }
       }
     }
+  }
+}
+
+// Particles::current_distribution, src/particles.cpp:476-686: the segment
+// (r_o, z_o) -> (r_n, z_n) is split at cell faces into 1, 2 or 3 pieces.
+__device__ __forceinline__ void deposit_rz(const GridDev &g, double q, double r_n, double z_n,
+                                           double r_o, double z_o) {
+  const double dr = g.dr, dz = g.dz;
+  int i_n = cell_number(r_n, dr), k_n = cell_number(z_n, dz);
+  int i_o = cell_number(r_o, dr), k_o = cell_number(z_o, dz);
+  if (i_n < 0) i_n = 0;
+  if (k_n < 0) k_n = 0;
+  if (i_o < 0) i_o = 0;
+  if (k_o < 0) k_o = 0;
+  if (r_o == (i_o + 1) * dr) i_o = i_n;
+  if (z_o == (k_o + 1) * dz) k_o = k_n;
+  if (r_n == (i_n + 1) * dr) i_n = i_o;
+  if (z_n == (k_n + 1) * dz) k_n = k_o;
+  const int res_cell = abs(i_n - i_o) + abs(k_n - k_o);
+  if ((fabs(r_n - r_o) < MNZL) || (fabs(z_n - z_o) < MNZL)) {
+    strict_motion(DepGrid64{g.jr, g.jz, g.err, g.nr, g.nz, g.dr, g.dz, g.dt}, q, r_n, z_n, r_o,
+                  z_o);
+    return;
+  }
+  if (res_cell == 0) {
+    simple_current(g, q, r_n, z_n, r_o, z_o, i_n, k_n);
+  } else {
+    deposit_rz_cross(DepGrid64{g.jr, g.jz, g.err, g.nr, g.nz, g.dr, g.dz, g.dt}, q, r_n, z_n, r_o,
+                     z_o, i_n, k_n, i_o, k_o, res_cell);
   }
 }
 
