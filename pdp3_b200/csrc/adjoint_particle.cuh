@@ -18,9 +18,14 @@
 
 #ifdef __CUDACC__
 #define PDP3_HD __host__ __device__ __forceinline__
+// rare branches: out of line on the GPU, so that the particle loop keeps
+// none of their code (arguments and results by value)
+#define PDP3_COLD __host__ __device__ __noinline__
 #else
 #define PDP3_HD inline
+#define PDP3_COLD inline
 #endif
+
 
 namespace pdp3g {
 namespace adj {
@@ -90,6 +95,19 @@ PDP3_HD T sel4(int p, T a0, T a1, T a2, T a3) {
 
 // ---------------------------------------------------------------- pieces
 
+template <typename T>
+struct EpsDeriv {
+  T eps, deps;
+};
+
+// eps and its derivative for s^2 >= 0.01 (a radial move of a fifth of the
+// radius or more in one piece: rare)
+template <typename T>
+PDP3_COLD EpsDeriv<T> eps_far(T s) {
+  const T at = atanh(s);
+  return EpsDeriv<T>{at / s - T(1), (T(1) / (T(1) - s * s) - at / s) / s};
+}
+
 // eps(s) = atanh(s)/s - 1 and its derivative
 template <typename T>
 PDP3_HD void eps_and_deriv(T s, T &eps, T &deps) {
@@ -98,9 +116,9 @@ PDP3_HD void eps_and_deriv(T s, T &eps, T &deps) {
     eps = s2 * (T(1) / 3 + s2 * (T(0.2) + s2 * (T(1) / 7 + s2 * (T(1) / 9))));
     deps = s * (T(2) / 3 + s2 * (T(0.8) + s2 * (T(6) / 7 + s2 * (T(8) / 9))));
   } else {
-    const T at = atanh(s);
-    eps = at / s - T(1);
-    deps = (T(1) / (T(1) - s2) - at / s) / s;
+    const EpsDeriv<T> r = eps_far(s);
+    eps = r.eps;
+    deps = r.deps;
   }
 }
 
@@ -377,6 +395,16 @@ PDP3_HD void forward(const Consts<T> &C, Tape<T> &tp) {
   const int di = in - tp.i, dk = kn - tp.k;
   if (di < -1 || di > 1 || dk < -1 || dk > 1) return;
   tp.path_ok = true;
+  if (di == 0 && dk == 0) {
+    // the step stays in its cell: one piece from (a, b) to (an, bn)
+    tp.qa0 = tp.a;
+    tp.qb0 = tp.b;
+    tp.qa1 = an;
+    tp.qb1 = bn;
+    tp.pci0 = tp.i;
+    tp.pck0 = tp.k;
+    return;
+  }
   const T A = T(di) + an, B = T(dk) + bn;
   T tr = 2, tz = 2;
   if (di != 0) tr = ((di > 0 ? T(1) : T(0)) - tp.a) / (A - tp.a);

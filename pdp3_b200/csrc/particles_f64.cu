@@ -601,7 +601,8 @@ __global__ void __launch_bounds__(256, 4) k_push_deposit_f64(GridDev g, SpeciesD
       for (int c = 0; c < 6; c++) {
         const double *f =
             c == 0 ? g.er
-                   : (c == 1 ? g.ez : (c == 2 ? g.ephi : (c == 3 ? g.hzh : (c == 4 ? g.hrh : g.hphih))));
+                   : (c == 1 ? g.ez
+                             : (c == 2 ? g.ephi : (c == 3 ? g.hzh : (c == 4 ? g.hrh : g.hphih))));
         const bool rh = (c == 0) || (c == 3) || (c == 5);
         const bool zh = (c == 1) || (c == 4) || (c == 5);
         const double val = gather_one(g, f, r, z, rh, zh);
