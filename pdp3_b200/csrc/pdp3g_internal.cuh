@@ -286,4 +286,15 @@ void adj_launch_inject(const AdjSpeciesDev &S, long long start, long long count,
 void adj_launch_seed(const GridDev &g, const AdjGrids &A, int r0, int r1, int z0, int z1,
                      double *loss, cudaStream_t st);
 
+#ifdef __CUDACC__
+// L2 prefetch of [ptr, ptr + bytes) by the bulk-copy unit (bytes a multiple
+// of 16; skipped unless ptr is 16-byte aligned).  A hint: nothing waits on
+// it.  The particle kernels let one thread per CTA ask for the CTA's next
+// chunk while its warps step the current one.
+__device__ __forceinline__ void prefetch_l2(const void *ptr, unsigned bytes) {
+  if ((reinterpret_cast<unsigned long long>(ptr) & 15ull) != 0) return;
+  asm volatile("cp.async.bulk.prefetch.L2.global [%0], %1;" ::"l"(ptr), "r"(bytes) : "memory");
+}
+#endif
+
 }  // namespace pdp3g
