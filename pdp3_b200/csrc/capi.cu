@@ -48,6 +48,7 @@ struct pdp3g_ctx {
   double dr = 0, dz = 0, t = 0;
   double *grid_mem = nullptr;
   float *mirror = nullptr;       // FP32 contexts: E and half-step H in FP32 (6 grids)
+  float4 *quads = nullptr;       // FP32 contexts: the same per cell (GridDev::q32)
   GridDev g{};
   unsigned *d_err = nullptr;
   double *d_inv_pow11 = nullptr;
@@ -316,6 +317,10 @@ pdp3g_status pdp3g_create(const pdp3g_config *cfg, pdp3g_ctx **out) {
       return bail(PDP3G_CUDA_ERROR);
     g.e32 = ctx->mirror;
     g.hh32 = ctx->mirror + 3 * ng;
+    const size_t ncells = (size_t)(cfg->n_grid_r - 1) * (cfg->n_grid_z - 1);
+    if ((e = dalloc(ctx, &ctx->quads, 6 * ncells)) != cudaSuccess)
+      return bail(e == cudaErrorMemoryAllocation ? PDP3G_NO_MEMORY : PDP3G_CUDA_ERROR);
+    g.q32 = ctx->quads;
   }
   if ((e = cudaDeviceSynchronize()) != cudaSuccess) return bail(PDP3G_CUDA_ERROR);
   *out = ctx;
@@ -347,6 +352,7 @@ void pdp3g_destroy(pdp3g_ctx *ctx) {
     for (auto &e : se.ev) cudaEventDestroy(e);
   cudaFree(ctx->grid_mem);
   cudaFree(ctx->mirror);
+  cudaFree(ctx->quads);
   cudaFree(ctx->d_err);
   cudaFree(ctx->d_inv_pow11);
   cudaFree(ctx->d_rho0);
@@ -796,9 +802,19 @@ static cudaStream_t species_stream(const pdp3g_ctx *ctx, size_t j) {
 // partial round of CTAs of one species' kernel overlaps the next kernel.
 // The fork and join are checked: if the join's wait failed, the phases
 // after this one would no longer be ordered after the side stream's J sums.
+// the per-cell FP32 quads of E and the half-step H from their node copies,
+// before every FP32 particle phase (the Yee updates, set_field and the
+// checkpoint restores write the node copies)
+static void pack_quads(pdp3g_ctx *ctx) {
+  if (!ctx->quads) return;
+  launch_pack_quads(ctx->g, ctx->quads, ctx->stream);
+  ctx->launches++;
+}
+
 static cudaError_t phase_particles(pdp3g_ctx *ctx) {
   const bool fork = ctx->species.size() >= 2;
   cudaError_t e;
+  pack_quads(ctx);
   if (fork) {
     if ((e = cudaEventRecord(ctx->ev_fork, ctx->stream)) != cudaSuccess) return e;
     if ((e = cudaStreamWaitEvent(ctx->stream_side, ctx->ev_fork, 0)) != cudaSuccess) return e;
@@ -2210,6 +2226,7 @@ pdp3g_status adj_forward_step(pdp3g_adjoint *a, int cap) {
   CK(cudaMemcpyAsync(a->cap_fields + (size_t)cap * 6 * ng, ctx->mirror, sizeof(float) * 6 * ng,
                      cudaMemcpyDeviceToDevice, ctx->stream));
   CK(phase_reset_j(ctx));
+  pack_quads(ctx);
   CK(species_fork(ctx));
   for (size_t j = 0; j < ctx->species.size(); j++) {
     const SpeciesF32 in = slot_view(a, j, cap), nx = slot_view(a, j, cap + 1);

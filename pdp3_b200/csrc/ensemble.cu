@@ -133,7 +133,7 @@ __global__ void __launch_bounds__(F32_THREADS, F32_MIN_BLOCKS) k_ensemble(Ensemb
       }
       __syncthreads();
       for (int c = first; c < ce; c += G)
-        f32_chunk<false, PUSHER>(desc.g, desc.s, SpeciesOut{}, desc.pusher, c - cb, sm);
+        f32_chunk<false, PUSHER, false>(desc.g, desc.s, SpeciesOut{}, desc.pusher, c - cb, sm);
     }
     grid.sync();
     // ---- phase C: E update, t += dt

@@ -40,6 +40,21 @@ __global__ void k_to_f32(const double *src, float *dst, size_t n) {
     dst[t] = (float)src[t];
 }
 
+// thread t = c * ncells + cell: the 2x2 nodes of the cell of component c
+// (0-2 E_r, E_phi, E_z from e32; 3-5 the half-step H_r, H_phi, H_z from hh32)
+__global__ void k_pack_quads(GridDev g, float4 *q) {
+  const int nz = g.nz, ncz = nz - 1;
+  const long long ng = (long long)g.nr * nz, ncells = (long long)(g.nr - 1) * ncz;
+  for (long long t = blockIdx.x * (long long)blockDim.x + threadIdx.x; t < 6 * ncells;
+       t += (long long)gridDim.x * blockDim.x) {
+    const int c = (int)(t / ncells);
+    const long long cell = t - c * ncells;
+    const int i = (int)(cell / ncz), k = (int)(cell - (long long)i * ncz);
+    const float *f = (c < 3 ? g.e32 : g.hh32) + (c % 3) * ng + (long long)i * nz + k;
+    q[t] = make_float4(__ldg(f), __ldg(f + nz), __ldg(f + 1), __ldg(f + nz + 1));
+  }
+}
+
 static int grid_blocks(long long total) {
   long long b = (total + 255) / 256;
   if (b > 148 * 16) b = 148 * 16;
@@ -58,6 +73,10 @@ void launch_yee_e(const GridDev &g, cudaStream_t st) {
 }  // namespace pdp3g
 
 namespace pdp3g {
+void launch_pack_quads(const GridDev &g, float4 *q, cudaStream_t st) {
+  k_pack_quads<<<grid_blocks(6LL * (g.nr - 1) * (g.nz - 1)), 256, 0, st>>>(g, q);
+}
+
 void launch_to_f32(const double *src, float *dst, size_t n, cudaStream_t st) {
   long long b = ((long long)n + 255) / 256;
   if (b > 148 * 16) b = 148 * 16;

@@ -294,6 +294,13 @@ __device__ __forceinline__ float gather4(const GridDev &g, const float *__restri
   return wz0 * (f00 * wr0 + f10 * wr1) + wz1 * (f01 * wr0 + f11 * wr1);
 }
 
+// The same from the cell's packed quad (GridDev::q32): one 16-byte load.
+__device__ __forceinline__ float gather_quad(const float4 *__restrict__ q, float wr0, float wr1,
+                                             float wz0, float wz1) {
+  const float4 v = __ldg(q);
+  return wz0 * (v.x * wr0 + v.y * wr1) + wz1 * (v.z * wr0 + v.w * wr1);
+}
+
 
 // Per-warp staging of a warp chunk in shared memory: element e of the chunk
 // (particle base + e, lane e / F32_PER_LANE's j-th particle with
@@ -364,7 +371,9 @@ __device__ __forceinline__ void stage_out(T *dst, const T *src, long long base, 
 // stays the same, and the warp adds the lanes' sums up with one segmented
 // reduction per chunk before the FP64 atomics.
 // OUT = false: the step in place (o unused); OUT = true: results go to o.
-template <bool OUT, int PUSHER>
+// QUAD: gather from the packed quads (GridDev::q32) instead of the node
+// copies (the persistent ensemble kernel, which does not pack them).
+template <bool OUT, int PUSHER, bool QUAD>
 __device__ __forceinline__ void f32_warp_chunk(const GridDev &g, const SpeciesF32 &s,
                                                const SpeciesOut &o, int pusher_rt,
                                                long long wchunk, WarpStage &ws) {
@@ -431,13 +440,28 @@ __device__ __forceinline__ void f32_warp_chunk(const GridDev &g, const SpeciesF3
       const float wzn0 = 1.0f - b, wzn1 = b;
       const int ir_n = i, kz_n = k;
       float e[3], h[3];
-      const size_t ng = (size_t)g.nr * g.nz;
-      e[0] = gather4(g, g.e32, ir_h, kz_n, wrh0, wrh1, wzn0, wzn1);
-      e[1] = gather4(g, g.e32 + ng, ir_n, kz_n, wrn0, wrn1, wzn0, wzn1);
-      e[2] = gather4(g, g.e32 + 2 * ng, ir_n, kz_h, wrn0, wrn1, wzh0, wzh1);
-      h[0] = gather4(g, g.hh32, ir_n, kz_h, wrn0, wrn1, wzh0, wzh1);
-      h[1] = gather4(g, g.hh32 + ng, ir_h, kz_h, wrh0, wrh1, wzh0, wzh1);
-      h[2] = gather4(g, g.hh32 + 2 * ng, ir_h, kz_n, wrh0, wrh1, wzn0, wzn1);
+      if (QUAD) {
+        // quads of the cells (ir, kz): the particle's own cell c for the
+        // node weights, one row (ncz) and/or one column lower for the half
+        // weights when the particle sits in the lower half
+        const size_t ncells = (size_t)(g.nr - 1) * (size_t)ncz;
+        const unsigned q_nn = (unsigned)c, q_hn = q_nn - (unsigned)(i - ir_h) * (unsigned)ncz;
+        const unsigned q_nh = q_nn - (unsigned)(k - kz_h), q_hh = q_hn - (unsigned)(k - kz_h);
+        e[0] = gather_quad(g.q32 + q_hn, wrh0, wrh1, wzn0, wzn1);
+        e[1] = gather_quad(g.q32 + ncells + q_nn, wrn0, wrn1, wzn0, wzn1);
+        e[2] = gather_quad(g.q32 + 2 * ncells + q_nh, wrn0, wrn1, wzh0, wzh1);
+        h[0] = gather_quad(g.q32 + 3 * ncells + q_nh, wrn0, wrn1, wzh0, wzh1);
+        h[1] = gather_quad(g.q32 + 4 * ncells + q_hh, wrh0, wrh1, wzh0, wzh1);
+        h[2] = gather_quad(g.q32 + 5 * ncells + q_hn, wrh0, wrh1, wzn0, wzn1);
+      } else {
+        const size_t ng = (size_t)g.nr * g.nz;
+        e[0] = gather4(g, g.e32, ir_h, kz_n, wrh0, wrh1, wzn0, wzn1);
+        e[1] = gather4(g, g.e32 + ng, ir_n, kz_n, wrn0, wrn1, wzn0, wzn1);
+        e[2] = gather4(g, g.e32 + 2 * ng, ir_n, kz_h, wrn0, wrn1, wzh0, wzh1);
+        h[0] = gather4(g, g.hh32, ir_n, kz_h, wrn0, wrn1, wzh0, wzh1);
+        h[1] = gather4(g, g.hh32 + ng, ir_h, kz_h, wrh0, wrh1, wzh0, wzh1);
+        h[2] = gather4(g, g.hh32 + 2 * ng, ir_h, kz_n, wrh0, wrh1, wzn0, wzn1);
+      }
       // ---- push
       float inv_g = 1.0f;
       if (pusher == 1) {
@@ -600,12 +624,12 @@ __device__ __forceinline__ void f32_warp_chunk(const GridDev &g, const SpeciesF3
 
 // One CTA chunk of F32_CHUNK consecutive particles: warp w takes the w-th
 // warp chunk.  No CTA-wide synchronisation: warps are independent.
-template <bool OUT, int PUSHER = -1>
+template <bool OUT, int PUSHER = -1, bool QUAD = true>
 __device__ __forceinline__ void f32_chunk(const GridDev &g, const SpeciesF32 &s,
                                           const SpeciesOut &o, int pusher, long long chunk,
                                           F32Shared &sm) {
   const int warp = threadIdx.x >> 5;
-  f32_warp_chunk<OUT, PUSHER>(g, s, o, pusher, chunk * F32_WARPS + warp, sm.stage[warp]);
+  f32_warp_chunk<OUT, PUSHER, QUAD>(g, s, o, pusher, chunk * F32_WARPS + warp, sm.stage[warp]);
 }
 
 }  // namespace pdp3g

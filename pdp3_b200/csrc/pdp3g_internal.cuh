@@ -38,8 +38,14 @@ struct GridDev {
   unsigned *err;
   // FP32 contexts only (else null): FP32 copies of E (3 grids) and of the
   // half-step H (3 grids, right after them), written by the Yee updates
-  // beside the FP64 values, gathered by the FP32 particle phase
+  // beside the FP64 values
   float *e32, *hh32;
+  // FP32 contexts only: the same 6 components per cell, q32[c * ncells +
+  // i * (nz - 1) + k] = (f[i][k], f[i+1][k], f[i][k+1], f[i+1][k+1]) for the
+  // cell (i, k), packed from e32/hh32 before each particle phase
+  // (launch_pack_quads), so that the FP32 particle kernel gathers a
+  // component with one 16-byte load
+  const float4 *q32;
 };
 
 // FP64 structure-of-arrays species (the plain form).
@@ -189,6 +195,8 @@ int sort_keys(const unsigned *keys, long long n, int key_bits, char *scratch,
 
 // host-side launchers (fields.cu, particles_f64.cu, particles_f32.cu, diag.cu)
 void launch_to_f32(const double *src, float *dst, size_t n, cudaStream_t st);
+// packs GridDev::q32 (at q, 6 * (nr-1) * (nz-1) entries) from e32/hh32
+void launch_pack_quads(const GridDev &g, float4 *q, cudaStream_t st);
 void launch_yee_h(const GridDev &g, cudaStream_t st);
 void launch_yee_e(const GridDev &g, cudaStream_t st);
 void launch_push_deposit_f64(const GridDev &g, const SpeciesDev &s, int pusher, int n_sm,
