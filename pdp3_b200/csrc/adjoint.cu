@@ -103,10 +103,6 @@ __global__ void k_adj_h(GridDev g, AdjGrids A) {
   }
 }
 
-__device__ __forceinline__ float node_val(const GridDev &g, const float *f, int i, int k) {
-  return __ldg(f + (size_t)i * g.nz + k);
-}
-
 // adjoint of J at (i, k), 0 outside the grid
 __device__ __forceinline__ float lget(const GridDev &g, const float *f, int i, int k) {
   if ((unsigned)i >= (unsigned)g.nr || (unsigned)k >= (unsigned)g.nz) return 0.0f;
@@ -184,18 +180,18 @@ __device__ __forceinline__ bool warp_seg_sum(int key, float (&v)[N]) {
   return tail && key >= 0;
 }
 
-// step 2: particles.  E3 = E of step s, Hh3 = H half-time of step s (three
-// consecutive grids each).  Each thread takes one particle; the 24
+// step 2: particles.  Q = E and the half-step H of step s as per-cell quads
+// (the 2x2 nodes of a cell, GridDev::q32's layout, as the forward step
+// gathered them).  Each thread takes one particle; the 24
 // field-node adjoints of a warp's particles are summed over runs of lanes
 // that share their gather nodes (particles sorted by cell) and each run adds
 // its totals to the FP64 grids.  Warps are independent.  WALLS: whether the
 // wall-reflection jump terms (face bit 1) are compiled in.
 template <bool WALLS>
 __global__ void __launch_bounds__(ADJ_THREADS, ADJ_MIN_BLOCKS) k_adj_particles(
-    GridDev g, const float *E3, const float *Hh3, AdjSpeciesDev S, AdjGrids A, int face,
-    float face_h) {
+    GridDev g, const float4 *Q, AdjSpeciesDev S, AdjGrids A, int face, float face_h) {
   const int ncz = g.nz - 1;
-  const size_t ng = (size_t)g.nr * g.nz;
+  const size_t ncells = (size_t)(g.nr - 1) * ncz;
   adj::Consts<float> C;
   C.ke = S.st.ke;
   C.kb = S.st.kb;
@@ -241,20 +237,20 @@ __global__ void __launch_bounds__(ADJ_THREADS, ADJ_MIN_BLOCKS) k_adj_particles(
         {
           const int ir = adj::comp_rhalf(0, cc) ? ir_h : ir_n;
           const int kz = adj::comp_zhalf(0, cc) ? kz_h : kz_n;
-          const float *f = E3 + cc * ng;
-          tp.fe[cc][0] = node_val(g, f, ir, kz);
-          tp.fe[cc][1] = node_val(g, f, ir + 1, kz);
-          tp.fe[cc][2] = node_val(g, f, ir, kz + 1);
-          tp.fe[cc][3] = node_val(g, f, ir + 1, kz + 1);
+          const float4 v = __ldg(Q + cc * ncells + (size_t)ir * ncz + kz);
+          tp.fe[cc][0] = v.x;
+          tp.fe[cc][1] = v.y;
+          tp.fe[cc][2] = v.z;
+          tp.fe[cc][3] = v.w;
         }
         {
           const int ir = adj::comp_rhalf(1, cc) ? ir_h : ir_n;
           const int kz = adj::comp_zhalf(1, cc) ? kz_h : kz_n;
-          const float *f = Hh3 + cc * ng;
-          tp.fh[cc][0] = node_val(g, f, ir, kz);
-          tp.fh[cc][1] = node_val(g, f, ir + 1, kz);
-          tp.fh[cc][2] = node_val(g, f, ir, kz + 1);
-          tp.fh[cc][3] = node_val(g, f, ir + 1, kz + 1);
+          const float4 v = __ldg(Q + (3 + cc) * ncells + (size_t)ir * ncz + kz);
+          tp.fh[cc][0] = v.x;
+          tp.fh[cc][1] = v.y;
+          tp.fh[cc][2] = v.z;
+          tp.fh[cc][3] = v.w;
         }
       }
       adj::forward(C, tp);
@@ -384,9 +380,8 @@ void adj_launch_h(const GridDev &g, const AdjGrids &A, cudaStream_t st) {
   k_adj_h<<<blocks_for((long long)g.nr * g.nz, 256), 256, 0, st>>>(g, A);
 }
 
-void adj_launch_particles(const GridDev &g, const float *E3, const float *Hh3,
-                          const AdjSpeciesDev &S, const AdjGrids &A, int face, float face_h,
-                          cudaStream_t st) {
+void adj_launch_particles(const GridDev &g, const float4 *Q, const AdjSpeciesDev &S,
+                          const AdjGrids &A, int face, float face_h, cudaStream_t st) {
   if (S.st.n <= 0) return;
   const long long nchunks = (S.st.n + ADJ_THREADS - 1) / ADJ_THREADS;
   auto kernel = (face & 2) ? k_adj_particles<true> : k_adj_particles<false>;
@@ -398,7 +393,7 @@ void adj_launch_particles(const GridDev &g, const float *E3, const float *Hh3,
   cudaGetDevice(&dev);
   cudaDeviceGetAttribute(&nsm, cudaDevAttrMultiProcessorCount, dev);
   const long long blocks = std::min<long long>(nchunks, (long long)bpsm * nsm);
-  kernel<<<(int)std::max<long long>(blocks, 1), ADJ_THREADS, 0, st>>>(g, E3, Hh3, S, A, face,
+  kernel<<<(int)std::max<long long>(blocks, 1), ADJ_THREADS, 0, st>>>(g, Q, S, A, face,
                                                                          face_h);
 }
 

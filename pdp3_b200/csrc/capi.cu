@@ -2104,7 +2104,8 @@ struct pdp3g_adjoint {
   std::vector<std::vector<AdjSnap>> ck_parts;  // [nwin + 1][species]
   std::vector<double> ck_t;
   std::vector<int64_t> ck_steps;
-  float *cap_fields = nullptr;                 // interval x 6 grids (E, H half), FP32
+  float4 *cap_quads = nullptr;                 // interval x 6 x cells: E and the half-step
+                                               // H per cell (GridDev::q32), FP32
   std::vector<std::vector<AdjSnap>> cap_parts; // [interval + 1][species]: states of the
                                                // recomputed interval, slot j = step j's input
   std::vector<double> cap_t;
@@ -2208,7 +2209,7 @@ SpeciesF32 slot_view(const pdp3g_adjoint *a, size_t j, int slot) {
 // slot cap keeps the particle phase's input for the reverse, with no copy.
 pdp3g_status adj_forward_step(pdp3g_adjoint *a, int cap) {
   pdp3g_ctx *ctx = a->ctx;
-  const size_t ng = (size_t)ctx->cfg.n_grid_r * ctx->cfg.n_grid_z;
+  const size_t ncells = (size_t)(ctx->cfg.n_grid_r - 1) * (ctx->cfg.n_grid_z - 1);
   if (cap < 0) {
     phase_inject(ctx);
     phase_calc_h(ctx);
@@ -2222,11 +2223,12 @@ pdp3g_status adj_forward_step(pdp3g_adjoint *a, int cap) {
   for (size_t j = 0; j < ctx->species.size(); j++)
     if (ctx->species[j].is_bunch) inject_f32(ctx, ctx->species[j], slot_view(a, j, cap));
   phase_calc_h(ctx);
-  // the FP32 copies of E and the half-step H are current after the H update
-  CK(cudaMemcpyAsync(a->cap_fields + (size_t)cap * 6 * ng, ctx->mirror, sizeof(float) * 6 * ng,
-                     cudaMemcpyDeviceToDevice, ctx->stream));
   CK(phase_reset_j(ctx));
+  // the per-cell FP32 quads of E and the half-step H that this step's
+  // particles gather, kept for the reverse
   pack_quads(ctx);
+  CK(cudaMemcpyAsync(a->cap_quads + (size_t)cap * 6 * ncells, ctx->quads,
+                     sizeof(float4) * 6 * ncells, cudaMemcpyDeviceToDevice, ctx->stream));
   CK(species_fork(ctx));
   for (size_t j = 0; j < ctx->species.size(); j++) {
     const SpeciesF32 in = slot_view(a, j, cap), nx = slot_view(a, j, cap + 1);
@@ -2245,9 +2247,9 @@ pdp3g_status adj_forward_step(pdp3g_adjoint *a, int cap) {
 // two streams as in the forward step
 cudaError_t adj_reverse_step(pdp3g_adjoint *a, int cap) {
   pdp3g_ctx *ctx = a->ctx;
-  const size_t ng = (size_t)ctx->cfg.n_grid_r * ctx->cfg.n_grid_z;
+  const size_t ncells = (size_t)(ctx->cfg.n_grid_r - 1) * (ctx->cfg.n_grid_z - 1);
   adj_launch_e(ctx->g, a->A, ctx->stream);
-  const float *E3 = a->cap_fields + (size_t)cap * 6 * ng;
+  const float4 *Q = a->cap_quads + (size_t)cap * 6 * ncells;
   cudaError_t e = species_fork(ctx);
   if (e != cudaSuccess) return e;
   for (size_t j = 0; j < ctx->species.size(); j++) {
@@ -2255,7 +2257,7 @@ cudaError_t adj_reverse_step(pdp3g_adjoint *a, int cap) {
     const cudaStream_t st = species_stream(ctx, j);
     AdjSpeciesDev S = a->ls[j];
     S.st = slot_view(a, j, cap);
-    adj_launch_particles(ctx->g, E3, E3 + 3 * ng, S, a->A, a->face_terms, a->face_h, st);
+    adj_launch_particles(ctx->g, Q, S, a->A, a->face_terms, a->face_h, st);
     if (sp.is_bunch) {
       long long start, count;
       inject_range(ctx, sp, a->cap_t[cap], start, count);
@@ -2344,7 +2346,8 @@ pdp3g_status pdp3g_adjoint_create(pdp3g_ctx *ctx, int32_t window_steps,
   a->ck_steps.assign(a->nwin + 1, 0);
   for (int c = 0; c <= a->nwin; c++)
     for (size_t j = 0; j < nsp; j++) ACK(snap_alloc(a, ctx->species[j].f32, a->ck_parts[c][j]));
-  ACK(aalloc(a, &a->cap_fields, (size_t)a->interval * 6 * ng));
+  const size_t ncells = (size_t)(nr - 1) * (nz - 1);
+  ACK(aalloc(a, &a->cap_quads, (size_t)a->interval * 6 * ncells));
   a->cap_parts.assign(a->interval + 1, std::vector<AdjSnap>(nsp));
   a->cap_t.assign(a->interval, 0.0);
   for (int c = 0; c <= a->interval; c++)

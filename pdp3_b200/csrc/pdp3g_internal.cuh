@@ -285,9 +285,9 @@ void launch_mp_write(const MpArrays &arr, long long n, double dr, double dz, int
 
 void adj_launch_e(const GridDev &g, const AdjGrids &A, cudaStream_t st);
 void adj_launch_h(const GridDev &g, const AdjGrids &A, cudaStream_t st);
-void adj_launch_particles(const GridDev &g, const float *E3, const float *Hh3,
-                          const AdjSpeciesDev &S, const AdjGrids &A, int face, float face_h,
-                          cudaStream_t st);
+// Q: the step's per-cell quads of E and the half-step H (GridDev::q32 layout)
+void adj_launch_particles(const GridDev &g, const float4 *Q, const AdjSpeciesDev &S,
+                          const AdjGrids &A, int face, float face_h, cudaStream_t st);
 void adj_launch_inject(const AdjSpeciesDev &S, long long start, long long count, double dt,
                        double dz, double velocity, const double *inv_pow11, double *lv,
                        cudaStream_t st);
