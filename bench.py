@@ -859,21 +859,27 @@ def run_adjoint(args, rank, world, local_rank, dist=None):
 
 def load_traffic(workload, precision, wl):
     """DRAM bytes (read + write) of one pass of the particle phase, from the
-    committed ncu summary of the same kernel on the 8-ppc case of this
-    workload, scaled by particle count (the traffic is per particle: the
-    kernel streams each particle once).  None when no summary exists."""
+    committed ncu summary of the same kernel on the small cases of this
+    workload: a per-particle part scaled by the plasma particle count (the
+    kernel streams each particle once) plus, where the summary gives one, a
+    fixed part per species launch (the field data the launch reads, the same
+    at every particle count).  None when no summary exists."""
     path = os.path.join(ROOT, "profiles", "push_deposit_%s_%s_ppc8.md" % (precision, workload))
+    per = fixed = None
     try:
         with open(path) as f:
             for line in f:
                 if line.startswith("dram_bytes_per_particle:"):
                     per = float(line.split(":")[1])
-                    n_plasma = wl.n_particles - (wl.beam.number_macro * wl.beam.number_bunches
-                                                 if wl.beam is not None else 0)
-                    return per * n_plasma
+                elif line.startswith("dram_bytes_per_launch_fixed:"):
+                    fixed = float(line.split(":")[1])
     except OSError:
-        pass
-    return None
+        return None
+    if per is None:
+        return None
+    n_plasma = wl.n_particles - (wl.beam.number_macro * wl.beam.number_bunches
+                                 if wl.beam is not None else 0)
+    return per * n_plasma + (fixed or 0.0) * len(wl.species)
 
 
 def run_e2e(sim, wl, torch, stream, steps):
