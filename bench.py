@@ -2,7 +2,7 @@
 
     python bench.py [--gpus N] [--steps K] [--warmup W] [--impl ours|reference]
                     [--precision fp64|fp32]
-                    [--workload wake|thermal|large|ensemble|adjoint]
+                    [--workload wake|thermal|large|ensemble|adjoint|diag]
 
 Workload (default): the beam-plasma wake case, 256 x 2048 cells over
 r in [0, 0.1] m, z in [0, 0.8] m, electrons and protons at 64 macroparticles
@@ -23,6 +23,11 @@ are far larger than L2, so no L2 flush is needed between steps.
 
 --impl reference times the upstream OpenMP CPU step (oracle/_ref, the
 unmodified upstream sources) on a bounded sample of the same workload.
+
+--workload diag times the upstream's diagnostics and initial-field solve
+through their C-ABI calls (charge density, temperature, density, a full
+probe frame on the wake case; the Dirichlet Poisson solve on a 257 x 2047
+grid) beside the upstream CPU code, one JSON line with one entry per call.
 """
 import argparse
 import json
@@ -273,7 +278,7 @@ def main():
     ap.add_argument("--precision", default="fp32", choices=["fp64", "fp32"],
                     help="the form reported as value (the other is measured beside it)")
     ap.add_argument("--workload", default="wake",
-                    choices=["wake", "thermal", "large", "ensemble", "adjoint"])
+                    choices=["wake", "thermal", "large", "ensemble", "adjoint", "diag"])
     ap.add_argument("--adjoint-scale", type=int, default=1,
                     help="--workload adjoint: divide the grid's cells in r and z by this "
                          "(1: the 128x1024 case)")
@@ -305,6 +310,8 @@ def main():
 
     if args.impl == "reference":
         return run_reference(args, rank, world)
+    if args.workload == "diag":
+        return run_diag(args, rank, world)
     if args.workload in ("ensemble", "adjoint"):
         import torch
         dist = None
@@ -854,6 +861,169 @@ def run_adjoint(args, rank, world, local_rank, dist=None):
                         "fd": "FP64 form, cubic fit over 8 relative steps in [-2%, 2%]",
                         "params": {str(j): v for j, v in fd.items()}, "summary": summary},
             "clocks": clk}), flush=True)
+    return 0
+
+
+# ------------------------------------------------------ diagnostics (rows f1, f2, f4)
+
+DIAG_POISSON_GRID = (257, 2047)  # the wake grid's size where 2 n_grid_z + 2 is a power of two
+
+
+def diag_cpu_times(wl, fractions, threads):
+    """The upstream CPU charge weighting, TemperatureClassic and
+    ParticlesDensity (oracle/_ref) on the wake grid with seeded subsets of
+    the plasma: milliseconds per call at each sample size, and a straight
+    line through them in the particle count extrapolated to the full count
+    (all plasma species for the charge density, the electrons for the
+    per-species diagnostics)."""
+    from oracle import refsim
+    if not refsim.available("boris"):
+        return None
+    rng = np.random.default_rng(4321)
+    rows = []
+    for frac in fractions:
+        sim = refsim.RefSim(wl.r_size, wl.z_size, wl.n_grid_r, wl.n_grid_z, wl.dt, end_time=1.0,
+                            pml=wl.pml, pusher="boris")
+        sim.L.ref_set_threads(threads)
+        counts = []
+        for s in wl.species:
+            k = max(1, int(s.n * frac))
+            idx = np.sort(rng.choice(s.n, size=k, replace=False))
+            sim.add_species(s.name, s.charge_e, s.mass_me, s.r[idx], s.z[idx], s.vr[idx],
+                            s.vphi[idx], s.vz[idx], s.w[idx])
+            counts.append(k)
+        t = {}
+        for name, fn in (("charge_density", lambda: sim.charge_density()),
+                         ("temperature_electrons", lambda: sim.temperature(0)),
+                         ("density_electrons", lambda: sim.density(0))):
+            fn()
+            reps = []
+            for _ in range(3):
+                t0 = time.perf_counter()
+                fn()
+                reps.append(time.perf_counter() - t0)
+            t[name] = 1e3 * statistics.median(reps)
+        rows.append(({"charge_density": sum(counts), "temperature_electrons": counts[0],
+                      "density_electrons": counts[0]}, t))
+        sim.close()
+    full = {"charge_density": sum(s.n for s in wl.species),
+            "temperature_electrons": wl.species[0].n, "density_electrons": wl.species[0].n}
+    out = {}
+    (c0, t0), (c1, t1) = rows[0], rows[-1]
+    for name in t0:
+        slope = (t1[name] - t0[name]) / max(c1[name] - c0[name], 1)
+        out[name] = {"ms_extrapolated": max(t1[name], t1[name] + slope * (full[name] - c1[name])),
+                     "samples": [{"particles": c[name], "ms": tt[name]} for c, tt in rows]}
+    return out
+
+
+def diag_cpu_poisson(threads):
+    from oracle import refsim
+    if not refsim.available("boris"):
+        return None
+    nr, nz = DIAG_POISSON_GRID
+    sim = refsim.RefSim(0.1, 0.8, nr, nz, 4.6e-13, end_time=1.0, pml=None, pusher="boris")
+    sim.L.ref_set_threads(threads)
+    rho = np.random.default_rng(5).normal(0.0, 1e-3, (nr, nz))
+    sim.poisson_dirichlet(rho)
+    reps = []
+    for _ in range(3):
+        t0 = time.perf_counter()
+        sim.poisson_dirichlet(rho)
+        reps.append(time.perf_counter() - t0)
+    sim.close()
+    return 1e3 * statistics.median(reps)
+
+
+def run_diag(args, rank, world):
+    """The upstream's diagnostics and initial-field solve on one GPU: charge
+    density (Particles::charge_weighting), TemperatureClassic and
+    ParticlesDensity of the electrons, a full-frame E_z probe read
+    (ProbePlain frame) on the wake case, and PoissonDirichlet on a 257 x 2047
+    grid, each through its C-ABI call with the result copied to host memory;
+    device time with CUDA events on the context's stream, the upstream CPU
+    code timed beside it."""
+    if rank != 0:
+        return 0
+    import torch
+    from pdp3_b200 import api
+    peaks, peak_src = load_peaks()
+    hbm = peaks["hbm_gbs"]
+    wl = make_workload("wake", 1002, args.ppc)
+    sim = api.from_workload(wl, precision=args.precision)
+    sim.step(args.warmup)
+    sim.sync()
+    stream = torch.cuda.ExternalStream(sim.stream_ptr)
+    n_all = sum(sim.species_size(s) for s in range(len(wl.species)))
+    n_el = sim.species_size(0)
+    ng = wl.n_grid_r * wl.n_grid_z
+    part_b = 16 if args.precision == "fp32" else 24  # position (+ cell) and weight
+    vel_b = 12 if args.precision == "fp32" else 24
+
+    def timed(fn, reps=5):
+        fn()
+        ms = []
+        for _ in range(reps):
+            e0, e1 = torch.cuda.Event(enable_timing=True), torch.cuda.Event(enable_timing=True)
+            e0.record(stream)
+            fn()
+            e1.record(stream)
+            e1.synchronize()
+            ms.append(e0.elapsed_time(e1))
+        return statistics.median(ms)
+
+    items = {}
+
+    def add(name, ms, nbytes, what):
+        achieved = nbytes / (ms * 1e-3) / 1e9
+        items[name] = {"ms": ms, "algorithmic_bytes": nbytes, "what": what,
+                       "achieved_gbs": achieved, "frac": achieved / hbm}
+
+    add("charge_density", timed(lambda: sim.charge_density()),
+        n_all * part_b + ng * 8 * 2,
+        "every plasma particle's position and weight read, the rho grid written and copied out")
+    add("temperature_electrons", timed(lambda: sim.temperature(0)),
+        n_el * (part_b + vel_b) + ng * 8 * 2,
+        "the electrons' positions, velocities and weights read, the T grid written and copied out")
+    add("density_electrons", timed(lambda: sim.density(0)),
+        n_el * part_b + ng * 8 * 2,
+        "the electrons' positions and weights read, the density grid written and copied out")
+    add("probe_frame_E_z", timed(lambda: sim.probe("E_z", "frame", 0, 0, wl.n_grid_r,
+                                                     wl.n_grid_z)),
+        ng * 8 * 2, "the E_z grid read and its frame copied out")
+    sim.close()
+    nr, nz = DIAG_POISSON_GRID
+    ps = api.Simulation(0.1, 0.8, nr, nz, 4.6e-13, precision=args.precision)
+    rho = np.random.default_rng(5).normal(0.0, 1e-3, (nr, nz))
+    ps_stream = torch.cuda.ExternalStream(ps.stream_ptr)
+    stream = ps_stream
+    add("poisson_dirichlet_257x2047", timed(lambda: ps.poisson_solve(rho)),
+        nr * nz * 8 * 5, "rho copied in, phi, E_r, E_z written, phi copied out")
+    ps.close()
+    cpu = None if args.no_cpu_baseline else diag_cpu_times(
+        wl, (1.0 / 64, 1.0 / 32), os.cpu_count() or 1)
+    cpu_p = None if args.no_cpu_baseline else diag_cpu_poisson(os.cpu_count() or 1)
+    if cpu:
+        for name in ("charge_density", "temperature_electrons", "density_electrons"):
+            items[name]["cpu_reference_ms"] = cpu[name]["ms_extrapolated"]
+            items[name]["cpu_samples"] = cpu[name]["samples"]
+            items[name]["speedup_vs_cpu"] = cpu[name]["ms_extrapolated"] / items[name]["ms"]
+    if cpu_p is not None:
+        items["poisson_dirichlet_257x2047"]["cpu_reference_ms"] = cpu_p
+        items["poisson_dirichlet_257x2047"]["speedup_vs_cpu"] = (
+            cpu_p / items["poisson_dirichlet_257x2047"]["ms"])
+    total = sum(v["ms"] for v in items.values())
+    print(json.dumps({
+        "metric": "diagnostics and Poisson solve, device ms per C-ABI call (result copied out)",
+        "value": total, "unit": "ms", "n_gpus": 1, "higher_is_better": False,
+        "dtype": "f64 arithmetic on " + args.precision + " particle state",
+        "data": "synthetic (seeded)",
+        "config": {"workload": wl.name, "particles": n_all,
+                   "poisson_grid": "%dx%d nodes" % DIAG_POISSON_GRID,
+                   "cpu_reference": ("upstream code (oracle/_ref), %d threads, seeded plasma "
+                                     "subsets of 1/64 and 1/32, linear in the particle count"
+                                     % (os.cpu_count() or 1))},
+        "items": items, "peak_gbs": hbm, "peak_source": peak_src}), flush=True)
     return 0
 
 
