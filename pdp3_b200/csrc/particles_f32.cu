@@ -117,17 +117,26 @@ __global__ void k_bunch_inject_f32(SpeciesF32 s, long long start, long long coun
 
 // Particles::charge_weighting (src/particles.cpp:101-226) for the cell-local
 // form: positions are rebuilt in FP64 from (cell, offsets) and weighted with
-// the upstream formulas.
+// the upstream formulas; runs of lanes on the same node block are summed in
+// the warp before the atomics (charge_run_add).  The loop runs whole warps
+// (every lane takes part in the warp sums).
 __global__ void k_charge_density_f32(GridDev g, SpeciesF32 s, double charge, double *rho) {
   const int ncz = g.nz - 1;
   const double dr = g.dr, dz = g.dz;
-  for (long long p = blockIdx.x * (long long)blockDim.x + threadIdx.x; p < s.n;
-       p += (long long)gridDim.x * blockDim.x) {
-    if (s.alive != nullptr && !s.alive[p]) continue;
-    const int c = s.cell[p];
-    const int ci = c / ncz, ck = c - ci * ncz;
-    const double r = (ci + (double)s.fr[p]) * dr, z = (ck + (double)s.fz[p]) * dz;
-    charge_weight_one(g, rho, r, z, charge * (double)s.w[p]);
+  const long long stride = (long long)gridDim.x * blockDim.x;
+  for (long long p0 = blockIdx.x * (long long)blockDim.x + (threadIdx.x & ~31); p0 < s.n;
+       p0 += stride) {
+    const long long p = p0 + (threadIdx.x & 31);
+    const bool live = p < s.n && (s.alive == nullptr || s.alive[p]);
+    int r_i = 0, z_k = 0;
+    double w[4] = {0, 0, 0, 0};
+    if (live) {
+      const int c = s.cell[p];
+      const int ci = c / ncz, ck = c - ci * ncz;
+      const double r = (ci + (double)s.fr[p]) * dr, z = (ck + (double)s.fz[p]) * dz;
+      charge_weights(g, r, z, charge * (double)s.w[p], r_i, z_k, w);
+    }
+    charge_run_add(g, rho, live, r_i, z_k, w);
   }
 }
 

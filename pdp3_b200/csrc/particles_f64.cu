@@ -668,53 +668,31 @@ __global__ void __launch_bounds__(256, 4) k_push_deposit_f64(GridDev g, SpeciesD
   }
 }
 
-// Particles::charge_weighting, src/particles.cpp:101-226
+// Particles::charge_weighting, src/particles.cpp:101-226, with the per
+// particle values of charge_weights (the upstream expressions, compiled here
+// without FMA contraction like the rest of the FP64 form); runs of lanes on
+// the same node block are summed in the warp before the FP64 atomics
+// (charge_run_add), so only the summation order of rho differs from the CPU
+// loop's.  The loop runs whole warps (every lane takes part in the sums).
 __global__ void __launch_bounds__(256) k_charge_density_f64(GridDev g, SpeciesDev s,
                                                             double *rho) {
-  const double dr = g.dr, dz = g.dz;
-  for (long long p = blockIdx.x * (long long)blockDim.x + threadIdx.x; p < s.n;
-       p += (long long)gridDim.x * blockDim.x) {
-    if (s.alive != nullptr && !s.alive[p]) continue;
-    const double r = s.r[p], z = s.z[p], q = s.charge * s.w[p];
-    if (isnan(r) || isinf(r) || isnan(z) || isinf(z)) {
-      flag(g, ERR_NAN);
-      continue;
+  const long long stride = (long long)gridDim.x * blockDim.x;
+  for (long long p0 = blockIdx.x * (long long)blockDim.x + (threadIdx.x & ~31); p0 < s.n;
+       p0 += stride) {
+    const long long p = p0 + (threadIdx.x & 31);
+    bool live = p < s.n && (s.alive == nullptr || s.alive[p]);
+    int r_i = 0, z_k = 0;
+    double w[4] = {0, 0, 0, 0};
+    if (live) {
+      const double r = s.r[p], z = s.z[p], q = s.charge * s.w[p];
+      if (isnan(r) || isinf(r) || isnan(z) || isinf(z)) {
+        flag(g, ERR_NAN);
+        live = false;
+      } else {
+        charge_weights(g, r, z, q, r_i, z_k, w);
+      }
     }
-    int r_i = cell_number(r, dr), z_k = cell_number(z, dz);
-    if (r_i < 0) r_i = 0;
-    if (z_k < 0) z_k = 0;
-    double r1, r2, r3, ro_v, v_1, v_2;
-    const double dz1 = (z_k + 0.5) * dz - (z - 0.5 * dz);
-    const double dz2 = (z + 0.5 * dz) - (z_k + 0.5) * dz;
-    if (r > dr) {
-      r1 = r - 0.5 * dr; r2 = (r_i + 0.5) * dr; r3 = r + 0.5 * dr;
-      ro_v = q / (2. * PI * dz * dr * r);
-      v_1 = PI * dz * dr * dr * 2.0 * (r_i);
-      v_2 = PI * dz * dr * dr * 2.0 * (r_i + 1);
-      add(g, rho, r_i, z_k, ro_v * PI * (dz1) * ((r2) * (r2) - (r1) * (r1)) / v_1);
-      add(g, rho, r_i + 1, z_k, ro_v * PI * (dz1) * ((r3) * (r3) - (r2) * (r2)) / v_2);
-      add(g, rho, r_i, z_k + 1, ro_v * PI * (dz2) * ((r2) * (r2) - (r1) * (r1)) / v_1);
-      add(g, rho, r_i + 1, z_k + 1, ro_v * PI * (dz2) * ((r3) * (r3) - (r2) * (r2)) / v_2);
-    } else if (r <= dr / 2.) {
-      r_i = 0;
-      r2 = (r_i + 0.5) * dr; r3 = r + 0.5 * dr;
-      ro_v = q / (PI * dz * (2. * r * r + dr * dr / 2.));
-      v_1 = PI * (dz) * (dr) * (dr) / 4.;
-      v_2 = PI * dz * dr * dr * 2.0 * (r_i + 1);
-      add(g, rho, r_i, z_k, ro_v * PI * dz1 * (dr * dr / 2. - r * dr + r * r) / v_1);
-      add(g, rho, r_i + 1, z_k, ro_v * PI * (dz1) * ((r3) * (r3) - (r2) * (r2)) / v_2);
-      add(g, rho, r_i, z_k + 1, ro_v * PI * dz2 * (dr * dr / 2. - r * dr + r * r) / v_1);
-      add(g, rho, r_i + 1, z_k + 1, ro_v * PI * (dz2) * ((r3) * (r3) - (r2) * (r2)) / v_2);
-    } else {
-      r1 = r - 0.5 * dr; r2 = (r_i + 0.5) * dr; r3 = r + 0.5 * dr;
-      ro_v = q / (2. * PI * dz * dr * r);
-      v_1 = PI * (dz) * (dr) * (dr) / 4.;
-      v_2 = PI * dz * dr * dr * 2.0 * (r_i + 1);
-      add(g, rho, r_i, z_k, ro_v * PI * (dz1) * ((r2) * (r2) - (r1) * (r1)) / v_1);
-      add(g, rho, r_i + 1, z_k, ro_v * PI * (dz1) * ((r3) * (r3) - (r2) * (r2)) / v_2);
-      add(g, rho, r_i, z_k + 1, ro_v * PI * (dz2) * ((r2) * (r2) - (r1) * (r1)) / v_1);
-      add(g, rho, r_i + 1, z_k + 1, ro_v * PI * (dz2) * ((r3) * (r3) - (r2) * (r2)) / v_2);
-    }
+    charge_run_add(g, rho, live, r_i, z_k, w);
   }
 }
 

@@ -93,15 +93,18 @@ __host__ __device__ inline SpeciesOut in_place(const SpeciesF32 &s) {
   return SpeciesOut{s.cell, s.fr, s.fz, s.ur, s.uphi, s.uz, s.alive};
 }
 
-// Particles::charge_weighting per particle, src/particles.cpp:101-226
-// (adds q at (r, z) into rho with the upstream volume weights).
-__device__ __forceinline__ void charge_weight_one(const GridDev &g, double *rho, double r,
-                                                  double z, double q) {
+// Particles::charge_weighting per particle, src/particles.cpp:101-226: the
+// node block (r_i, z_k) and the 4 values (nodes (r_i, z_k), (r_i+1, z_k),
+// (r_i, z_k+1), (r_i+1, z_k+1)) of charge q at (r, z) with the upstream
+// volume weights.
+__device__ __forceinline__ void charge_weights(const GridDev &g, double r, double z, double q,
+                                               int &r_i, int &z_k, double w[4]) {
   const double dr = g.dr, dz = g.dz;
-  int r_i = (int)ceil(r / dr) - 1, z_k = (int)ceil(z / dz) - 1;
+  r_i = (int)ceil(r / dr) - 1;
+  z_k = (int)ceil(z / dz) - 1;
   if (r_i < 0) r_i = 0;
   if (z_k < 0) z_k = 0;
-  double r1, r2, r3, ro_v, v_1, v_2, w[4];
+  double r1, r2, r3, ro_v, v_1, v_2;
   const double dz1 = (z_k + 0.5) * dz - (z - 0.5 * dz);
   const double dz2 = (z + 0.5 * dz) - (z_k + 0.5) * dz;
   if (r > dr) {
@@ -133,6 +136,47 @@ __device__ __forceinline__ void charge_weight_one(const GridDev &g, double *rho,
     w[2] = ro_v * PI * dz2 * (r2 * r2 - r1 * r1) / v_1;
     w[3] = ro_v * PI * dz2 * (r3 * r3 - r2 * r2) / v_2;
   }
+}
+
+// Segmented sum over runs of consecutive lanes with the same key: every lane
+// of the warp calls it; afterwards the last lane of each run (returns true)
+// holds the run's totals.  Particles sorted by cell form long runs, so the
+// FP64 atomics that follow are one per run and node instead of one per
+// particle and node on the same few addresses.  A lane that must not merge
+// with its neighbours passes a key of its own (e.g. -2 - lane).
+template <int N>
+__device__ __forceinline__ bool warp_run_sum_f64(int key, double (&v)[N]) {
+  const unsigned FULL = 0xffffffffu;
+  const int lane = threadIdx.x & 31;
+  const int prev = __shfl_up_sync(FULL, key, 1);
+  const int next = __shfl_down_sync(FULL, key, 1);
+  const bool head = lane == 0 || prev != key;
+  const bool tail = lane == 31 || next != key;
+  const unsigned heads = __ballot_sync(FULL, head);
+  const unsigned le = lane == 31 ? FULL : ((2u << lane) - 1u);
+  const int seg_start = 31 - __clz(heads & le);
+#pragma unroll
+  for (int j = 0; j < N; j++) {
+    double x = v[j];
+#pragma unroll
+    for (int off = 1; off < 32; off <<= 1) {
+      const double y = __shfl_up_sync(FULL, x, off);
+      if (lane >= seg_start + off) x += y;
+    }
+    v[j] = x;
+  }
+  return tail;
+}
+
+// rho += the charge weights of a warp's particles (charge_weights), one run
+// sum per node block (r_i, z_k).  live: this lane holds a particle.  Blocks
+// that reach outside the grid are not merged (their lanes raise
+// ERR_OUT_OF_GRID for the nodes outside, as one particle would).
+__device__ __forceinline__ void charge_run_add(const GridDev &g, double *rho, bool live, int r_i,
+                                               int z_k, double (&w)[4]) {
+  const bool inside = r_i <= g.nr - 2 && z_k <= g.nz - 2;
+  const int key = !live ? -1 : (inside ? r_i * g.nz + z_k : -2 - (int)(threadIdx.x & 31));
+  if (!warp_run_sum_f64<4>(key, w) || !live) return;
   const int ii[4] = {r_i, r_i + 1, r_i, r_i + 1}, kk[4] = {z_k, z_k, z_k + 1, z_k + 1};
 #pragma unroll
   for (int j = 0; j < 4; j++) {

@@ -11,31 +11,53 @@
 // volumes, with the upstream's three radial branches.
 //
 // Compiled with --fmad=false: the per-particle and per-cell arithmetic keeps
-// the upstream order; only the order of the sums (FP64 atomics) differs.
+// the upstream order; only the order of the sums (warp run sums, then FP64
+// atomics) differs.
 #include "pdp3g_internal.cuh"
 
 namespace pdp3g {
 
 constexpr double REL_LIMIT = 5e7;  // src/temperatureClassic.cpp:4-6
 
-// acc: 5 grids [nr][nz]: sum |v|, sum v_r, sum v_phi, sum v_z, count
-__device__ __forceinline__ void temp_add(const GridDev &g, double *acc, int ri, int zk, double vr,
-                                         double vphi, double vz) {
-  if ((unsigned)ri >= (unsigned)g.nr || (unsigned)zk >= (unsigned)g.nz) return;
+// acc: 5 grids [nr][nz]: sum |v|, sum v_r, sum v_phi, sum v_z, count.
+// Every lane of the warp calls it (live: this lane holds a particle); runs
+// of lanes in the same cell are summed in the warp (warp_run_sum_f64) and
+// added with one set of FP64 atomics.  A cell outside the grid adds nothing.
+__device__ __forceinline__ void temp_run_add(const GridDev &g, double *acc, bool live, int ri,
+                                             int zk, double vr, double vphi, double vz) {
+  const bool inside = live && (unsigned)ri < (unsigned)g.nr && (unsigned)zk < (unsigned)g.nz;
+  double v[5] = {0, 0, 0, 0, 0};
+  if (inside) {
+    v[0] = sqrt(vr * vr + vphi * vphi + vz * vz);
+    v[1] = vr;
+    v[2] = vphi;
+    v[3] = vz;
+    v[4] = 1.0;
+  }
+  const int key = inside ? ri * g.nz + zk : -1;
+  if (!warp_run_sum_f64<5>(key, v) || !inside) return;
   const size_t ng = (size_t)g.nr * g.nz, t = (size_t)ri * g.nz + zk;
-  const double vel = sqrt(vr * vr + vphi * vphi + vz * vz);
-  atomicAdd(acc + t, vel);
-  atomicAdd(acc + ng + t, vr);
-  atomicAdd(acc + 2 * ng + t, vphi);
-  atomicAdd(acc + 3 * ng + t, vz);
-  atomicAdd(acc + 4 * ng + t, 1.0);
+#pragma unroll
+  for (int j = 0; j < 5; j++) atomicAdd(acc + j * ng + t, v[j]);
 }
 
+// The loops below run whole warps: every lane takes part in the warp sums.
 __global__ void k_temp_accum_f64(GridDev g, SpeciesDev s, double *acc) {
-  for (long long p = blockIdx.x * (long long)blockDim.x + threadIdx.x; p < s.n;
-       p += (long long)gridDim.x * blockDim.x) {
-    const int ri = (int)ceil(s.r[p] / g.dr) - 1, zk = (int)ceil(s.z[p] / g.dz) - 1;
-    temp_add(g, acc, ri, zk, s.vr[p], s.vphi[p], s.vz[p]);
+  const long long stride = (long long)gridDim.x * blockDim.x;
+  for (long long p0 = blockIdx.x * (long long)blockDim.x + (threadIdx.x & ~31); p0 < s.n;
+       p0 += stride) {
+    const long long p = p0 + (threadIdx.x & 31);
+    const bool live = p < s.n;
+    int ri = -1, zk = -1;
+    double vr = 0, vphi = 0, vz = 0;
+    if (live) {
+      ri = (int)ceil(s.r[p] / g.dr) - 1;
+      zk = (int)ceil(s.z[p] / g.dz) - 1;
+      vr = s.vr[p];
+      vphi = s.vphi[p];
+      vz = s.vz[p];
+    }
+    temp_run_add(g, acc, live, ri, zk, vr, vphi, vz);
   }
 }
 
@@ -43,15 +65,26 @@ __global__ void k_temp_accum_f64(GridDev g, SpeciesDev s, double *acc) {
 // does (r = (i + f_r) dr, v = u c / sqrt(1 + u^2)), then CELL_NUMBER as above
 __global__ void k_temp_accum_f32(GridDev g, SpeciesF32 s, double *acc) {
   const int ncz = g.nz - 1;
-  for (long long p = blockIdx.x * (long long)blockDim.x + threadIdx.x; p < s.n;
-       p += (long long)gridDim.x * blockDim.x) {
-    const int c = s.cell[p];
-    const int i = c / ncz, k = c - i * ncz;
-    const double r = (i + (double)s.fr[p]) * g.dr, z = (k + (double)s.fz[p]) * g.dz;
-    const int ri = (int)ceil(r / g.dr) - 1, zk = (int)ceil(z / g.dz) - 1;
-    const double ur = s.ur[p], up = s.uphi[p], uz = s.uz[p];
-    const double gc = LIGHT_SPEED / sqrt(1.0 + (ur * ur + up * up + uz * uz));
-    temp_add(g, acc, ri, zk, ur * gc, up * gc, uz * gc);
+  const long long stride = (long long)gridDim.x * blockDim.x;
+  for (long long p0 = blockIdx.x * (long long)blockDim.x + (threadIdx.x & ~31); p0 < s.n;
+       p0 += stride) {
+    const long long p = p0 + (threadIdx.x & 31);
+    const bool live = p < s.n;
+    int ri = -1, zk = -1;
+    double vr = 0, vphi = 0, vz = 0;
+    if (live) {
+      const int c = s.cell[p];
+      const int i = c / ncz, k = c - i * ncz;
+      const double r = (i + (double)s.fr[p]) * g.dr, z = (k + (double)s.fz[p]) * g.dz;
+      ri = (int)ceil(r / g.dr) - 1;
+      zk = (int)ceil(z / g.dz) - 1;
+      const double ur = s.ur[p], up = s.uphi[p], uz = s.uz[p];
+      const double gc = LIGHT_SPEED / sqrt(1.0 + (ur * ur + up * up + uz * uz));
+      vr = ur * gc;
+      vphi = up * gc;
+      vz = uz * gc;
+    }
+    temp_run_add(g, acc, live, ri, zk, vr, vphi, vz);
   }
 }
 
@@ -84,12 +117,13 @@ __global__ void k_temp_normalize(GridDev g, const double *acc, double mass, doub
   }
 }
 
-// ParticlesDensity::calc_density for one particle (r, z, mass_array m)
-__device__ __forceinline__ void density_add(const GridDev &g, double *out, double r, double z,
-                                            double m) {
+// ParticlesDensity::calc_density for one particle (r, z, mass_array m):
+// the node block (ri, zk) and the 4 values (nodes ri..ri+1 x zk..zk+1)
+__device__ __forceinline__ void density_values(const GridDev &g, double r, double z, double m,
+                                               int &ri, int &zk, double (&out)[4]) {
   const double dr = g.dr, dz = g.dz;
-  int ri = (int)ceil(r / dr) - 1;
-  const int zk = (int)ceil(z / dz) - 1;
+  ri = (int)ceil(r / dr) - 1;
+  zk = (int)ceil(z / dz) - 1;
   const bool outer = r > dr, inner = !outer && r <= dr / 2.;
   if (inner) ri = 0;
   const double rif = (double)ri;
@@ -112,27 +146,55 @@ __device__ __forceinline__ void density_add(const GridDev &g, double *out, doubl
   }
   val[1] = PI * dz1 * (r3 * r3 - r2 * r2) / v2;
   val[3] = PI * dz2 * (r3 * r3 - r2 * r2) / v2;
+#pragma unroll
+  for (int j = 0; j < 4; j++) out[j] = ro_p * val[j];
+}
+
+// out += the density values of a warp's particles, one run sum per node
+// block; nodes outside the grid are skipped (no flag, as upstream's bounds
+// test); a block that reaches outside the grid is not merged with others.
+__device__ __forceinline__ void density_run_add(const GridDev &g, double *out, bool live, int ri,
+                                                int zk, double (&v)[4]) {
+  const bool inside = ri >= 0 && zk >= 0 && ri <= g.nr - 2 && zk <= g.nz - 2;
+  const int key = !live ? -1 : (inside ? ri * g.nz + zk : -2 - (int)(threadIdx.x & 31));
+  if (!warp_run_sum_f64<4>(key, v) || !live) return;
+#pragma unroll
   for (int j = 0; j < 4; j++) {
     const int i = ri + (j & 1), k = zk + (j >> 1);
     if ((unsigned)i < (unsigned)g.nr && (unsigned)k < (unsigned)g.nz)
-      atomicAdd(out + (size_t)i * g.nz + k, ro_p * val[j]);
+      atomicAdd(out + (size_t)i * g.nz + k, v[j]);
   }
 }
 
 __global__ void k_density_f64(GridDev g, SpeciesDev s, double *out) {
-  for (long long p = blockIdx.x * (long long)blockDim.x + threadIdx.x; p < s.n;
-       p += (long long)gridDim.x * blockDim.x)
-    density_add(g, out, s.r[p], s.z[p], s.mass * s.w[p]);
+  const long long stride = (long long)gridDim.x * blockDim.x;
+  for (long long p0 = blockIdx.x * (long long)blockDim.x + (threadIdx.x & ~31); p0 < s.n;
+       p0 += stride) {
+    const long long p = p0 + (threadIdx.x & 31);
+    const bool live = p < s.n;
+    int ri = 0, zk = 0;
+    double v[4] = {0, 0, 0, 0};
+    if (live) density_values(g, s.r[p], s.z[p], s.mass * s.w[p], ri, zk, v);
+    density_run_add(g, out, live, ri, zk, v);
+  }
 }
 
 __global__ void k_density_f32(GridDev g, SpeciesF32 s, double mass, double *out) {
   const int ncz = g.nz - 1;
-  for (long long p = blockIdx.x * (long long)blockDim.x + threadIdx.x; p < s.n;
-       p += (long long)gridDim.x * blockDim.x) {
-    const int c = s.cell[p];
-    const int i = c / ncz, k = c - i * ncz;
-    density_add(g, out, (i + (double)s.fr[p]) * g.dr, (k + (double)s.fz[p]) * g.dz,
-                mass * (double)s.w[p]);
+  const long long stride = (long long)gridDim.x * blockDim.x;
+  for (long long p0 = blockIdx.x * (long long)blockDim.x + (threadIdx.x & ~31); p0 < s.n;
+       p0 += stride) {
+    const long long p = p0 + (threadIdx.x & 31);
+    const bool live = p < s.n;
+    int ri = 0, zk = 0;
+    double v[4] = {0, 0, 0, 0};
+    if (live) {
+      const int c = s.cell[p];
+      const int i = c / ncz, k = c - i * ncz;
+      density_values(g, (i + (double)s.fr[p]) * g.dr, (k + (double)s.fz[p]) * g.dz,
+                     mass * (double)s.w[p], ri, zk, v);
+    }
+    density_run_add(g, out, live, ri, zk, v);
   }
 }
 
