@@ -205,6 +205,22 @@ pdp3g_status pdp3g_exchange_species(pdp3g_ctx *ctx, int32_t id, double *out_r, d
                                     uint8_t *out_alive, const double *in_r, const double *in_z,
                                     const double *in_vr, const double *in_vphi,
                                     const double *in_vz, const uint8_t *in_alive);
+/* pdp3g_exchange_species for several species in one call, for a host that
+   holds every species' state (ParticlesList::part_list, particlesList.h:9-26):
+   the copies of all items run as one pipeline (species after species on
+   each PCIe direction, with no gap at a species boundary) and the FP32
+   form's conversions to and from the FP64 host layout run on a third stream
+   beside them.  Each species at most once; returns when every copy is done.
+   Same arrays, checks and in == out rule as pdp3g_exchange_species. */
+typedef struct {
+  int32_t id;
+  double *out_r, *out_z, *out_vr, *out_vphi, *out_vz;
+  uint8_t *out_alive;
+  const double *in_r, *in_z, *in_vr, *in_vphi, *in_vz;
+  const uint8_t *in_alive;
+} pdp3g_exchange_item;
+pdp3g_status pdp3g_exchange_all(pdp3g_ctx *ctx, const pdp3g_exchange_item *items,
+                                int32_t n_items);
 pdp3g_status pdp3g_set_species(pdp3g_ctx *ctx, int32_t id, const double *r, const double *z,
                                const double *vr, const double *vphi, const double *vz,
                                const uint8_t *alive);

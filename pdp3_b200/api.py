@@ -57,6 +57,16 @@ class EnsembleInfo(ctypes.Structure):
                 ("graph_blocks_per_sm", ctypes.c_int32)]
 
 
+class ExchangeItem(ctypes.Structure):
+    _fields_ = ([("id", ctypes.c_int32)] +
+                [("out_" + k, ctypes.POINTER(ctypes.c_double))
+                 for k in ("r", "z", "vr", "vphi", "vz")] +
+                [("out_alive", ctypes.POINTER(ctypes.c_uint8))] +
+                [("in_" + k, ctypes.POINTER(ctypes.c_double))
+                 for k in ("r", "z", "vr", "vphi", "vz")] +
+                [("in_alive", ctypes.POINTER(ctypes.c_uint8))])
+
+
 class Timing(ctypes.Structure):
     _fields_ = [("ms_step_total", ctypes.c_double), ("ms_particles", ctypes.c_double),
                 ("ms_fields", ctypes.c_double), ("ms_sort", ctypes.c_double),
@@ -129,6 +139,7 @@ EXPORTS = [
     ("pdp3g_temperature", _I32, [_VP, _I32, _D]),
     ("pdp3g_density", _I32, [_VP, _I32, _D]),
     ("pdp3g_exchange_species", _I32, [_VP, _I32] + [_D] * 5 + [_U8] + [_D] * 5 + [_U8]),
+    ("pdp3g_exchange_all", _I32, [_VP, ctypes.POINTER(ExchangeItem), _I32]),
     ("pdp3g_poisson_solve", _I32, [_VP, _D, _D]),
     ("pdp3g_probe_particles", _I32, [_VP] + [_I32] * 5 + [_D] * 5 +
      [ctypes.c_int64, ctypes.POINTER(ctypes.c_int64)]),
@@ -292,6 +303,30 @@ class Simulation:
             oa.ctypes.data_as(_U8) if oa is not None else None,
             *[_p(inp[k]) for k in keys],
             ia.ctypes.data_as(_U8) if ia is not None else None), "exchange_species")
+
+    def exchange_all(self, items):
+        """pdp3g_exchange_all: items is a list of (sid, out, inp) with out and
+        inp as in exchange_species; one pipeline over all of them."""
+        keys = ("r", "z", "vr", "vphi", "vz")
+        arr = (ExchangeItem * len(items))()
+        for j, (sid, out, inp) in enumerate(items):
+            n = self.species_size(sid)
+            for d in (out, inp):
+                for k in keys:
+                    a = d[k]
+                    assert a.dtype == np.float64 and a.flags.c_contiguous and a.size == n, k
+                for k in ("alive",):
+                    a = d.get(k)
+                    assert a is None or (a.dtype == np.uint8 and a.size == n), k
+            it = arr[j]
+            it.id = sid
+            for k in keys:
+                setattr(it, "out_" + k, _p(out[k]))
+                setattr(it, "in_" + k, _p(inp[k]))
+            oa, ia = out.get("alive"), inp.get("alive")
+            it.out_alive = oa.ctypes.data_as(_U8) if oa is not None else None
+            it.in_alive = ia.ctypes.data_as(_U8) if ia is not None else None
+        self._check(self.L.pdp3g_exchange_all(self.h, arr, len(items)), "exchange_all")
 
     def set_species(self, sid, r=None, z=None, vr=None, vphi=None, vz=None, alive=None):
         keep = [None if a is None else _f64(a) for a in (r, z, vr, vphi, vz)]

@@ -45,6 +45,10 @@ struct pdp3g_ctx {
   cudaStream_t stream_side = nullptr;
   cudaEvent_t ev_fork = nullptr, ev_join = nullptr;
   cudaEvent_t ev_chunk = nullptr, ev_up = nullptr;
+  // pdp3g_exchange_all: FP64 staging of every FP32 item, and 2 events per item
+  double *d_xstage = nullptr;
+  size_t xstage_n = 0;
+  std::vector<cudaEvent_t> xev;
   double dr = 0, dz = 0, t = 0;
   double *grid_mem = nullptr;
   float *mirror = nullptr;       // FP32 contexts: E and half-step H in FP32 (6 grids)
@@ -371,6 +375,8 @@ void pdp3g_destroy(pdp3g_ctx *ctx) {
   if (ctx->ev_join) cudaEventDestroy(ctx->ev_join);
   if (ctx->ev_chunk) cudaEventDestroy(ctx->ev_chunk);
   if (ctx->ev_up) cudaEventDestroy(ctx->ev_up);
+  for (cudaEvent_t e : ctx->xev) cudaEventDestroy(e);
+  cudaFree(ctx->d_xstage);
   delete ctx;
 }
 
@@ -1079,6 +1085,130 @@ pdp3g_status pdp3g_exchange_species(pdp3g_ctx *ctx, int32_t id, double *out_r, d
     CK(cudaStreamSynchronize(down));
   }
   if (!dev_alive && out_alive) memset(out_alive, 1, n);
+  return PDP3G_OK;
+}
+
+// pdp3g_exchange_all: one pipeline over the items.  Streams: the context's
+// stream (down) carries every device->host copy, item after item; stream_up
+// every host->device copy, chunk c of an item after that chunk went out;
+// stream_side the FP32 items' conversions, to the FP64 layout before their
+// copies out (side by side with the previous items' copies) and back after
+// their copies in.  Each FP32 item has its own FP64 staging, so no item
+// waits for another's conversion.
+pdp3g_status pdp3g_exchange_all(pdp3g_ctx *ctx, const pdp3g_exchange_item *items,
+                                int32_t n_items) {
+  if (!ctx || n_items < 0 || (n_items > 0 && !items)) return PDP3G_INVALID_ARG;
+  const int nsp = (int)ctx->species.size();
+  std::vector<char> seen(nsp, 0);
+  size_t stage_total = 0;
+  for (int j = 0; j < n_items; j++) {
+    const pdp3g_exchange_item &it = items[j];
+    if (it.id < 0 || it.id >= nsp || seen[it.id])
+      return fail(ctx, PDP3G_INVALID_ARG, "exchange_all: unknown or repeated species id");
+    seen[it.id] = 1;
+    const void *arr[10] = {it.out_r, it.out_z, it.out_vr, it.out_vphi, it.out_vz,
+                           it.in_r,  it.in_z,  it.in_vr,  it.in_vphi,  it.in_vz};
+    for (const void *a : arr)
+      if (!a) return fail(ctx, PDP3G_INVALID_ARG, "exchange_all: null array");
+    const Species &sp = ctx->species[it.id];
+    if (sp.fp32) stage_total += 5 * (size_t)sp.f32.n;
+  }
+  if (n_items == 0) return PDP3G_OK;
+  CK(cudaSetDevice(ctx->device));
+  if (!ctx->stream_up) {
+    CK(cudaStreamCreateWithFlags(&ctx->stream_up, cudaStreamNonBlocking));
+    CK(cudaEventCreateWithFlags(&ctx->ev_chunk, cudaEventDisableTiming));
+    CK(cudaEventCreateWithFlags(&ctx->ev_up, cudaEventDisableTiming));
+  }
+  while (ctx->xev.size() < 2 * (size_t)n_items + 2) {
+    cudaEvent_t e;
+    CK(cudaEventCreateWithFlags(&e, cudaEventDisableTiming));
+    ctx->xev.push_back(e);
+  }
+  if (ctx->xstage_n < stage_total) {
+    cudaFree(ctx->d_xstage);
+    ctx->d_xstage = nullptr;
+    ctx->xstage_n = 0;
+    CK(dalloc(ctx, &ctx->d_xstage, stage_total));
+    ctx->xstage_n = stage_total;
+  }
+  cudaStream_t down = ctx->stream, up = ctx->stream_up, side = ctx->stream_side;
+  cudaEvent_t *ev_conv = ctx->xev.data(), *ev_in = ctx->xev.data() + n_items;
+  cudaEvent_t ev_begin = ctx->xev[2 * n_items], ev_side_end = ctx->xev[2 * n_items + 1];
+  // everything already queued on the context's stream first
+  CK(cudaEventRecord(ev_begin, down));
+  CK(cudaStreamWaitEvent(up, ev_begin, 0));
+  CK(cudaStreamWaitEvent(side, ev_begin, 0));
+  CK(cudaMemsetAsync(ctx->d_err + 1, 0, sizeof(unsigned), side));
+  const int ncz = ctx->cfg.n_grid_z - 1;
+  std::vector<double *> stage(n_items, nullptr);
+  size_t off = 0;
+  for (int j = 0; j < n_items; j++) {
+    Species &sp = ctx->species[items[j].id];
+    if (!sp.fp32) continue;
+    const size_t n = (size_t)sp.f32.n;
+    double *S = ctx->d_xstage + off;
+    off += 5 * n;
+    stage[j] = S;
+    launch_cell_to_f64(sp.f32, ctx->dr, ctx->dz, ncz, S, S + n, S + 2 * n, S + 3 * n, S + 4 * n,
+                       nullptr, side);
+    ctx->launches++;
+    CK(cudaEventRecord(ev_conv[j], side));
+  }
+  for (int j = 0; j < n_items; j++) {
+    const pdp3g_exchange_item &it = items[j];
+    Species &sp = ctx->species[it.id];
+    const size_t n = (size_t)(sp.fp32 ? sp.f32.n : sp.dev.n);
+    double *outs[5] = {it.out_r, it.out_z, it.out_vr, it.out_vphi, it.out_vz};
+    const double *ins[5] = {it.in_r, it.in_z, it.in_vr, it.in_vphi, it.in_vz};
+    double *dev[5];
+    uint8_t *dev_alive = sp.fp32 ? sp.f32.alive : sp.dev.alive;
+    if (sp.fp32) {
+      for (int k = 0; k < 5; k++) dev[k] = stage[j] + k * n;
+      CK(cudaStreamWaitEvent(down, ev_conv[j], 0));
+    } else {
+      double *a[5] = {sp.dev.r, sp.dev.z, sp.dev.vr, sp.dev.vphi, sp.dev.vz};
+      for (int k = 0; k < 5; k++) dev[k] = a[k];
+    }
+    for (size_t c0 = 0; c0 < n; c0 += EXCHANGE_CHUNK) {
+      const size_t cn = std::min(EXCHANGE_CHUNK, n - c0), b = sizeof(double) * cn;
+      for (int k = 0; k < 5; k++)
+        CK(cudaMemcpyAsync(outs[k] + c0, dev[k] + c0, b, cudaMemcpyDeviceToHost, down));
+      if (dev_alive && it.out_alive)
+        CK(cudaMemcpyAsync(it.out_alive + c0, dev_alive + c0, cn, cudaMemcpyDeviceToHost, down));
+      CK(cudaEventRecord(ctx->ev_chunk, down));
+      CK(cudaStreamWaitEvent(up, ctx->ev_chunk, 0));
+      for (int k = 0; k < 5; k++)
+        CK(cudaMemcpyAsync(dev[k] + c0, ins[k] + c0, b, cudaMemcpyHostToDevice, up));
+      if (dev_alive && it.in_alive)
+        CK(cudaMemcpyAsync(dev_alive + c0, it.in_alive + c0, cn, cudaMemcpyHostToDevice, up));
+    }
+    CK(cudaEventRecord(ev_in[j], up));
+    if (sp.fp32) {
+      CK(cudaStreamWaitEvent(side, ev_in[j], 0));
+      launch_f64_to_cell(sp.f32, stage[j], stage[j] + n, stage[j] + 2 * n, stage[j] + 3 * n,
+                         stage[j] + 4 * n, nullptr, ctx->dr, ctx->dz, ctx->cfg.n_grid_r,
+                         ctx->cfg.n_grid_z, ctx->d_err + 1, side);
+      ctx->launches++;
+    }
+  }
+  // the context's stream continues after the last copy in and conversion
+  CK(cudaEventRecord(ev_side_end, side));
+  CK(cudaEventRecord(ctx->ev_up, up));
+  CK(cudaStreamWaitEvent(down, ev_side_end, 0));
+  CK(cudaStreamWaitEvent(down, ctx->ev_up, 0));
+  unsigned err = 0;
+  CK(cudaMemcpyAsync(&err, ctx->d_err + 1, sizeof(unsigned), cudaMemcpyDeviceToHost, down));
+  CK(cudaStreamSynchronize(down));
+  for (int j = 0; j < n_items; j++) {
+    const Species &sp = ctx->species[items[j].id];
+    const uint8_t *dev_alive = sp.fp32 ? sp.f32.alive : sp.dev.alive;
+    if (!dev_alive && items[j].out_alive)
+      memset(items[j].out_alive, 1, (size_t)(sp.fp32 ? sp.f32.n : sp.dev.n));
+  }
+  if (err & ERR_NAN) return fail(ctx, PDP3G_NAN_DETECTED, "particle position is NaN or Inf");
+  if (err & ERR_V_GE_C) return fail(ctx, PDP3G_V_GE_C, "velocity >= c");
+  if (err & ERR_OUT_OF_GRID) return fail(ctx, PDP3G_OUT_OF_GRID, "particle outside the grid");
   return PDP3G_OK;
 }
 

@@ -8,6 +8,10 @@ copy directions pipelined by chunks of 2^20 particles on two streams.
   state is unchanged and the next step equals the step of a context that
   made no round trip (to 1e-12 in the FP64 form: its grid currents are
   summed by atomics in a varying order).
+* pdp3g_exchange_all (every species in one pipeline): out receives the
+  state as pdp3g_exchange_species's out does, and the state loaded from the
+  same input arrays equals what one pdp3g_exchange_species call per species
+  loads, in any item order; a repeated species or a null array is refused.
 """
 import numpy as np
 import pytest
@@ -91,3 +95,59 @@ def test_round_trip_in_place_several_chunks(precision):
         assert rel_inf(a.field(c), b.field(c)) <= tol, c
     a.close()
     b.close()
+
+
+@pytest.mark.parametrize("precision", ["fp64", "fp32"])
+def test_exchange_all_equals_one_call_per_species(precision):
+    wl = W.wake_config(ppc=3)          # 2 chunks per plasma species, and the bunch
+    a = api.from_workload(wl, precision=precision)
+    b = api.from_workload(wl, precision=precision)
+    for s_ in (a, b):
+        s_.step(3)
+        s_.sync()
+    n_sp = 3
+    # each context's own state (two runs differ by the atomics' summation order)
+    states = [a.species(sid) for sid in range(n_sp)]
+    states_b = [b.species(sid) for sid in range(n_sp)]
+    outs_a, outs_b, inps = [], [], []
+    for sid in range(n_sp):
+        n = states[sid]["r"].size
+        inp = {k: pinned(states[sid][k]) for k in KEYS}
+        inp["vz"] = pinned(states[sid]["vz"] * 0.5)
+        inp["alive"] = pinned(states[sid]["alive"])
+        inps.append(inp)
+        for outs in (outs_a, outs_b):
+            o = {k: pinned(np.zeros(n)) for k in KEYS}
+            o["alive"] = pinned(np.zeros(n, dtype=np.uint8))
+            outs.append(o)
+    # items in reverse species order: the order of the items is free
+    a.exchange_all([(sid, outs_a[sid], inps[sid]) for sid in reversed(range(n_sp))])
+    for sid in range(n_sp):
+        b.exchange_species(sid, outs_b[sid], inps[sid])
+    for sid in range(n_sp):
+        for k in KEYS + ("alive",):
+            assert np.array_equal(outs_a[sid][k], states[sid][k]), (sid, k)
+            assert np.array_equal(outs_b[sid][k], states_b[sid][k]), (sid, k)
+        # the state loaded from the same input arrays is the same
+        sa, sb = a.species(sid), b.species(sid)
+        for k in KEYS + ("alive",):
+            assert np.array_equal(sa[k], sb[k]), (sid, k)
+    # in place, all species at once
+    bufs = [{k: pinned(a.species(sid)[k]) for k in KEYS + ("alive",)} for sid in range(n_sp)]
+    keep = [{k: v.copy() for k, v in bf.items()} for bf in bufs]
+    a.exchange_all([(sid, bufs[sid], bufs[sid]) for sid in range(n_sp)])
+    for sid in range(n_sp):
+        now = a.species(sid)
+        for k in KEYS:
+            assert np.array_equal(bufs[sid][k], keep[sid][k]), (sid, k)
+            if precision == "fp64":
+                assert np.array_equal(now[k], keep[sid][k]), (sid, k)
+    with pytest.raises(api.Pdp3gError):
+        a.exchange_all([(0, bufs[0], bufs[0]), (0, bufs[0], bufs[0])])
+    arr = (api.ExchangeItem * 1)()
+    arr[0].id = 0
+    with pytest.raises(api.Pdp3gError):
+        a._check(a.L.pdp3g_exchange_all(a.h, arr, 1), "exchange_all")
+    a.close()
+    b.close()
+
