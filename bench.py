@@ -356,10 +356,10 @@ def main():
         torch.cuda.synchronize()
         alive0 = alive_count(sim, wl)
         sim.reset_timing()
-        sim.set_timing(True)
         if sample_clocks:
             clocks.start()
             time.sleep(0.3)
+        # the timed steps as a user runs them: one captured graph per step
         ev0 = torch.cuda.Event(enable_timing=True)
         ev1 = torch.cuda.Event(enable_timing=True)
         ev0.record(stream)
@@ -369,9 +369,18 @@ def main():
         torch.cuda.synchronize()
         clk = clocks.stop() if sample_clocks else None
         ms = ev0.elapsed_time(ev1)
-        tm = sim.timing()
-        sim.set_timing(False)
+        launches = sim.timing()["launches"]
         alive1 = alive_count(sim, wl)
+        # the per-phase breakdown (kernel_ms, the roofline's particle-phase
+        # time) from further steps launched one by one with events between
+        # the phases
+        sim.reset_timing()
+        sim.set_timing(True)
+        sim.step(max(3, min(args.steps, 10)))
+        sim.sync()
+        tm = sim.timing()
+        tm["launches"] = launches
+        sim.set_timing(False)
         particle_steps = 0.5 * (alive0 + alive1) * args.steps
         ms_max, total_ps = aggregate_ranks(dist, ms, particle_steps, "cuda")
         diag = sim.diagnostics()
@@ -412,7 +421,7 @@ def main():
         "fp32_over_fp64": v32 / v64,
         "field_energy_rel_diff": abs(d32["field_energy"] - d64["field_energy"]) /
         d64["field_energy"] if d64["field_energy"] > 0 else None,
-        "after_steps": args.warmup + args.steps,
+        "after_steps": args.warmup + args.steps + max(3, min(args.steps, 10)),
     }
 
     # end to end through the public API from pinned host buffers: every step

@@ -65,6 +65,36 @@ __global__ void k_adj_e(GridDev g, AdjGrids A) {
   }
 }
 
+// Between steps 1 and 2: cell (i, k) is active when any adjoint of J that
+// the particles starting in it read is nonzero.  A particle's step moves it
+// at most half a cell (Courant 0.5), so its mid-step and path cells lie
+// within one cell of its start cell and the nodes it reads adjoints of J at
+// within i-1..i+2, k-1..k+2.  The adjoints of the fields spread from the
+// probe by one node per step (the Yee stencil), so early in the reverse most
+// cells are inactive; a particle whose own adjoints are zero in an inactive
+// cell has a reverse whose every output is zero (the reverse is linear in
+// them) and is skipped.
+__global__ void k_adj_active(GridDev g, AdjGrids A, uint8_t *active) {
+  const int nr = g.nr, nz = g.nz, ncz = nz - 1;
+  const long long total = (long long)(nr - 1) * ncz;
+  for (long long t = blockIdx.x * (long long)blockDim.x + threadIdx.x; t < total;
+       t += (long long)gridDim.x * blockDim.x) {
+    const int i = (int)(t / ncz), k = (int)(t - (long long)i * ncz);
+    const int i0 = max(i - 1, 0), i1 = min(i + 2, nr - 1);
+    const int k0 = max(k - 1, 0), k1 = min(k + 2, nz - 1);
+    bool any = false;
+    for (int ii = i0; ii <= i1 && !any; ii++)
+      for (int kk = k0; kk <= k1; kk++) {
+        const size_t n = AIDX(ii, kk);
+        if (A.lJr[n] != 0.0f || A.lJphi[n] != 0.0f || A.lJz[n] != 0.0f) {
+          any = true;
+          break;
+        }
+      }
+    active[t] = any ? 1 : 0;
+  }
+}
+
 // step 4: H update transposed, every node: where the H update ran,
 // lE += a^T(lH + lHh/2) and lH += lHh; everywhere lHh = 0 (the half-step
 // values the update did not write never change, so their adjoints are
@@ -189,7 +219,8 @@ __device__ __forceinline__ bool warp_seg_sum(int key, float (&v)[N]) {
 // wall-reflection jump terms (face bit 1) are compiled in.
 template <bool WALLS>
 __global__ void __launch_bounds__(ADJ_THREADS, ADJ_MIN_BLOCKS) k_adj_particles(
-    GridDev g, const float4 *Q, AdjSpeciesDev S, AdjGrids A, int face, float face_h) {
+    GridDev g, const float4 *Q, AdjSpeciesDev S, AdjGrids A, const uint8_t *active, int face,
+    float face_h) {
   const int ncz = g.nz - 1;
   const size_t ncells = (size_t)(g.nr - 1) * ncz;
   adj::Consts<float> C;
@@ -212,6 +243,12 @@ __global__ void __launch_bounds__(ADJ_THREADS, ADJ_MIN_BLOCKS) k_adj_particles(
     bool live = p < S.st.n && (S.st.alive == nullptr || S.st.alive[p]);
     const int c = live ? S.st.cell[p] : 0;
     if (c < 0 || c >= (g.nr - 1) * ncz) live = false;  // flagged by the forward step
+    // zero adjoints of the particle and none of J within its reach (k_adj_active):
+    // every output of its reverse is zero, nothing to do
+    if (live && S.la[p] == 0.0f && S.lb[p] == 0.0f && S.lur[p] == 0.0f && S.luphi[p] == 0.0f &&
+        S.luz[p] == 0.0f && !active[c])
+      live = false;
+    if (__all_sync(0xffffffffu, !live)) continue;  // the whole warp: no sums to add either
     const int ci = c / ncz, ck = c - (c / ncz) * ncz;
     float lf[24];  // this lane's field-node adjoints, reduced across the warp
     int key = -1, q_ir_h = 0, q_kz_h = 0;
@@ -380,8 +417,13 @@ void adj_launch_h(const GridDev &g, const AdjGrids &A, cudaStream_t st) {
   k_adj_h<<<blocks_for((long long)g.nr * g.nz, 256), 256, 0, st>>>(g, A);
 }
 
+void adj_launch_active(const GridDev &g, const AdjGrids &A, uint8_t *active, cudaStream_t st) {
+  k_adj_active<<<blocks_for((long long)(g.nr - 1) * (g.nz - 1), 256), 256, 0, st>>>(g, A, active);
+}
+
 void adj_launch_particles(const GridDev &g, const float4 *Q, const AdjSpeciesDev &S,
-                          const AdjGrids &A, int face, float face_h, cudaStream_t st) {
+                          const AdjGrids &A, const uint8_t *active, int face, float face_h,
+                          cudaStream_t st) {
   if (S.st.n <= 0) return;
   const long long nchunks = (S.st.n + ADJ_THREADS - 1) / ADJ_THREADS;
   auto kernel = (face & 2) ? k_adj_particles<true> : k_adj_particles<false>;
@@ -393,8 +435,8 @@ void adj_launch_particles(const GridDev &g, const float4 *Q, const AdjSpeciesDev
   cudaGetDevice(&dev);
   cudaDeviceGetAttribute(&nsm, cudaDevAttrMultiProcessorCount, dev);
   const long long blocks = std::min<long long>(nchunks, (long long)bpsm * nsm);
-  kernel<<<(int)std::max<long long>(blocks, 1), ADJ_THREADS, 0, st>>>(g, Q, S, A, face,
-                                                                         face_h);
+  kernel<<<(int)std::max<long long>(blocks, 1), ADJ_THREADS, 0, st>>>(g, Q, S, A, active,
+                                                                         face, face_h);
 }
 
 void adj_launch_inject(const AdjSpeciesDev &S, long long start, long long count, double dt,

@@ -80,6 +80,15 @@ struct pdp3g_ctx {
   std::string last_error;
   int64_t bytes = 0;
   int f32_blocks_per_sm = 0;  // CTAs per SM for the FP32 particle kernel (0: its default)
+  // pdp3g_step without timing replays one captured graph per step; the graph
+  // reads and advances the device copy of t.  Recaptured when the species or
+  // the particle kernel's launch shape change.
+  double *d_time = nullptr;
+  cudaGraphExec_t step_exec = nullptr;
+  size_t graph_nsp = 0;
+  int graph_bpsm = -1;
+  int64_t graph_launches = 0, graph_particle_launches = 0;
+  bool graph_off = false;  // a capture failed: eager steps from then on
 };
 
 namespace {
@@ -314,6 +323,8 @@ pdp3g_status pdp3g_create(const pdp3g_config *cfg, pdp3g_ctx **out) {
   g.jz = comp_ptr(ctx, PDP3G_J_Z);
   g.sigma = comp_ptr(ctx, PDP3G_SIGMA);
   g.err = ctx->d_err;
+  if ((e = dalloc(ctx, &ctx->d_time, 1)) != cudaSuccess)
+    return bail(e == cudaErrorMemoryAllocation ? PDP3G_NO_MEMORY : PDP3G_CUDA_ERROR);
   if (cfg->precision == PDP3G_FP32_CELL) {
     if ((e = dalloc(ctx, &ctx->mirror, 6 * ng)) != cudaSuccess)
       return bail(e == cudaErrorMemoryAllocation ? PDP3G_NO_MEMORY : PDP3G_CUDA_ERROR);
@@ -355,6 +366,8 @@ void pdp3g_destroy(pdp3g_ctx *ctx) {
   for (auto &se : ctx->step_events)
     for (auto &e : se.ev) cudaEventDestroy(e);
   cudaFree(ctx->grid_mem);
+  if (ctx->step_exec) cudaGraphExecDestroy(ctx->step_exec);
+  cudaFree(ctx->d_time);
   cudaFree(ctx->mirror);
   cudaFree(ctx->quads);
   cudaFree(ctx->d_err);
@@ -855,33 +868,137 @@ static void phase_advance(pdp3g_ctx *ctx) {
   ctx->steps++;
 }
 
+// Bunch::bunch_inject of every bunch with the schedule evaluated on the
+// device from the device copy of t (the form a captured step uses); the
+// window constants are computed here as inject_range computes them.
+static void phase_inject_dev(pdp3g_ctx *ctx) {
+  const double dt = ctx->cfg.dt;
+  for (auto &sp : ctx->species) {
+    if (!sp.is_bunch) continue;
+    const double begin = sp.duration * sp.bunch_number + sp.hole_duration * sp.bunch_number;
+    const double end = begin + sp.duration;
+    const int steps_amount = (int)std::ceil(sp.duration / dt);
+    const unsigned number = (unsigned)(sp.fp32 ? sp.f32.n : sp.dev.n);
+    const unsigned pis = steps_amount > 0 ? number / steps_amount : 0;
+    const double dl = sp.velocity * dt;
+    if (sp.fp32) {
+      const double b2 = sp.velocity * sp.velocity / LIGHT_SPEED_POW_2;
+      const double gv = sp.velocity / (LIGHT_SPEED * std::sqrt(1.0 - b2));
+      launch_bunch_inject_f32_dev(sp.f32, ctx->d_time, begin, end, dt, pis, dl, ctx->dz / 2.0,
+                                  ctx->dz, ctx->cfg.n_grid_z - 1, (float)gv, ctx->d_inv_pow11,
+                                  ctx->stream);
+    } else {
+      launch_bunch_inject_dev(sp.dev, ctx->d_time, begin, end, dt, pis, dl, ctx->dz / 2.0,
+                              sp.velocity, ctx->d_inv_pow11, ctx->stream);
+    }
+    if (pis > 0) ctx->launches++;
+  }
+}
+
+// One step of LoadInitParam::run's loop body, launched one kernel at a time
+// (the timing path, re-sort steps, and the fallback of a failed capture).
+static pdp3g_status step_eager(pdp3g_ctx *ctx) {
+  cudaStream_t st = ctx->stream;
+  StepEvents *ev = ctx->timing ? next_events(ctx) : nullptr;
+  if (ev) cudaEventRecord(ev->ev[0], st);
+  phase_inject(ctx);
+  if (ev) cudaEventRecord(ev->ev[1], st);
+  phase_calc_h(ctx);
+  if (ev) cudaEventRecord(ev->ev[2], st);
+  CK(phase_reset_j(ctx));
+  if (ev) cudaEventRecord(ev->ev[3], st);
+  if (ctx->cfg.sort_interval > 0 && ctx->steps % ctx->cfg.sort_interval == 0) {
+    pdp3g_status ss = sort_all(ctx);
+    if (ss != PDP3G_OK) return ss;
+  }
+  if (ev) cudaEventRecord(ev->ev[4], st);
+  CK(phase_particles(ctx));
+  if (ev) cudaEventRecord(ev->ev[5], st);
+  phase_calc_e(ctx);
+  if (ev) cudaEventRecord(ev->ev[6], st);
+  phase_advance(ctx);
+  if (ctx->timing && ctx->events_used >= 4096) {
+    pdp3g_status hs = harvest_timing(ctx);
+    if (hs != PDP3G_OK) return hs;
+  }
+  return PDP3G_OK;
+}
+
+// Captures one step (injection from the device time, H, J clear, particles,
+// E, t += dt on the device) as a graph.  False when the capture or the
+// instantiation failed (nothing is left pending: the caller steps eagerly).
+static bool capture_step(pdp3g_ctx *ctx) {
+  if (ctx->step_exec) cudaGraphExecDestroy(ctx->step_exec);
+  ctx->step_exec = nullptr;
+  const int64_t l0 = ctx->launches, p0 = ctx->particle_launches;
+  cudaStream_t st = ctx->stream;
+  if (cudaStreamBeginCapture(st, cudaStreamCaptureModeThreadLocal) != cudaSuccess) {
+    cudaGetLastError();
+    return false;
+  }
+  phase_inject_dev(ctx);
+  phase_calc_h(ctx);
+  cudaError_t e = phase_reset_j(ctx);
+  if (e == cudaSuccess) e = phase_particles(ctx);
+  if (e == cudaSuccess) {
+    phase_calc_e(ctx);
+    launch_advance_time(ctx->d_time, ctx->cfg.dt, st);
+    ctx->launches++;
+  }
+  cudaGraph_t graph = nullptr;
+  const cudaError_t ee = cudaStreamEndCapture(st, &graph);
+  ctx->graph_launches = ctx->launches - l0;
+  ctx->graph_particle_launches = ctx->particle_launches - p0;
+  ctx->launches = l0;
+  ctx->particle_launches = p0;
+  bool ok = e == cudaSuccess && ee == cudaSuccess && graph != nullptr &&
+            cudaGraphInstantiate(&ctx->step_exec, graph, 0) == cudaSuccess;
+  if (graph) cudaGraphDestroy(graph);
+  if (!ok) {
+    ctx->step_exec = nullptr;
+    cudaGetLastError();
+    return false;
+  }
+  ctx->graph_nsp = ctx->species.size();
+  ctx->graph_bpsm = ctx->f32_blocks_per_sm;
+  return true;
+}
+
 pdp3g_status pdp3g_step(pdp3g_ctx *ctx, int32_t nsteps) {
   if (!ctx || nsteps < 0) return PDP3G_INVALID_ARG;
   CK(cudaSetDevice(ctx->device));
   cudaStream_t st = ctx->stream;
+  // without timing: one graph launch per step (the launches of a step are
+  // too short on small grids for the host to keep the GPU busy one by one)
+  bool graph = !ctx->timing && !ctx->graph_off && nsteps > 0;
+  if (graph && (!ctx->step_exec || ctx->graph_nsp != ctx->species.size() ||
+                ctx->graph_bpsm != ctx->f32_blocks_per_sm)) {
+    if (!capture_step(ctx)) {
+      ctx->graph_off = true;
+      graph = false;
+    }
+  }
+  if (graph) {
+    launch_set_time(ctx->d_time, ctx->t, st);
+    ctx->launches++;
+  }
   for (int s = 0; s < nsteps; s++) {
-    StepEvents *ev = ctx->timing ? next_events(ctx) : nullptr;
-    if (ev) cudaEventRecord(ev->ev[0], st);
-    phase_inject(ctx);
-    if (ev) cudaEventRecord(ev->ev[1], st);
-    phase_calc_h(ctx);
-    if (ev) cudaEventRecord(ev->ev[2], st);
-    CK(phase_reset_j(ctx));
-    if (ev) cudaEventRecord(ev->ev[3], st);
-    if (ctx->cfg.sort_interval > 0 && ctx->steps % ctx->cfg.sort_interval == 0) {
-      pdp3g_status ss = sort_all(ctx);
-      if (ss != PDP3G_OK) return ss;
+    const bool sort_step =
+        ctx->cfg.sort_interval > 0 && ctx->steps % ctx->cfg.sort_interval == 0;
+    if (!graph || sort_step) {
+      pdp3g_status es = step_eager(ctx);
+      if (es != PDP3G_OK) return es;
+      if (graph) {
+        launch_set_time(ctx->d_time, ctx->t, st);  // the eager step advanced the host's t
+        ctx->launches++;
+      }
+      continue;
     }
-    if (ev) cudaEventRecord(ev->ev[4], st);
-    CK(phase_particles(ctx));
-    if (ev) cudaEventRecord(ev->ev[5], st);
-    phase_calc_e(ctx);
-    if (ev) cudaEventRecord(ev->ev[6], st);
-    phase_advance(ctx);
-    if (ctx->timing && ctx->events_used >= 4096) {
-      pdp3g_status hs = harvest_timing(ctx);
-      if (hs != PDP3G_OK) return hs;
-    }
+    CK(cudaGraphLaunch(ctx->step_exec, st));
+    ctx->t = ctx->t + ctx->cfg.dt;  // the device did the same addition
+    ctx->steps++;
+    ctx->launches += ctx->graph_launches;
+    ctx->particle_launches += ctx->graph_particle_launches;
   }
   CK(cudaGetLastError());
   return PDP3G_OK;
@@ -2234,6 +2351,7 @@ struct pdp3g_adjoint {
   std::vector<std::vector<AdjSnap>> ck_parts;  // [nwin + 1][species]
   std::vector<double> ck_t;
   std::vector<int64_t> ck_steps;
+  uint8_t *active = nullptr;                   // per cell, the reverse step's k_adj_active
   float4 *cap_quads = nullptr;                 // interval x 6 x cells: E and the half-step
                                                // H per cell (GridDev::q32), FP32
   std::vector<std::vector<AdjSnap>> cap_parts; // [interval + 1][species]: states of the
@@ -2379,6 +2497,7 @@ cudaError_t adj_reverse_step(pdp3g_adjoint *a, int cap) {
   pdp3g_ctx *ctx = a->ctx;
   const size_t ncells = (size_t)(ctx->cfg.n_grid_r - 1) * (ctx->cfg.n_grid_z - 1);
   adj_launch_e(ctx->g, a->A, ctx->stream);
+  adj_launch_active(ctx->g, a->A, a->active, ctx->stream);
   const float4 *Q = a->cap_quads + (size_t)cap * 6 * ncells;
   cudaError_t e = species_fork(ctx);
   if (e != cudaSuccess) return e;
@@ -2387,7 +2506,7 @@ cudaError_t adj_reverse_step(pdp3g_adjoint *a, int cap) {
     const cudaStream_t st = species_stream(ctx, j);
     AdjSpeciesDev S = a->ls[j];
     S.st = slot_view(a, j, cap);
-    adj_launch_particles(ctx->g, Q, S, a->A, a->face_terms, a->face_h, st);
+    adj_launch_particles(ctx->g, Q, S, a->A, a->active, a->face_terms, a->face_h, st);
     if (sp.is_bunch) {
       long long start, count;
       inject_range(ctx, sp, a->cap_t[cap], start, count);
@@ -2478,6 +2597,7 @@ pdp3g_status pdp3g_adjoint_create(pdp3g_ctx *ctx, int32_t window_steps,
     for (size_t j = 0; j < nsp; j++) ACK(snap_alloc(a, ctx->species[j].f32, a->ck_parts[c][j]));
   const size_t ncells = (size_t)(nr - 1) * (nz - 1);
   ACK(aalloc(a, &a->cap_quads, (size_t)a->interval * 6 * ncells));
+  ACK(aalloc(a, &a->active, ncells));
   a->cap_parts.assign(a->interval + 1, std::vector<AdjSnap>(nsp));
   a->cap_t.assign(a->interval, 0.0);
   for (int c = 0; c <= a->interval; c++)

@@ -85,34 +85,49 @@ static void launch_f32_kernel(const GridDev &g, const SpeciesF32 &s, const Speci
 
 // Bunch::bunch_inject in the cell-local form: z = dl * random_reverse(idx, 11)
 // + dz/2 (computed in FP64 as upstream), v_z = v_beam (u_z = gamma v / c).
+__device__ __forceinline__ void inject_slot_f32(const SpeciesF32 &s, long long idx, double dl,
+                                                double half_dz, double dz, int ncz, float uz,
+                                                const double *inv_pow11) {
+  int int_vel = (int)floor((double)(unsigned)idx);
+  double ost = 0, rr = 0;
+  int order = 1;
+  while (int_vel >= 1 && order < 40) {
+    ost = int_vel % 11;
+    rr = rr + ost * inv_pow11[order];
+    int_vel = (int)((int_vel - ost) / 11);
+    order = order + 1;
+  }
+  if (idx < s.n) {
+    const double z = dl * rr + half_dz;
+    int k = (int)ceil(z / dz) - 1;
+    if (k < 0) k = 0;
+    if (k > ncz - 1) k = ncz - 1;
+    const int c = s.cell[idx];
+    const int i = c / ncz;
+    s.cell[idx] = i * ncz + k;
+    s.fz[idx] = (float)(z / dz - k);
+    s.uz[idx] = uz;
+    s.alive[idx] = 1;
+  }
+}
+
 __global__ void k_bunch_inject_f32(SpeciesF32 s, long long start, long long count, double dl,
                                    double half_dz, double dz, int ncz, float uz,
                                    const double *inv_pow11) {
   for (long long j = blockIdx.x * (long long)blockDim.x + threadIdx.x; j < count;
-       j += (long long)gridDim.x * blockDim.x) {
-    const long long idx = start + j;
-    int int_vel = (int)floor((double)(unsigned)idx);
-    double ost = 0, rr = 0;
-    int order = 1;
-    while (int_vel >= 1 && order < 40) {
-      ost = int_vel % 11;
-      rr = rr + ost * inv_pow11[order];
-      int_vel = (int)((int_vel - ost) / 11);
-      order = order + 1;
-    }
-    if (idx < s.n) {
-      const double z = dl * rr + half_dz;
-      int k = (int)ceil(z / dz) - 1;
-      if (k < 0) k = 0;
-      if (k > ncz - 1) k = ncz - 1;
-      const int c = s.cell[idx];
-      const int i = c / ncz;
-      s.cell[idx] = i * ncz + k;
-      s.fz[idx] = (float)(z / dz - k);
-      s.uz[idx] = uz;
-      s.alive[idx] = 1;
-    }
-  }
+       j += (long long)gridDim.x * blockDim.x)
+    inject_slot_f32(s, start + j, dl, half_dz, dz, ncz, uz, inv_pow11);
+}
+
+// the same with the schedule evaluated from the device time (a captured step)
+__global__ void k_bunch_inject_f32_dev(SpeciesF32 s, const double *d_t, double begin, double end,
+                                       double dt, unsigned pis, double dl, double half_dz,
+                                       double dz, int ncz, float uz, const double *inv_pow11) {
+  long long start, count;
+  if (!inject_window(*d_t, begin, end, dt, pis, (unsigned)s.n, start, count)) return;
+  for (long long j = blockIdx.x * (long long)blockDim.x + threadIdx.x; j < count;
+       j += (long long)gridDim.x * blockDim.x)
+    inject_slot_f32(s, start + j, dl, half_dz, dz, ncz, uz, inv_pow11);
 }
 
 // Particles::charge_weighting (src/particles.cpp:101-226) for the cell-local
@@ -265,6 +280,17 @@ void launch_bunch_inject_f32(const SpeciesF32 &s, long long start, long long cou
   if (blocks > 1024) blocks = 1024;
   k_bunch_inject_f32<<<(int)blocks, 256, 0, st>>>(s, start, count, dl, half_dz, dz, ncz, uz,
                                                   inv_pow11);
+}
+
+void launch_bunch_inject_f32_dev(const SpeciesF32 &s, const double *d_t, double begin,
+                                 double end, double dt, unsigned pis, double dl, double half_dz,
+                                 double dz, int ncz, float uz, const double *inv_pow11,
+                                 cudaStream_t st) {
+  if (pis == 0) return;
+  long long blocks = ((long long)pis + 255) / 256;
+  if (blocks > 1024) blocks = 1024;
+  k_bunch_inject_f32_dev<<<(int)blocks, 256, 0, st>>>(s, d_t, begin, end, dt, pis, dl, half_dz,
+                                                      dz, ncz, uz, inv_pow11);
 }
 
 void launch_charge_density_f32(const GridDev &g, const SpeciesF32 &s, double charge,

@@ -700,28 +700,48 @@ __global__ void __launch_bounds__(256) k_charge_density_f64(GridDev g, SpeciesDe
 // get z = dl * random_reverse(index, 11) + dz/2, v_z = v_beam, alive.
 // inv_pow11[o] holds pow(11., -o) computed on the host with the same libm
 // the CPU step uses.
+__device__ __forceinline__ void inject_slot(const SpeciesDev &s, long long idx, double dl,
+                                            double half_dz, double velocity,
+                                            const double *inv_pow11) {
+  // random_reverse(idx, 11), src/math/rand.cpp:40-53
+  int int_vel = (int)floor((double)(unsigned)idx);
+  double ost = 0, rr = 0;
+  int order = 1;
+  while (int_vel >= 1 && order < 40) {
+    ost = int_vel % 11;
+    rr = rr + ost * inv_pow11[order];
+    int_vel = (int)((int_vel - ost) / 11);
+    order = order + 1;
+  }
+  if (idx < s.n) {
+    s.z[idx] = dl * rr + half_dz;
+    s.vz[idx] = velocity;
+    s.alive[idx] = 1;
+  }
+}
+
 __global__ void k_bunch_inject(SpeciesDev s, long long start, long long count, double dl,
                                double half_dz, double velocity, const double *inv_pow11) {
   for (long long i = blockIdx.x * (long long)blockDim.x + threadIdx.x; i < count;
-       i += (long long)gridDim.x * blockDim.x) {
-    const long long idx = start + i;
-    // random_reverse(idx, 11), src/math/rand.cpp:40-53
-    int int_vel = (int)floor((double)(unsigned)idx);
-    double ost = 0, rr = 0;
-    int order = 1;
-    while (int_vel >= 1 && order < 40) {
-      ost = int_vel % 11;
-      rr = rr + ost * inv_pow11[order];
-      int_vel = (int)((int_vel - ost) / 11);
-      order = order + 1;
-    }
-    if (idx < s.n) {
-      s.z[idx] = dl * rr + half_dz;
-      s.vz[idx] = velocity;
-      s.alive[idx] = 1;
-    }
-  }
+       i += (long long)gridDim.x * blockDim.x)
+    inject_slot(s, start + i, dl, half_dz, velocity, inv_pow11);
 }
+
+// the same with the schedule evaluated from the device time (a captured step)
+__global__ void k_bunch_inject_dev(SpeciesDev s, const double *d_t, double begin, double end,
+                                   double dt, unsigned pis, double dl, double half_dz,
+                                   double velocity, const double *inv_pow11) {
+  long long start, count;
+  if (!inject_window(*d_t, begin, end, dt, pis, (unsigned)s.n, start, count)) return;
+  for (long long i = blockIdx.x * (long long)blockDim.x + threadIdx.x; i < count;
+       i += (long long)gridDim.x * blockDim.x)
+    inject_slot(s, start + i, dl, half_dz, velocity, inv_pow11);
+}
+
+// the device copy of the context's time (a captured step reads and advances
+// it; the host keeps its own copy with the same additions)
+__global__ void k_set_time(double *d_t, double v) { *d_t = v; }
+__global__ void k_advance_time(double *d_t, double dt) { *d_t = *d_t + dt; }
 
 void launch_push_deposit_f64(const GridDev &g, const SpeciesDev &s, int pusher, int n_sm,
                              cudaStream_t st) {
@@ -743,6 +763,22 @@ void launch_charge_density_f64(const GridDev &g, const SpeciesDev &s, double *rh
   long long blocks = (s.n + 255) / 256;
   if (blocks > 148 * 8) blocks = 148 * 8;
   k_charge_density_f64<<<(int)blocks, 256, 0, st>>>(g, s, rho);
+}
+
+void launch_bunch_inject_dev(const SpeciesDev &s, const double *d_t, double begin, double end,
+                             double dt, unsigned pis, double dl, double half_dz, double velocity,
+                             const double *inv_pow11, cudaStream_t st) {
+  if (pis == 0) return;
+  long long blocks = ((long long)pis + 255) / 256;
+  if (blocks > 1024) blocks = 1024;
+  k_bunch_inject_dev<<<(int)blocks, 256, 0, st>>>(s, d_t, begin, end, dt, pis, dl, half_dz,
+                                                  velocity, inv_pow11);
+}
+
+void launch_set_time(double *d_t, double v, cudaStream_t st) { k_set_time<<<1, 1, 0, st>>>(d_t, v); }
+
+void launch_advance_time(double *d_t, double dt, cudaStream_t st) {
+  k_advance_time<<<1, 1, 0, st>>>(d_t, dt);
 }
 
 void launch_bunch_inject(const SpeciesDev &s, long long start, long long count, double dl,

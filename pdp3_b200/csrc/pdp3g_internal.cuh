@@ -253,6 +253,18 @@ void launch_push_deposit_f32(const GridDev &g, const SpeciesF32 &s, int pusher, 
                              int blocks_per_sm, cudaStream_t st);
 void launch_push_deposit_f32_to(const GridDev &g, const SpeciesF32 &s, const SpeciesOut &o,
                                 int pusher, int n_sm, int blocks_per_sm, cudaStream_t st);
+// the step-graph forms of the injection: the schedule is evaluated on the
+// device from *d_t (inject_window); grid sized for pis slots
+void launch_bunch_inject_f32_dev(const SpeciesF32 &s, const double *d_t, double begin,
+                                 double end, double dt, unsigned pis, double dl, double half_dz,
+                                 double dz, int ncz, float uz, const double *inv_pow11,
+                                 cudaStream_t st);
+void launch_bunch_inject_dev(const SpeciesDev &s, const double *d_t, double begin, double end,
+                             double dt, unsigned pis, double dl, double half_dz, double velocity,
+                             const double *inv_pow11, cudaStream_t st);
+// *d_t = v, and *d_t = *d_t + dt (t += dt, src/loadInitParam.cpp:586)
+void launch_set_time(double *d_t, double v, cudaStream_t st);
+void launch_advance_time(double *d_t, double dt, cudaStream_t st);
 void launch_bunch_inject_f32(const SpeciesF32 &s, long long start, long long count, double dl,
                              double half_dz, double dz, int ncz, float uz,
                              const double *inv_pow11, cudaStream_t st);
@@ -329,9 +341,13 @@ void launch_mp_write(const MpArrays &arr, long long n, double dr, double dz, int
 
 void adj_launch_e(const GridDev &g, const AdjGrids &A, cudaStream_t st);
 void adj_launch_h(const GridDev &g, const AdjGrids &A, cudaStream_t st);
-// Q: the step's per-cell quads of E and the half-step H (GridDev::q32 layout)
+// per cell: 1 when an adjoint of J within reach of its particles is nonzero
+void adj_launch_active(const GridDev &g, const AdjGrids &A, uint8_t *active, cudaStream_t st);
+// Q: the step's per-cell quads of E and the half-step H (GridDev::q32
+// layout); active: adj_launch_active's flags of the step
 void adj_launch_particles(const GridDev &g, const float4 *Q, const AdjSpeciesDev &S,
-                          const AdjGrids &A, int face, float face_h, cudaStream_t st);
+                          const AdjGrids &A, const uint8_t *active, int face, float face_h,
+                          cudaStream_t st);
 void adj_launch_inject(const AdjSpeciesDev &S, long long start, long long count, double dt,
                        double dz, double velocity, const double *inv_pow11, double *lv,
                        cudaStream_t st);
@@ -339,6 +355,25 @@ void adj_launch_seed(const GridDev &g, const AdjGrids &A, int r0, int r1, int z0
                      double *loss, cudaStream_t st);
 
 #ifdef __CUDACC__
+// Bunch::bunch_inject's schedule at time t (src/bunch.cpp:87-124): the slots
+// [start, start + count) injected in the step, from the host-computed window
+// [begin, end) and particles per step.  The one operation done here,
+// (t - begin) / dt * pis, is the host's (no contraction is possible), so the
+// device schedule of a captured step equals the host's.
+__device__ __forceinline__ bool inject_window(double t, double begin, double end, double dt,
+                                              unsigned pis, unsigned number, long long &start,
+                                              long long &count) {
+  start = 0;
+  count = 0;
+  if (!(t >= begin && t < end) || pis == 0) return false;
+  const int start_number = (t - begin) / dt * pis;
+  start = (long long)(unsigned)start_number;
+  count = pis;
+  if (start >= (long long)number) count = 0;
+  else if (start + count > (long long)number) count = (long long)number - start;
+  return count > 0;
+}
+
 // L2 prefetch of [ptr, ptr + bytes) by the bulk-copy unit (bytes a multiple
 // of 16; skipped unless ptr is 16-byte aligned).  A hint: nothing waits on
 // it.  The particle kernels let one thread per CTA ask for the CTA's next

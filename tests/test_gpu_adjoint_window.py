@@ -14,7 +14,7 @@ Asserted (measured on B200 in brackets):
   * density coefficients, norm-wise over the four bumps nearest the probe:
     within 1e-3 (1.4e-4);
   * bunch radius: within 1e-3 (1.5e-4);
-  * backward / forward device time: at most 4 (3.9);
+  * backward / forward device time: at most 4 (2.7);
   * bunch gamma: within 2.5e-3 (1.5e-3).  The 1e-3 target is not met for
     gamma: FD fits over +-1% and +-2% themselves differ by 1e-3, the FP32
     adjoint's pathwise part differs from the FP64 pathwise derivative
