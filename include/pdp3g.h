@@ -149,7 +149,13 @@ pdp3g_status pdp3g_add_bunch(pdp3g_ctx *ctx, double charge_e, double mass_me, in
 /* nsteps passes of the LoadInitParam::run loop body (src/loadInitParam.cpp:
    481-527, 586): bunch injection, HField::calc_field, Current::reset_j,
    ParticlesList::step_v + full_current_distribution, EField::calc_field,
-   t += dt.  Asynchronous on the context's stream. */
+   t += dt.  Asynchronous on the context's stream.  With timing off
+   (pdp3g_set_timing) each step is one launch of a graph captured on the
+   first call (the injection schedule and t += dt evaluated on the device,
+   with the host's arithmetic), recaptured when species are added; re-sort
+   steps and timed steps launch their kernels one by one.  The context's
+   stream must not be under a caller's stream capture (the call then falls
+   back to one-by-one launches). */
 pdp3g_status pdp3g_step(pdp3g_ctx *ctx, int32_t nsteps);
 
 /* The phases of pdp3g_step, one per upstream call of the loop body, for
@@ -175,8 +181,10 @@ pdp3g_status pdp3g_set_time(pdp3g_ctx *ctx, double current_time);
 /* Stable sort of every plasma species by cell index (an integer LSD radix
    sort of (cell, index) pairs; the permutation equals a stable sort of the
    cell keys).  No upstream counterpart: upstream particles stay in creation
-   order.  Bunch species keep their slot order.  pdp3g_step also sorts every
-   cfg.sort_interval steps. */
+   order.  Bunch species keep their slot order.  pdp3g_step also sorts
+   before the particle phase of every step whose count since the context's
+   creation is a multiple of cfg.sort_interval (timing resets do not change
+   that count). */
 pdp3g_status pdp3g_sort(pdp3g_ctx *ctx);
 
 /* Waits for the stream and reports device-side error flags. */

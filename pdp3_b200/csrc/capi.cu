@@ -76,7 +76,8 @@ struct pdp3g_ctx {
   std::vector<StepEvents> step_events;
   size_t events_used = 0;
   pdp3g_timing acc{};
-  int64_t launches = 0, particle_launches = 0, steps = 0;
+  int64_t launches = 0, particle_launches = 0, steps = 0;  // since the last timing reset
+  int64_t sim_steps = 0;  // steps since creation: the re-sort schedule (not reset by timing)
   std::string last_error;
   int64_t bytes = 0;
   int f32_blocks_per_sm = 0;  // CTAs per SM for the FP32 particle kernel (0: its default)
@@ -866,6 +867,7 @@ static void phase_calc_e(pdp3g_ctx *ctx) {
 static void phase_advance(pdp3g_ctx *ctx) {
   ctx->t = ctx->t + ctx->cfg.dt;
   ctx->steps++;
+  ctx->sim_steps++;
 }
 
 // Bunch::bunch_inject of every bunch with the schedule evaluated on the
@@ -907,7 +909,7 @@ static pdp3g_status step_eager(pdp3g_ctx *ctx) {
   if (ev) cudaEventRecord(ev->ev[2], st);
   CK(phase_reset_j(ctx));
   if (ev) cudaEventRecord(ev->ev[3], st);
-  if (ctx->cfg.sort_interval > 0 && ctx->steps % ctx->cfg.sort_interval == 0) {
+  if (ctx->cfg.sort_interval > 0 && ctx->sim_steps % ctx->cfg.sort_interval == 0) {
     pdp3g_status ss = sort_all(ctx);
     if (ss != PDP3G_OK) return ss;
   }
@@ -984,7 +986,7 @@ pdp3g_status pdp3g_step(pdp3g_ctx *ctx, int32_t nsteps) {
   }
   for (int s = 0; s < nsteps; s++) {
     const bool sort_step =
-        ctx->cfg.sort_interval > 0 && ctx->steps % ctx->cfg.sort_interval == 0;
+        ctx->cfg.sort_interval > 0 && ctx->sim_steps % ctx->cfg.sort_interval == 0;
     if (!graph || sort_step) {
       pdp3g_status es = step_eager(ctx);
       if (es != PDP3G_OK) return es;
@@ -997,6 +999,7 @@ pdp3g_status pdp3g_step(pdp3g_ctx *ctx, int32_t nsteps) {
     CK(cudaGraphLaunch(ctx->step_exec, st));
     ctx->t = ctx->t + ctx->cfg.dt;  // the device did the same addition
     ctx->steps++;
+    ctx->sim_steps++;
     ctx->launches += ctx->graph_launches;
     ctx->particle_launches += ctx->graph_particle_launches;
   }
@@ -2107,6 +2110,7 @@ static pdp3g_status ens_segment_graph(pdp3g_ensemble *e, int nsteps, float *ms_o
   for (auto *c : e->runs) {
     for (int i = 0; i < launched; i++) c->t = c->t + c->cfg.dt;
     c->steps += launched;
+    c->sim_steps += launched;
   }
   e->steps_total += launched;
   *ms_out = ms;
@@ -2141,6 +2145,7 @@ static pdp3g_status ens_segment(pdp3g_ensemble *e, int nsteps, bool allow_graph,
   for (auto *c : e->runs) {
     for (int i = 0; i < status[0]; i++) c->t = c->t + c->cfg.dt;
     c->steps += status[0];
+    c->sim_steps += status[0];
   }
   e->steps_total += status[0];
   *ms_out = ms;
@@ -2414,7 +2419,7 @@ pdp3g_status adj_save_checkpoint(pdp3g_adjoint *a, int idx) {
   for (size_t j = 0; j < ctx->species.size(); j++)
     CK(snap_copy(ctx->species[j].f32, a->ck_parts[idx][j], 0, ctx->stream));
   a->ck_t[idx] = ctx->t;
-  a->ck_steps[idx] = ctx->steps;
+  a->ck_steps[idx] = ctx->sim_steps;
   return PDP3G_OK;
 }
 
@@ -2429,7 +2434,7 @@ pdp3g_status adj_restore_checkpoint(pdp3g_adjoint *a, int idx, bool particles = 
   for (size_t j = 0; particles && j < ctx->species.size(); j++)
     CK(snap_copy(ctx->species[j].f32, a->ck_parts[idx][j], 1, ctx->stream));
   ctx->t = a->ck_t[idx];
-  ctx->steps = a->ck_steps[idx];
+  ctx->sim_steps = a->ck_steps[idx];
   return PDP3G_OK;
 }
 
