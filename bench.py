@@ -574,21 +574,25 @@ def run_ensemble(args, rank, world, local_rank, dist=None):
     for s_ in sims:
         s_.step(args.warmup)
         s_.sync()
-    # each run stepped alone, one after another: device time from the first
-    # to the last launch of each run's K steps (CUDA events on its stream),
-    # summed; the sum of its kernels' own times is reported beside it
+    # each run stepped alone, one after another, as pdp3g_step runs it
+    # (one captured graph per step): device time from the first to the last
+    # launch of each run's K steps (CUDA events on its stream), summed; the
+    # sum of its kernels' own times (K more steps launched one by one with
+    # per-phase events) is reported beside it
     seq_ms = seq_kernel_ms = 0.0
     for s_ in sims:
         st_ = torch.cuda.ExternalStream(s_.stream_ptr, device=torch.device("cuda", local_rank))
         e0 = torch.cuda.Event(enable_timing=True)
         e1 = torch.cuda.Event(enable_timing=True)
-        s_.reset_timing()
-        s_.set_timing(True)
         e0.record(st_)
         s_.step(args.steps)
         e1.record(st_)
         s_.sync()
         seq_ms += e0.elapsed_time(e1)
+        s_.reset_timing()
+        s_.set_timing(True)
+        s_.step(args.steps)
+        s_.sync()
         seq_kernel_ms += s_.timing()["ms_step_total"]
         s_.set_timing(False)
     ens = api.Ensemble(sims)
@@ -667,9 +671,10 @@ def run_ensemble(args, rank, world, local_rank, dist=None):
                                       "the fastest is kept"},
             "sequential": {"value": seq_value, "ms_per_step": seq_ms_max / args.steps,
                            "kernel_ms_per_step": seq_kernel_ms / args.steps,
-                           "note": "same runs, each stepped alone with per-run launches; "
-                                   "ms_per_step spans each run's launches on its stream, "
-                                   "kernel_ms_per_step sums the kernels alone"},
+                           "note": "same runs, each stepped alone by pdp3g_step (one "
+                                   "captured graph per step); ms_per_step spans each run's "
+                                   "steps on its stream, kernel_ms_per_step sums the "
+                                   "kernels alone (steps launched one by one)"},
             "ensemble_over_sequential": value / seq_value,
             "cell_updates_per_s": nodes * world * args.steps / (ms_max / 1000.0),
             "roofline": {"bound": "hbm", "achieved": achieved, "peak": peaks.get("hbm_gbs"),
