@@ -1076,8 +1076,11 @@ def run_e2e(sim, wl, torch, stream, steps):
     bufs = []
     for sid in range(n_sp):
         n = sim.species_size(sid)
-        arrs = {k: torch.empty(n, dtype=torch.float64, pin_memory=True).numpy()
-                for k in ("r", "z", "vr", "vphi", "vz")}
+        # the five arrays of a species in one pinned block: the exchange then
+        # moves each chunk of all five with one 2-D copy per direction
+        block = torch.empty(5 * n, dtype=torch.float64, pin_memory=True).numpy()
+        arrs = {k: block[j * n:(j + 1) * n]
+                for j, k in enumerate(("r", "z", "vr", "vphi", "vz"))}
         alive = torch.empty(n, dtype=torch.uint8, pin_memory=True).numpy()
         st = sim.species(sid)
         for k in arrs:

@@ -1290,16 +1290,49 @@ pdp3g_status pdp3g_exchange_all(pdp3g_ctx *ctx, const pdp3g_exchange_item *items
       double *a[5] = {sp.dev.r, sp.dev.z, sp.dev.vr, sp.dev.vphi, sp.dev.vz};
       for (int k = 0; k < 5; k++) dev[k] = a[k];
     }
+    // five arrays at one stride on both sides (the device side only in the
+    // FP32 form, whose staging is one allocation; the host arrays when they
+    // are one block): one 2-D copy of 5 rows per chunk and direction
+    // instead of five copies.  A 2-D copy the runtime refuses (host arrays
+    // equally spaced but not one allocation) falls back to five copies.
+    const auto strided = [](const void *const p[5], ptrdiff_t &pitch) {
+      pitch = (const char *)p[1] - (const char *)p[0];
+      if (pitch <= 0 || pitch >= ((ptrdiff_t)1 << 30)) return false;  // 2-D copy pitch limit
+      for (int k = 2; k < 5; k++)
+        if ((const char *)p[k] - (const char *)p[k - 1] != pitch) return false;
+      return true;
+    };
+    ptrdiff_t p_dev = 0, p_out = 0, p_in = 0;
+    const void *pd[5] = {dev[0], dev[1], dev[2], dev[3], dev[4]};
+    const void *po[5] = {outs[0], outs[1], outs[2], outs[3], outs[4]};
+    const void *pi[5] = {ins[0], ins[1], ins[2], ins[3], ins[4]};
+    bool rows_out = sp.fp32 && strided(pd, p_dev) && strided(po, p_out);
+    bool rows_in = sp.fp32 && strided(pd, p_dev) && strided(pi, p_in);
     for (size_t c0 = 0; c0 < n; c0 += EXCHANGE_CHUNK) {
       const size_t cn = std::min(EXCHANGE_CHUNK, n - c0), b = sizeof(double) * cn;
-      for (int k = 0; k < 5; k++)
-        CK(cudaMemcpyAsync(outs[k] + c0, dev[k] + c0, b, cudaMemcpyDeviceToHost, down));
+      if (rows_out && cudaMemcpy2DAsync(outs[0] + c0, (size_t)p_out, dev[0] + c0,
+                                        (size_t)p_dev, b, 5, cudaMemcpyDeviceToHost,
+                                        down) != cudaSuccess) {
+        cudaGetLastError();  // refused before anything was queued
+        rows_out = false;
+      }
+      if (!rows_out) {
+        for (int k = 0; k < 5; k++)
+          CK(cudaMemcpyAsync(outs[k] + c0, dev[k] + c0, b, cudaMemcpyDeviceToHost, down));
+      }
       if (dev_alive && it.out_alive)
         CK(cudaMemcpyAsync(it.out_alive + c0, dev_alive + c0, cn, cudaMemcpyDeviceToHost, down));
       CK(cudaEventRecord(ctx->ev_chunk, down));
       CK(cudaStreamWaitEvent(up, ctx->ev_chunk, 0));
-      for (int k = 0; k < 5; k++)
-        CK(cudaMemcpyAsync(dev[k] + c0, ins[k] + c0, b, cudaMemcpyHostToDevice, up));
+      if (rows_in && cudaMemcpy2DAsync(dev[0] + c0, (size_t)p_dev, ins[0] + c0, (size_t)p_in,
+                                       b, 5, cudaMemcpyHostToDevice, up) != cudaSuccess) {
+        cudaGetLastError();
+        rows_in = false;
+      }
+      if (!rows_in) {
+        for (int k = 0; k < 5; k++)
+          CK(cudaMemcpyAsync(dev[k] + c0, ins[k] + c0, b, cudaMemcpyHostToDevice, up));
+      }
       if (dev_alive && it.in_alive)
         CK(cudaMemcpyAsync(dev_alive + c0, it.in_alive + c0, cn, cudaMemcpyHostToDevice, up));
     }

@@ -151,3 +151,45 @@ def test_exchange_all_equals_one_call_per_species(precision):
     a.close()
     b.close()
 
+
+@pytest.mark.parametrize("precision", ["fp64", "fp32"])
+def test_exchange_all_with_one_host_block_per_species(precision):
+    """The five host arrays of a species in one block (equally spaced): the
+    exchange moves them with 2-D copies; same result as separate arrays."""
+    wl = W.wake_config(ppc=3)
+    a = api.from_workload(wl, precision=precision)
+    a.step(2)
+    a.sync()
+    n_sp = 3
+    before = [a.species(sid) for sid in range(n_sp)]
+    blocks, bufs = [], []
+    for sid in range(n_sp):
+        n = before[sid]["r"].size
+        blk = pinned(np.zeros(5 * n))
+        d = {k: blk[j * n:(j + 1) * n] for j, k in enumerate(KEYS)}
+        for k in KEYS:
+            d[k][:] = before[sid][k]
+        d["alive"] = pinned(before[sid]["alive"])
+        blocks.append(blk)
+        bufs.append(d)
+    inp = [{k: (pinned(before[sid][k] * (0.5 if k == "vz" else 1.0)) if k != "alive"
+                else pinned(before[sid]["alive"])) for k in KEYS + ("alive",)}
+           for sid in range(n_sp)]
+    # out into the blocks, in from separate arrays
+    a.exchange_all([(sid, bufs[sid], inp[sid]) for sid in range(n_sp)])
+    for sid in range(n_sp):
+        for k in KEYS:
+            assert np.array_equal(bufs[sid][k], before[sid][k]), (sid, k)
+    loaded = [a.species(sid) for sid in range(n_sp)]
+    # in from the blocks (now holding the previous state), out to separate arrays
+    outs = [{k: pinned(np.zeros(before[sid]["r"].size)) for k in KEYS} for sid in range(n_sp)]
+    a.exchange_all([(sid, outs[sid], bufs[sid]) for sid in range(n_sp)])
+    for sid in range(n_sp):
+        for k in KEYS:
+            assert np.array_equal(outs[sid][k], loaded[sid][k]), (sid, k)
+        now = a.species(sid)
+        if precision == "fp64":
+            for k in KEYS:
+                assert np.array_equal(now[k], before[sid][k]), (sid, k)
+    a.close()
+
