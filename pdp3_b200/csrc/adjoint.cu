@@ -244,10 +244,15 @@ __global__ void __launch_bounds__(ADJ_THREADS, ADJ_MIN_BLOCKS) k_adj_particles(
     const int c = live ? S.st.cell[p] : 0;
     if (c < 0 || c >= (g.nr - 1) * ncz) live = false;  // flagged by the forward step
     // zero adjoints of the particle and none of J within its reach (k_adj_active):
-    // every output of its reverse is zero, nothing to do
-    if (live && S.la[p] == 0.0f && S.lb[p] == 0.0f && S.lur[p] == 0.0f && S.luphi[p] == 0.0f &&
-        S.luz[p] == 0.0f && !active[c])
-      live = false;
+    // every output of its reverse is zero, nothing to do.  The five loads are
+    // issued together and tested bitwise (a sign-only -0.0f counts as
+    // nonzero, which only costs a reverse that adds zeros).
+    if (live) {
+      const unsigned bits = __float_as_uint(S.la[p]) | __float_as_uint(S.lb[p]) |
+                            __float_as_uint(S.lur[p]) | __float_as_uint(S.luphi[p]) |
+                            __float_as_uint(S.luz[p]);
+      if (bits == 0u && !active[c]) live = false;
+    }
     if (__all_sync(0xffffffffu, !live)) continue;  // the whole warp: no sums to add either
     const int ci = c / ncz, ck = c - (c / ncz) * ncz;
     float lf[24];  // this lane's field-node adjoints, reduced across the warp
