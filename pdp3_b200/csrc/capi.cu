@@ -731,6 +731,20 @@ pdp3g_status pdp3g_sort(pdp3g_ctx *ctx) {
 
 // ---- the step's phases (LoadInitParam::run, src/loadInitParam.cpp:481-527, 586)
 
+// the window of a bunch's injection (src/bunch.cpp:87-124): slots are
+// injected while begin <= t < end, particles_in_step of them per step; one
+// computation for the host schedule below and the device one of a captured
+// step (phase_inject_dev)
+static void inject_window_of(const pdp3g_ctx *ctx, const Species &sp, double &begin, double &end,
+                             unsigned int &number, unsigned int &particles_in_step) {
+  const double dt = ctx->cfg.dt;
+  begin = sp.duration * sp.bunch_number + sp.hole_duration * sp.bunch_number;
+  end = begin + sp.duration;
+  const int steps_amount = (int)std::ceil(sp.duration / dt);
+  number = (unsigned int)(sp.fp32 ? sp.f32.n : sp.dev.n);
+  particles_in_step = steps_amount > 0 ? number / steps_amount : 0;
+}
+
 // Bunch::bunch_inject's schedule (src/bunch.cpp:87-124): the slots
 // [start, start + count) that the bunch injects at time t (count 0: none)
 static void inject_range(const pdp3g_ctx *ctx, const Species &sp, double t, long long &start,
@@ -738,11 +752,9 @@ static void inject_range(const pdp3g_ctx *ctx, const Species &sp, double t, long
   start = 0;
   count = 0;
   const double dt = ctx->cfg.dt;
-  double begin = sp.duration * sp.bunch_number + sp.hole_duration * sp.bunch_number;
-  double end = begin + sp.duration;
-  int steps_amount = (int)std::ceil(sp.duration / dt);
-  unsigned int number = (unsigned int)(sp.fp32 ? sp.f32.n : sp.dev.n);
-  unsigned int particles_in_step = number / steps_amount;
+  double begin, end;
+  unsigned int number, particles_in_step;
+  inject_window_of(ctx, sp, begin, end, number, particles_in_step);
   int start_number = (t - begin) / dt * particles_in_step;
   if (t >= begin && t < end && particles_in_step > 0) {
     // indices start_number + i for i < particles_in_step, kept below number
@@ -877,11 +889,9 @@ static void phase_inject_dev(pdp3g_ctx *ctx) {
   const double dt = ctx->cfg.dt;
   for (auto &sp : ctx->species) {
     if (!sp.is_bunch) continue;
-    const double begin = sp.duration * sp.bunch_number + sp.hole_duration * sp.bunch_number;
-    const double end = begin + sp.duration;
-    const int steps_amount = (int)std::ceil(sp.duration / dt);
-    const unsigned number = (unsigned)(sp.fp32 ? sp.f32.n : sp.dev.n);
-    const unsigned pis = steps_amount > 0 ? number / steps_amount : 0;
+    double begin, end;
+    unsigned number, pis;
+    inject_window_of(ctx, sp, begin, end, number, pis);
     const double dl = sp.velocity * dt;
     if (sp.fp32) {
       const double b2 = sp.velocity * sp.velocity / LIGHT_SPEED_POW_2;
