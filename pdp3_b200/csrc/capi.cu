@@ -701,10 +701,14 @@ int64_t pdp3g_species_size(pdp3g_ctx *ctx, int32_t id) {
 // slot order, which the injection schedule indexes)
 static pdp3g_status sort_all(pdp3g_ctx *ctx) {
   long long nmax = 0;
-  for (auto &sp : ctx->species)
-    if (!sp.is_bunch) nmax = std::max<long long>(nmax, sp.fp32 ? sp.f32.n : sp.dev.n);
+  size_t need = 0;
+  for (auto &sp : ctx->species) {
+    if (sp.is_bunch) continue;
+    const long long n = sp.fp32 ? sp.f32.n : sp.dev.n;
+    nmax = std::max<long long>(nmax, n);
+    need = std::max(need, sort_layout(n, sp.fp32 ? SORT_STATE_F32 : SORT_STATE_F64).total);
+  }
   if (nmax <= 1) return PDP3G_OK;
-  const size_t need = sort_layout(nmax).total;
   if (ctx->sort_bytes < need) {
     cudaFree(ctx->d_sort);
     ctx->d_sort = nullptr;

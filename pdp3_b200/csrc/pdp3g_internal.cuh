@@ -231,11 +231,12 @@ struct SortLayout {
   long long nsub, m, nb;
   size_t keys_a, keys_b, idx_a, idx_b, H, bs, tmp, total;
 };
-SortLayout sort_layout(long long n);
+// state bytes per particle that the gather stages (FP64: r, z, vr, vphi,
+// vz, w; FP32: cell, fr, fz, ur, uphi, uz, w)
+constexpr size_t SORT_STATE_F64 = 6 * 8, SORT_STATE_F32 = 7 * 4;
+SortLayout sort_layout(long long n, size_t state_bytes);
 int sort_species_f64(const GridDev &g, SpeciesDev &s, char *scratch, cudaStream_t st);
 int sort_species_f32(const GridDev &g, SpeciesF32 &s, char *scratch, cudaStream_t st);
-int sort_keys(const unsigned *keys, long long n, int key_bits, char *scratch,
-              unsigned *perm_out, cudaStream_t st);
 
 // host-side launchers (fields.cu, particles_f64.cu, particles_f32.cu, diag.cu)
 void launch_to_f32(const double *src, float *dst, size_t n, cudaStream_t st);

@@ -12,7 +12,8 @@
 // the keys (numpy.argsort(kind="stable")).
 //
 // Traffic per pass: read key+index (8 B), write key+index (8 B) per particle,
-// plus the count table; the gather reads and writes the particle state once.
+// plus the count table; the gather reads the permutation once, reads the
+// particle state in sorted order into scratch copies and copies them back.
 #include "pdp3g_internal.cuh"
 
 namespace pdp3g {
@@ -22,7 +23,15 @@ constexpr int SORT_THREADS = SORT_WARPS * 32;
 constexpr int SUB = 2048;                     // items per warp sub-range
 constexpr int RADIX = 256;
 
-// H[d * nsub + s] = number of items with digit d in sub-range s
+// Each warp loads BATCH 32-item steps of its sub-range before it ranks them,
+// so that BATCH loads per lane are in flight instead of one.
+constexpr int BATCH = 8;
+static_assert(SUB % (32 * BATCH) == 0, "a sub-range is whole batches");
+
+// H[d * nsub + s] = number of items with digit d in sub-range s.  Lanes with
+// the same digit are counted by the group's lowest lane (the cell keys of a
+// sorted or nearly sorted species give a whole warp one digit, which shared
+// memory atomics would serialise 32-fold).
 __global__ void __launch_bounds__(SORT_THREADS) k_digit_count(const unsigned *keys, long long n,
                                                               int shift, int nsub,
                                                               unsigned *H) {
@@ -34,9 +43,21 @@ __global__ void __launch_bounds__(SORT_THREADS) k_digit_count(const unsigned *ke
   if (sub < nsub) {
     const long long begin = sub * SUB;
     const long long end = begin + SUB < n ? begin + SUB : n;
-    for (long long p = begin + lane; p < end; p += 32)
-      atomicAdd(&cnt[warp][(keys[p] >> shift) & (RADIX - 1)], 1u);
-    __syncwarp();
+    const unsigned below = (1u << lane) - 1u;
+    for (long long p0 = begin; p0 < end; p0 += 32 * BATCH) {
+      unsigned d[BATCH];
+#pragma unroll
+      for (int j = 0; j < BATCH; j++) {
+        const long long p = p0 + j * 32 + lane;
+        d[j] = p < end ? (keys[p] >> shift) & (RADIX - 1) : RADIX;
+      }
+#pragma unroll
+      for (int j = 0; j < BATCH; j++) {
+        const unsigned peers = __match_any_sync(0xffffffffu, d[j]);
+        if (d[j] < RADIX && (peers & below) == 0u) cnt[warp][d[j]] += __popc(peers);
+        __syncwarp();
+      }
+    }
     for (int d = lane; d < RADIX; d += 32) H[(size_t)d * nsub + sub] = cnt[warp][d];
   }
 }
@@ -143,29 +164,35 @@ __global__ void __launch_bounds__(SORT_THREADS) k_digit_scatter(
   __syncwarp();
   const long long begin = sub * SUB;
   const long long end = begin + SUB < n ? begin + SUB : n;
-  const unsigned lt = (1u << lane) - 1u;
-  for (long long p0 = begin; p0 < end; p0 += 32) {
-    const long long p = p0 + lane;
-    const bool valid = p < end;
-    const unsigned active = __ballot_sync(0xffffffffu, valid);
-    unsigned key = 0, id = 0, d = RADIX;  // invalid lanes use a digit no valid lane has
-    if (valid) {
-      key = keys_in[p];
-      id = idx_in ? idx_in[p] : (unsigned)p;
-      d = (key >> shift) & (RADIX - 1);
+  const unsigned below = (1u << lane) - 1u;
+  for (long long p0 = begin; p0 < end; p0 += 32 * BATCH) {
+    unsigned key[BATCH], id[BATCH];
+#pragma unroll
+    for (int j = 0; j < BATCH; j++) {
+      const long long p = p0 + j * 32 + lane;
+      key[j] = 0;
+      id[j] = (unsigned)p;
+      if (p < end) {
+        key[j] = keys_in[p];
+        if (idx_in) id[j] = idx_in[p];
+      }
     }
-    const unsigned peers = __match_any_sync(0xffffffffu, d);
-    if (valid) {
-      const unsigned rank = __popc(peers & lt);
-      const unsigned pos = run[warp][d] + rank;
-      keys_out[pos] = key;
-      idx_out[pos] = id;
+    // the batch's steps in item order: ranks and runs as one step at a time
+#pragma unroll
+    for (int j = 0; j < BATCH; j++) {
+      const bool valid = p0 + j * 32 + lane < end;
+      const unsigned d = valid ? (key[j] >> shift) & (RADIX - 1) : RADIX;  // RADIX: no valid lane
+      const unsigned peers = __match_any_sync(0xffffffffu, d);
+      if (valid) {
+        const unsigned pos = run[warp][d] + __popc(peers & below);
+        keys_out[pos] = key[j];
+        idx_out[pos] = id[j];
+      }
+      __syncwarp();
+      // the highest lane of each digit group advances that digit's run
+      if (valid && (peers >> lane) == 1u) run[warp][d] += __popc(peers);
+      __syncwarp();
     }
-    __syncwarp();
-    // the highest lane of each digit group advances that digit's run
-    if (valid && (peers >> lane) == 1u) run[warp][d] += __popc(peers);
-    __syncwarp();
-    (void)active;
   }
 }
 
@@ -194,11 +221,33 @@ __global__ void k_gather(const T *src, const unsigned *perm, long long n, T *dst
     dst[p] = src[perm[p]];
 }
 
+// NA state arrays of one element type, gathered through one read of the
+// permutation: dst.a[j][p] = src.a[j][perm[p]]
+template <typename T, int NA>
+struct ArraySet {
+  T *a[NA];
+};
+
+template <typename T, int NA>
+__global__ void __launch_bounds__(256) k_gather_set(ArraySet<T, NA> src,
+                                                    const unsigned *__restrict__ perm,
+                                                    long long n, ArraySet<T, NA> dst) {
+  for (long long p = blockIdx.x * (long long)blockDim.x + threadIdx.x; p < n;
+       p += (long long)gridDim.x * blockDim.x) {
+    const unsigned q = perm[p];
+    T v[NA];
+#pragma unroll
+    for (int j = 0; j < NA; j++) v[j] = src.a[j][q];
+#pragma unroll
+    for (int j = 0; j < NA; j++) dst.a[j][p] = v[j];
+  }
+}
+
 // ---------------------------------------------------------------- host side
 
 static size_t align256(size_t x) { return (x + 255) & ~(size_t)255; }
 
-SortLayout sort_layout(long long n) {
+SortLayout sort_layout(long long n, size_t state_bytes) {
   SortLayout L;
   const long long nsub = (n + SUB - 1) / SUB;
   L.nsub = nsub;
@@ -211,7 +260,7 @@ SortLayout sort_layout(long long n) {
   L.idx_b = off;  off = align256(off + sizeof(unsigned) * (size_t)n);
   L.H = off;      off = align256(off + sizeof(unsigned) * (size_t)L.m);
   L.bs = off;     off = align256(off + sizeof(unsigned) * (size_t)L.nb);
-  L.tmp = off;    off = align256(off + 8 * (size_t)n);
+  L.tmp = off;    off = align256(off + state_bytes * (size_t)n);
   L.total = off;
   return L;
 }
@@ -254,66 +303,58 @@ static const unsigned *radix_sort(char *scratch, const SortLayout &L, long long 
   return iin;
 }
 
-template <typename T>
-static void permute(T *arr, const unsigned *perm, long long n, void *tmp, cudaStream_t st,
-                    int *nl) {
-  T *t = (T *)tmp;
-  k_gather<T><<<grid_for(n, 256), 256, 0, st>>>(arr, perm, n, t);
-  cudaMemcpyAsync(arr, t, sizeof(T) * (size_t)n, cudaMemcpyDeviceToDevice, st);
+// the sorted order of NA arrays: gathered into the scratch copies through
+// one read of the permutation, then copied back in place
+template <typename T, int NA>
+static void permute_set(T *const (&arr)[NA], const unsigned *perm, long long n, char *tmp,
+                        cudaStream_t st, int *nl) {
+  ArraySet<T, NA> src, dst;
+  for (int j = 0; j < NA; j++) {
+    src.a[j] = arr[j];
+    dst.a[j] = (T *)tmp + (size_t)j * n;
+  }
+  k_gather_set<T, NA><<<grid_for(n, 256), 256, 0, st>>>(src, perm, n, dst);
+  *nl += 1;
+  for (int j = 0; j < NA; j++)
+    cudaMemcpyAsync(arr[j], dst.a[j], sizeof(T) * (size_t)n, cudaMemcpyDeviceToDevice, st);
+}
+
+static void permute_alive(uint8_t *alive, const unsigned *perm, long long n, char *tmp,
+                          cudaStream_t st, int *nl) {
+  k_gather<uint8_t><<<grid_for(n, 256), 256, 0, st>>>(alive, perm, n, (uint8_t *)tmp);
+  cudaMemcpyAsync(alive, tmp, (size_t)n, cudaMemcpyDeviceToDevice, st);
   *nl += 1;
 }
 
 int sort_species_f64(const GridDev &g, SpeciesDev &s, char *scratch, cudaStream_t st) {
   const long long n = s.n;
   if (n <= 1) return 0;
-  const SortLayout L = sort_layout(n);
+  const SortLayout L = sort_layout(n, SORT_STATE_F64);
   int nl = 1;
   k_keys_f64<<<grid_for(n, 256), 256, 0, st>>>(s, g.dr, g.dz, g.nr, g.nz,
                                                 (unsigned *)(scratch + L.keys_a));
   const int bits = key_bits_for((long long)(g.nr - 1) * (g.nz - 1));
   const unsigned *perm = radix_sort(scratch, L, n, bits, st, &nl);
-  void *tmp = scratch + L.tmp;
-  permute(s.r, perm, n, tmp, st, &nl);
-  permute(s.z, perm, n, tmp, st, &nl);
-  permute(s.vr, perm, n, tmp, st, &nl);
-  permute(s.vphi, perm, n, tmp, st, &nl);
-  permute(s.vz, perm, n, tmp, st, &nl);
-  permute((double *)s.w, perm, n, tmp, st, &nl);
-  if (s.alive) permute(s.alive, perm, n, tmp, st, &nl);
+  double *const arrays[6] = {s.r, s.z, s.vr, s.vphi, s.vz, (double *)s.w};
+  permute_set(arrays, perm, n, scratch + L.tmp, st, &nl);
+  if (s.alive) permute_alive(s.alive, perm, n, scratch + L.tmp, st, &nl);
   return nl;
 }
 
 int sort_species_f32(const GridDev &g, SpeciesF32 &s, char *scratch, cudaStream_t st) {
   const long long n = s.n;
   if (n <= 1) return 0;
-  const SortLayout L = sort_layout(n);
+  const SortLayout L = sort_layout(n, SORT_STATE_F32);
   int nl = 1;
   k_keys_f32<<<grid_for(n, 256), 256, 0, st>>>(s, (unsigned *)(scratch + L.keys_a));
   const int bits = key_bits_for((long long)(g.nr - 1) * (g.nz - 1));
   const unsigned *perm = radix_sort(scratch, L, n, bits, st, &nl);
-  void *tmp = scratch + L.tmp;
-  permute(s.cell, perm, n, tmp, st, &nl);
-  permute(s.fr, perm, n, tmp, st, &nl);
-  permute(s.fz, perm, n, tmp, st, &nl);
-  permute(s.ur, perm, n, tmp, st, &nl);
-  permute(s.uphi, perm, n, tmp, st, &nl);
-  permute(s.uz, perm, n, tmp, st, &nl);
-  permute((float *)s.w, perm, n, tmp, st, &nl);
-  if (s.alive) permute(s.alive, perm, n, tmp, st, &nl);
-  return nl;
-}
-
-// Sorts keys (device, n entries) and writes the stable permutation into
-// perm_out (device); scratch must hold sort_layout(n).total bytes.  Used by
-// the sort test entry point.
-int sort_keys(const unsigned *keys, long long n, int key_bits, char *scratch,
-              unsigned *perm_out, cudaStream_t st) {
-  const SortLayout L = sort_layout(n);
-  int nl = 0;
-  cudaMemcpyAsync(scratch + L.keys_a, keys, sizeof(unsigned) * (size_t)n,
-                  cudaMemcpyDeviceToDevice, st);
-  const unsigned *perm = radix_sort(scratch, L, n, key_bits, st, &nl);
-  cudaMemcpyAsync(perm_out, perm, sizeof(unsigned) * (size_t)n, cudaMemcpyDeviceToDevice, st);
+  // the cell index and the FP32 values move as 32-bit words
+  unsigned *const arrays[7] = {(unsigned *)s.cell, (unsigned *)s.fr,   (unsigned *)s.fz,
+                               (unsigned *)s.ur,   (unsigned *)s.uphi, (unsigned *)s.uz,
+                               (unsigned *)s.w};
+  permute_set(arrays, perm, n, scratch + L.tmp, st, &nl);
+  if (s.alive) permute_alive(s.alive, perm, n, scratch + L.tmp, st, &nl);
   return nl;
 }
 

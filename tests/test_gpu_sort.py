@@ -47,6 +47,29 @@ def test_sort_is_the_stable_argsort(precision):
             assert np.array_equal(a[name], b[name][perm]), (precision, sid, name)
 
 
+@pytest.mark.parametrize("n", [2, 33, 257, 2049, 10007, 70001])
+def test_sort_of_ragged_counts(n):
+    """Counts that end inside a 32-item step, a load batch and a warp's
+    sub-range: the last items of the tail must land like the rest."""
+    wl = shuffled_workload(17, ppc=8)
+    for s in wl.species:
+        for name in ("r", "z", "vr", "vphi", "vz", "w"):
+            setattr(s, name, getattr(s, name)[:n].copy())
+    for precision in ("fp64", "fp32"):
+        sim = api.from_workload(wl, precision=precision)
+        before = [sim.species(s) for s in range(2)]
+        sim.sort()
+        sim.sync()
+        for sid in range(2):
+            b = before[sid]
+            assert b["r"].size == n
+            perm = np.argsort(cell_keys(b["r"], b["z"], wl), kind="stable")
+            a = sim.species(sid)
+            for name in ("r", "z", "vr", "vphi", "vz", "w"):
+                assert np.array_equal(a[name], b[name][perm]), (precision, n, sid, name)
+        sim.close()
+
+
 def test_sort_on_large_key_range_and_many_particles():
     """256 x 2048 cells (19-bit keys, three digit passes), 8 ppc, random order."""
     wl = W.wake_config(ppc=8)
