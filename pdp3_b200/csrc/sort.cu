@@ -28,10 +28,8 @@ constexpr int RADIX = 256;
 constexpr int BATCH = 8;
 static_assert(SUB % (32 * BATCH) == 0, "a sub-range is whole batches");
 
-// H[d * nsub + s] = number of items with digit d in sub-range s.  Lanes with
-// the same digit are counted by the group's lowest lane (the cell keys of a
-// sorted or nearly sorted species give a whole warp one digit, which shared
-// memory atomics would serialise 32-fold).
+// H[d * nsub + s] = number of items with digit d in sub-range s (shared
+// memory atomics: the count does not depend on their order).
 __global__ void __launch_bounds__(SORT_THREADS) k_digit_count(const unsigned *keys, long long n,
                                                               int shift, int nsub,
                                                               unsigned *H) {
@@ -43,7 +41,6 @@ __global__ void __launch_bounds__(SORT_THREADS) k_digit_count(const unsigned *ke
   if (sub < nsub) {
     const long long begin = sub * SUB;
     const long long end = begin + SUB < n ? begin + SUB : n;
-    const unsigned below = (1u << lane) - 1u;
     for (long long p0 = begin; p0 < end; p0 += 32 * BATCH) {
       unsigned d[BATCH];
 #pragma unroll
@@ -52,12 +49,10 @@ __global__ void __launch_bounds__(SORT_THREADS) k_digit_count(const unsigned *ke
         d[j] = p < end ? (keys[p] >> shift) & (RADIX - 1) : RADIX;
       }
 #pragma unroll
-      for (int j = 0; j < BATCH; j++) {
-        const unsigned peers = __match_any_sync(0xffffffffu, d[j]);
-        if (d[j] < RADIX && (peers & below) == 0u) cnt[warp][d[j]] += __popc(peers);
-        __syncwarp();
-      }
+      for (int j = 0; j < BATCH; j++)
+        if (d[j] < RADIX) atomicAdd(&cnt[warp][d[j]], 1u);
     }
+    __syncwarp();
     for (int d = lane; d < RADIX; d += 32) H[(size_t)d * nsub + sub] = cnt[warp][d];
   }
 }

@@ -70,6 +70,37 @@ def test_sort_of_ragged_counts(n):
         sim.close()
 
 
+@pytest.mark.parametrize("nodes", [(9, 17), (1025, 8193)])
+def test_sort_with_one_and_three_digit_passes(nodes):
+    """Key ranges of one 8-bit digit pass (8 x 16 cells, 7-bit keys) and of
+    three (1024 x 8192 cells, 23-bit keys); the thermal grid of the other
+    tests takes two, the wake and large grids three."""
+    nr, nz = nodes
+    if nr == 9:
+        wl = W.small_config(n_grid_r=nr, n_grid_z=nz, ppc=8)
+    else:
+        wl = W.small_config(n_grid_r=nr, n_grid_z=nz, r_size=0.1, z_size=0.8, ppc=1)
+    rng = np.random.default_rng(19)
+    for s in wl.species:
+        p = rng.permutation(s.n)[:300000]  # a random subset in random order
+        for name in ("r", "z", "vr", "vphi", "vz", "w"):
+            setattr(s, name, getattr(s, name)[p].copy())
+    for precision in ("fp64", "fp32"):
+        sim = api.from_workload(wl, precision=precision)
+        before = [sim.species(s) for s in range(2)]
+        sim.sort()
+        sim.sync()
+        for sid in range(2):
+            b = before[sid]
+            keys = cell_keys(b["r"], b["z"], wl)
+            assert keys.max() >= (nr - 1) * (nz - 1) // 2  # the upper digits are exercised
+            perm = np.argsort(keys, kind="stable")
+            a = sim.species(sid)
+            for name in ("r", "z", "vr", "vphi", "vz", "w"):
+                assert np.array_equal(a[name], b[name][perm]), (precision, nodes, sid, name)
+        sim.close()
+
+
 def test_sort_on_large_key_range_and_many_particles():
     """256 x 2048 cells (19-bit keys, three digit passes), 8 ppc, random order."""
     wl = W.wake_config(ppc=8)
