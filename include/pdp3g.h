@@ -184,7 +184,10 @@ pdp3g_status pdp3g_set_time(pdp3g_ctx *ctx, double current_time);
    order.  Bunch species keep their slot order.  pdp3g_step also sorts
    before the particle phase of every step whose count since the context's
    creation is a multiple of cfg.sort_interval (timing resets do not change
-   that count). */
+   that count).  The first sort allocates the context's sort scratch, kept
+   until pdp3g_destroy: for the largest plasma species, 16 B per particle
+   for keys and indices plus a staging copy of its state (28 B per particle
+   in the FP32 form, 48 B in the FP64 form). */
 pdp3g_status pdp3g_sort(pdp3g_ctx *ctx);
 
 /* Waits for the stream and reports device-side error flags. */
