@@ -385,6 +385,10 @@ __device__ __forceinline__ void f32_warp_chunk(const GridDev &g, const SpeciesF3
   const long long base = wchunk * F32_WARP_CHUNK;
   if (base >= s.n) return;
   const bool has_alive = s.alive != nullptr;
+  // cells per radial row a power of two (every benchmarked grid): the cell
+  // index splits into (i, k) by a shift and a mask
+  const bool row_pow2 = (ncz & (ncz - 1)) == 0;
+  const int row_shift = __ffs(ncz) - 1;
   stage_in(ws.cell, s.cell, base, s.n, lane);
   stage_in(ws.fr, s.fr, base, s.n, lane);
   stage_in(ws.fz, s.fz, base, s.n, lane);
@@ -416,10 +420,12 @@ __device__ __forceinline__ void f32_warp_chunk(const GridDev &g, const SpeciesF3
       flag32(g, ERR_OUT_OF_GRID);
       live = false;
     }
-    // c / ncz through the FP32 reciprocal (exact for c < 2^24), corrected to
-    // the exact quotient
+    // otherwise c / ncz through the FP32 reciprocal (exact for c < 2^24),
+    // corrected to the exact quotient
     int i;
-    if (c < (1 << 24)) {
+    if (row_pow2) {
+      i = c >> row_shift;
+    } else if (c < (1 << 24)) {
       i = (int)((float)c * (1.0f / (float)ncz));
       if (i * ncz > c) i--;
       if ((i + 1) * ncz <= c) i++;

@@ -20,8 +20,11 @@ from pdp3_b200 import workloads as W
 pytestmark = pytest.mark.gpu
 
 
-def test_fp32_one_step_small_vs_oracle():
-    wl = W.small_config(beam=True, steps=1)
+@pytest.mark.parametrize("n_grid_z", [33, 41])
+def test_fp32_one_step_small_vs_oracle(n_grid_z):
+    """32 cells per radial row (the cell index splits by a shift) and 40
+    (by a division)."""
+    wl = W.small_config(beam=True, steps=1, n_grid_z=n_grid_z, z_size=0.04 * (n_grid_z - 1) / 32)
     orc = oracle_from_workload(wl)
     gpu = api.from_workload(wl, precision="fp32")
     seed_fields([orc, gpu], (wl.n_grid_r, wl.n_grid_z), seed=3)
