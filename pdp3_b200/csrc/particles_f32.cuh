@@ -389,14 +389,21 @@ __device__ __forceinline__ void f32_warp_chunk(const GridDev &g, const SpeciesF3
   // index splits into (i, k) by a shift and a mask
   const bool row_pow2 = (ncz & (ncz - 1)) == 0;
   const int row_shift = __ffs(ncz) - 1;
-  stage_in(ws.cell, s.cell, base, s.n, lane);
-  stage_in(ws.fr, s.fr, base, s.n, lane);
-  stage_in(ws.fz, s.fz, base, s.n, lane);
-  stage_in(ws.ur, s.ur, base, s.n, lane);
-  stage_in(ws.uphi, s.uphi, base, s.n, lane);
-  stage_in(ws.uz, s.uz, base, s.n, lane);
-  stage_in(ws.w, s.w, base, s.n, lane);
-  if (has_alive) {
+  // OUT: the chunk is staged in shared memory and written out whole (slots
+  // of skipped particles carry their input over); in place: each particle
+  // is read and written where it lies (a lane's four consecutive particles
+  // share 16-byte segments, which L1 keeps between the lane's four passes)
+  constexpr bool STAGE = OUT;
+  if (STAGE) {
+    stage_in(ws.cell, s.cell, base, s.n, lane);
+    stage_in(ws.fr, s.fr, base, s.n, lane);
+    stage_in(ws.fz, s.fz, base, s.n, lane);
+    stage_in(ws.ur, s.ur, base, s.n, lane);
+    stage_in(ws.uphi, s.uphi, base, s.n, lane);
+    stage_in(ws.uz, s.uz, base, s.n, lane);
+    stage_in(ws.w, s.w, base, s.n, lane);
+  }
+  if (STAGE && has_alive) {
 #pragma unroll
     for (int j = 0; j < F32_PER_LANE; j++) {
       const long long e = base + F32_PER_LANE * lane + j;
@@ -414,8 +421,8 @@ __device__ __forceinline__ void f32_warp_chunk(const GridDev &g, const SpeciesF3
     const int slot = 32 * jp + lane;
     const long long p = base + F32_PER_LANE * lane + jp;
     bool live = p < s.n;
-    if (live && has_alive && !ws.alive[slot]) live = false;
-    int c = live ? ws.cell[slot] : 0;
+    if (live && has_alive && !(STAGE ? ws.alive[slot] : s.alive[p])) live = false;
+    int c = live ? (STAGE ? ws.cell[slot] : s.cell[p]) : 0;
     if (live && (c < 0 || c >= (g.nr - 1) * ncz)) {
       flag32(g, ERR_OUT_OF_GRID);
       live = false;
@@ -434,9 +441,18 @@ __device__ __forceinline__ void f32_warp_chunk(const GridDev &g, const SpeciesF3
     }
     const int k = c - i * ncz;
     if (live) {
-      const float a = ws.fr[slot], b = ws.fz[slot];
-      float u[3] = {ws.ur[slot], ws.uphi[slot], ws.uz[slot]};
-      const float w = ws.w[slot];
+      const float a = STAGE ? ws.fr[slot] : s.fr[p], b = STAGE ? ws.fz[slot] : s.fz[p];
+      float u[3];
+      if (STAGE) {
+        u[0] = ws.ur[slot];
+        u[1] = ws.uphi[slot];
+        u[2] = ws.uz[slot];
+      } else {
+        u[0] = s.ur[p];
+        u[1] = s.uphi[p];
+        u[2] = s.uz[p];
+      }
+      const float w = STAGE ? ws.w[slot] : s.w[p];
       // ---- gather E (time n) and H (time n+1/2)
       int ir_h, kz_h;
       float wrh0, wrh1, wrn0, wrn1, wzh0, wzh1;
@@ -590,22 +606,37 @@ __device__ __forceinline__ void f32_warp_chunk(const GridDev &g, const SpeciesF3
         u[0] = u0;
         u[1] = u1;
       }
-      if (has_alive) ws.alive[slot] = alive_now ? 1 : 0;
+      if (has_alive) {
+        if (STAGE)
+          ws.alive[slot] = alive_now ? 1 : 0;
+        else
+          s.alive[p] = alive_now ? 1 : 0;
+      }
       if (in > g.nr - 2 || kn > g.nz - 2) {
         flag32(g, ERR_OUT_OF_GRID);
         in = min(in, g.nr - 2);
         kn = min(kn, g.nz - 2);
       }
-      ws.cell[slot] = in * ncz + kn;
-      ws.fr[slot] = an;
-      ws.fz[slot] = bn;
-      ws.ur[slot] = u[0];
-      ws.uphi[slot] = u[1];
-      ws.uz[slot] = u[2];
+      if (STAGE) {
+        ws.cell[slot] = in * ncz + kn;
+        ws.fr[slot] = an;
+        ws.fz[slot] = bn;
+        ws.ur[slot] = u[0];
+        ws.uphi[slot] = u[1];
+        ws.uz[slot] = u[2];
+      } else {
+        s.cell[p] = in * ncz + kn;
+        s.fr[p] = an;
+        s.fz[p] = bn;
+        s.ur[p] = u[0];
+        s.uphi[p] = u[1];
+        s.uz[p] = u[2];
+      }
     }
   }
   warp_run_deposit<0>(g, acc_phi);
   warp_run_deposit<1>(g, acc_rz);
+  if (!STAGE) return;
   __syncwarp();
   // particles skipped above (dead, not yet injected) keep their staged state
   int *cell_o = OUT ? o.cell : s.cell;
